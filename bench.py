@@ -1,0 +1,341 @@
+#!/usr/bin/env python
+"""Throughput of the RTMC phonon transport hot path on B200.
+
+Workload (the metric's configuration): a thin film 300 x 300 x 145 nm
+(x transport between the two heat baths, z thickness, y periodic), pierced by
+3 through-thickness cylindrical holes of radius 50 nm at seeded positions,
+diffuse hole and z walls; a seeded Si-like 2000-mode spectrum with 64
+frequency bins; every mode runs at its own bulk MFP (per-mode gray runs);
+Nangle = 11 (10 simulated incident angles), 500 particles per (mode, angle):
+10^7 trajectories per step and per GPU.
+
+A step is one ptg_kappa call: the persistent FP32 transport kernel over all
+10^7 trajectories plus the FP64 kappa / per-bin reduction.
+  value : free flights / device time (CUDA events on the handle's stream
+          around the transport and reduction kernels), inputs resident.
+  e2e   : the same flights / wall time of the whole C-ABI call with host
+          buffers (task tables and mode constants copied in, kappa, bins and
+          EMFPs copied out).
+The plain FP64 one-phonon-per-thread kernel is timed on the same workload as
+the comparator, the CPU oracle (OpenMP, all host cores) on a bounded sample.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import datetime
+import importlib.util
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "p-trans_b200")
+
+METRIC = "phonon free-flights/s on 1 B200, batched FP32 vs plain FP64, at ≤1% κ std-err"
+UNIT = "free-flights/s"
+BYTES_PER_FLIGHT = 64       # FP32 SoA state: 32 B read + 32 B written per free flight
+FLOPS_PER_FLIGHT_C2 = 702   # 6 box quads x 95 + 3 z-cylinders x 24 + 60 per event
+FP32_PEAK_NOMINAL = 148 * 128 * 2 * 1.965e9 / 1e12   # TFLOP/s, 148 SMs x 128 lanes x FMA
+
+
+def load_pkg():
+    if "ptrans_b200" in sys.modules:
+        return sys.modules["ptrans_b200"]
+    spec = importlib.util.spec_from_file_location(
+        "ptrans_b200", os.path.join(PKG_DIR, "__init__.py"), submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["ptrans_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def workload(pkg, n_modes=2000, np_per_task=500):
+    A, synth = pkg.abi, pkg.synth
+    model = synth.film_with_holes(lx=300.0, ly=300.0, lz=145.0, nholes=3, radius=50.0, seed=0,
+                                  periodic_y=True, p_hole=0.0, t_hole=0.0, p_z=0.0)
+    spec = synth.spectrum(n_modes, seed=0)
+    cfg = {"workload": "thin film 300x300x145 nm, 3 z-holes r=50 nm (voids, diffuse), y periodic, "
+                       "z diffuse; 2000-mode Si-like spectrum, 64 bins; per-mode MFP runs",
+           "modes": n_modes, "bins": 64, "nangle": 11, "particles_per_task": np_per_task,
+           "samples_per_gpu": n_modes * 10 * np_per_task,
+           "l2": "256 MiB written between timed steps"}
+    return model, spec, cfg
+
+
+def make_run(pkg, spec, np_total, rank, nranks, precision, seed=12345):
+    A = pkg.abi
+    return A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=11, np_=np_total, seed=seed, rank=rank,
+                      nranks=nranks, precision=precision, temperature=300.0, nbins=64,
+                      bin_omega=(0.0, 15.0 * 2 * math.pi * 1e12))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.p = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_dev{device}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-i", str(self.device), "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_flight():
+    """DRAM bytes per free flight of the persistent kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "persistent_fp32_thinfilm_dram.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["dram_bytes_per_flight"])
+    return None
+
+
+def cpu_baseline(pkg, model, spec, target_s=10.0):
+    """The oracle (OpenMP, all host threads) on a bounded sample of the workload:
+    every (mode, angle) task with fewer particles."""
+    if ROOT not in sys.path:
+        sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    o = O.Oracle(model=model, spectrum=spec)
+    n = 2
+    run = make_run(pkg, spec, n, 0, 1, 0)
+    _, _, r = o.counts(run)
+    rate = r["flights"] / max(r["seconds"], 1e-6)
+    per_particle = r["seconds"] / n
+    n = max(2, min(500, int(target_s / max(per_particle, 1e-9))))
+    run = make_run(pkg, spec, n, 0, 1, 0)
+    _, _, r = o.counts(run)
+    return {"value": r["flights"] / r["seconds"], "unit": UNIT, "cores": int(r["threads"]),
+            "kind": "port", "seconds": r["seconds"], "flights": int(r["flights"]),
+            "sample": f"all 20000 (mode, angle) tasks with {n} particles each instead of 500 "
+                      f"({r['samples']} trajectories), same geometry, spectrum and seed"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    pkg = load_pkg()
+    model, spec, cfg = workload(pkg)
+    if ROOT not in sys.path:
+        sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    o = O.Oracle(model=model, spectrum=spec)
+    # size each step to about 5 s of CPU work
+    run = make_run(pkg, spec, 2, 0, 1, 0)
+    _, _, r = o.counts(run)
+    n = max(2, min(500, int(5.0 / max(r["seconds"] / 2, 1e-9))))
+    run = make_run(pkg, spec, n, 0, 1, 0)
+    for _ in range(args.warmup):
+        o.counts(run)
+    fl, sec = 0, 0.0
+    for _ in range(args.steps):
+        _, _, r = o.counts(run)
+        fl += r["flights"]
+        sec += r["seconds"]
+    v = fl / sec
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": cfg,
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": int(r["threads"]), "kind": "port",
+                             "sample": f"all 20000 (mode, angle) tasks with {n} particles each per step"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--np", type=int, default=500, help="particles per (mode, angle) per GPU")
+    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    pkg = load_pkg()
+    A = pkg.abi
+    model, spec, cfg = workload(pkg, np_per_task=args.np)
+    gb = A.GeomBuf(model)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def maxall(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sumall(x):
+        if dist is None:
+            return x
+        t = torch.tensor([float(x)], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t)
+        return float(t.item())
+
+    h = A.Handle(gb.view, spec, device=local)
+    run32 = make_run(pkg, spec, args.np * world, rank, world, A.PREC_FP32)
+    for _ in range(args.warmup):
+        h.kappa(run32)
+    clk = ClockSampler(local)
+    clk.start()
+    barrier()
+    dev_ms = kern_ms = wall = 0.0
+    flights = 0
+    h2d = d2h = 0
+    out = None
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = h.kappa(run32)
+        t1 = time.perf_counter()
+        st = h.stats()
+        wall += t1 - t0
+        kern_ms += st["kernel_ms"]
+        dev_ms += st["kernel_ms"] + st["reduce_ms"]
+        flights += st["flights"]
+        h2d, d2h = st["h2d_bytes"], st["d2h_bytes"]
+    barrier()
+    clocks = clk.stop()
+    launches_per_step = st["launches"]
+    grid, block = st["grid"], st["block"]
+    dev_ms, kern_ms, wall = maxall(dev_ms), maxall(kern_ms), maxall(wall)
+    flights = sumall(flights)
+    value = flights / (dev_ms * 1e-3)
+    e2e = flights / wall
+
+    # plain FP64 one-phonon-per-thread comparator on the same workload
+    run64 = make_run(pkg, spec, args.np * world, rank, world, A.PREC_FP64)
+    h.kappa(run64)
+    barrier()
+    f64_ms, f64_flights = 0.0, 0
+    for _ in range(args.fp64_steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        h.kappa(run64)
+        s64 = h.stats()
+        f64_ms += s64["kernel_ms"] + s64["reduce_ms"]
+        f64_flights += s64["flights"]
+    barrier()
+    f64_ms = maxall(f64_ms)
+    f64_flights = sumall(f64_flights)
+    fp64_value = f64_flights / (f64_ms * 1e-3)
+
+    result = None
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        per_launch_flights = flights / world / args.steps
+        launch_s = kern_ms / args.steps * 1e-3
+        achieved = BYTES_PER_FLIGHT * per_launch_flights / launch_s / 1e9
+        tpf = traffic_per_flight()
+        result = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: seeded film geometry and 2000-mode spectrum",
+            "config": dict(cfg, samples_total=cfg["samples_per_gpu"] * world,
+                           parallelism=f"{world} GPU(s), particle-strided shards, counts all-reduced"),
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches_per_step * args.steps),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
+                         "bytes_per_flight": BYTES_PER_FLIGHT,
+                         "traffic": (tpf * per_launch_flights) if tpf is not None else None,
+                         "kernel": "k_persistent", "launch_ms": launch_s * 1e3, "grid": grid, "block": block},
+            "fp32_roofline": {"flops_per_flight": FLOPS_PER_FLIGHT_C2,
+                              "achieved_tflops": FLOPS_PER_FLIGHT_C2 * per_launch_flights / launch_s / 1e12,
+                              "peak_tflops_nominal": FP32_PEAK_NOMINAL},
+            "plain_fp64": {"value": fp64_value, "unit": UNIT, "ms_per_step": f64_ms / args.fp64_steps,
+                           "speedup_fp32_over_fp64": value / fp64_value},
+            "kappa": out["kappa"] if out else None,
+            "kappa_stderr": out["kappa_stderr"] if out else None,
+            "kappa_rel_stderr": (out["kappa_stderr"] / out["kappa"]) if out and out["kappa"] else None,
+            "clocks": clocks,
+        }
+        if world == 1 and not args.no_cpu:
+            result["cpu_baseline"] = cpu_baseline(pkg, model, spec)
+    h.close()
+    del flush
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if result is not None:
+        print(json.dumps(result))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,318 @@
+/*
+ * ptrans_gpu.h - C ABI of the B200 (sm_100a) Monte Carlo ray-tracing (RTMC)
+ * phonon transport hot path.
+ *
+ * The reference solver (P-TRANS, Fortran module RTMC in src/RTMCphon.f90) runs
+ *   RayTrace -> TransmissionFunction -> calcTransmit -> findCollisionSurface /
+ *   calcSurfaceDistance* -> reflect* / determin* -> tally
+ * and then effectiveMFP (Simpson over the incident angle) and the kappa sum of
+ * fileoutput.  This header is the drop-in seam for that path: every entry point
+ * uses only int32_t / int64_t / uint64_t / double, plain pointers and structs of
+ * those, so a Fortran host binds it with ISO_C_BINDING (bind(C)).
+ *
+ * Conventions
+ *  - Every function returns an int status: PTG_OK (0) on success, matching the
+ *    reference loaders' "status /= 0 means error" convention
+ *    (src/RTMCphon.f90:254-269).  RayTrace's inverted logical status
+ *    (src/RTMCphon.f90:3427-3432) stays on the Fortran side.
+ *  - Indices inside arrays follow the reference: materials and grains are
+ *    1-based where the reference is 1-based (grain_to, material ids); array
+ *    positions are 0-based.  Two-dimensional arrays are Fortran column-major.
+ *  - Lengths are in nm, like the reference's box and mean free paths.
+ *  - The caller owns every input and output array.  A handle owns device
+ *    buffers only; no caller pointer is kept past a call.
+ *  - A handle is not re-entrant: one handle per host thread, one CUDA stream
+ *    per handle.
+ *
+ * Random numbers: counter-based Philox4x32-10.  Key = (lo32(seed), hi32(seed)),
+ * counter = (flight_no, sub | stream<<8, lo32(sample), hi32(sample)) where
+ *   sample = task * np + particle      (particle 0-based, 0 <= particle < np)
+ *   flight_no = 0 for the emission draws, n >= 1 for the n-th free flight.
+ * The task numbering is fixed by this header (see ptg_run), so a trajectory is
+ * the same whichever rank, kernel or launch runs it.
+ */
+#ifndef PTRANS_GPU_H
+#define PTRANS_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define PTG_OK              0
+#define PTG_ERR_INVALID     1  /* bad argument or inconsistent input        */
+#define PTG_ERR_CUDA        2  /* a CUDA runtime call failed                 */
+#define PTG_ERR_NO_DEVICE   3  /* no usable sm_100 device                    */
+#define PTG_ERR_TIMEOUT     4  /* a bounded device wait gave up              */
+#define PTG_ERR_LOST        5  /* lost-phonon fraction above the set limit   */
+#define PTG_ERR_NOMEM       6  /* allocation failed                          */
+#define PTG_ERR_IO          7  /* file missing or malformed                  */
+#define PTG_ERR_UNSUPPORTED 8  /* combination not implemented                */
+
+/* ---- enumerations (values equal the reference's parameters) ------------ */
+/* src/RTMCphon.f90:72-74 */
+#define PTG_SHAPE_POLYGON   1
+#define PTG_SHAPE_SPHERE    2
+#define PTG_SHAPE_CYLINDER  3   /* infinite cylinder, axis parallel to z */
+/* src/RTMCphon.f90:77-79 */
+#define PTG_TRANS_VALUE     1
+#define PTG_TRANS_GAMMA     2
+#define PTG_TRANS_TBC       3
+/* src/RTMCphon.f90:127-132 */
+#define PTG_MFP_MATTHIESSEN 1   /* no MeanFreePath key: ballistic MC + Matthiessen */
+#define PTG_MFP_GRID        2   /* MeanFreePath grid + linear interpolation        */
+#define PTG_MFP_PER_MODE    3   /* extension: each mode run at its own bulk MFP    */
+#define PTG_GRAIN_VORONOI   1
+#define PTG_GRAIN_BRICKS    2
+/* box face boundary kind (extension; 0 keeps the reference behaviour:
+   x faces absorb, the other faces reflect with CellSpecularity) */
+#define PTG_FACE_REFERENCE  0
+#define PTG_FACE_PERIODIC   1
+/* kernel selection */
+#define PTG_PREC_FP32       0   /* persistent FP32 kernel, FP64 tallies       */
+#define PTG_PREC_FP64       1   /* plain FP64 one-phonon-per-thread kernel    */
+
+/* material_to codes in ptg_model.surf_material_to */
+#define PTG_MATERIAL_INTERNAL  0   /* "Internal": connects to the fill grain */
+#define PTG_MATERIAL_BOUNDARY (-1) /* "Boundary" or any name not in the list */
+
+/*
+ * Raw structure description: what loadMCP reads from a .mcp file
+ * (loadParameterBox src/RTMCphon.f90:279-420, loadParameterTransmission
+ * :749-890, loadGeometry :894-1251).  ptg_geometry_build turns it into the
+ * built geometry exactly as setupBoxGrain / setupSurfaceGeometry /
+ * setupSurfaceTransmissivity / setupFillGrain do (:1253-1491).
+ */
+typedef struct ptg_model {
+  double box[3];            /* param%boxx/y/z = LXcell*NXcell ... [nm]          */
+  double cellspec[6];       /* CellSpecularity for x-,x+,y-,y+,z-,z+            */
+  int32_t face_kind[6];     /* PTG_FACE_* (extension); x faces must be 0        */
+  double specfluc;          /* FluctuationSpecularity (Gaussian sigma)          */
+  double scope[2];          /* ScopeY, ScopeZ                                   */
+  double temperature;       /* temp [K]                                         */
+  int32_t kind_grain;       /* PTG_GRAIN_VORONOI or PTG_GRAIN_BRICKS            */
+  int32_t nmaterial;        /* Nm                                               */
+  int32_t nt1, nt2;         /* "Nt" table shape                                 */
+  const int32_t* tt_kind;   /* [(nt2+1)*nt1] param%kindTrans(nt2+1,nt1)         */
+  const double* tt_trans;   /* [(nt2+1)*nt1] transmissivity, or gamma for      */
+                            /*   Gamma/TBC (TBC already solved to gamma)       */
+  const double* tt_spec;    /* [(nt2+1)*nt1] specularity                        */
+  int32_t ngrain;           /* Ng                                               */
+  const int32_t* grain_shape;       /* [ngrain] PTG_SHAPE_*                     */
+  const double* grain_generatrix;   /* [3*ngrain]                               */
+  const double* grain_diameter;     /* [ngrain] (sphere / cylinder)             */
+  const int32_t* grain_material;    /* [ngrain] 1-based material index          */
+  const int32_t* grain_nfacet;      /* [ngrain] facets (polygon grains), else 1 */
+  const int32_t* facet_nvertex;     /* [nfacet_poly] vertices per facet         */
+  const double* facet_vertex;       /* [3*sum(facet_nvertex)] open polygons     */
+  const int32_t* surf_material_to;  /* [nsurf_model] PTG_MATERIAL_* or 1-based  */
+  const int32_t* surf_grain_to;     /* [nsurf_model] grain_to as read           */
+  const double* surf_spec;          /* [nsurf_model] or NULL: per-surface       */
+                                    /*   specularity override (extension)       */
+  uint64_t fluct_seed;              /* seed of the specularity fluctuation      */
+} ptg_model;
+
+/* Per-mode bulk phonon data as held in Anphon_type after loadAnphon
+   (src/RTMCphon.f90:149-163, :661-733).  Arrays are (nbranch,nkpoint)
+   column-major: element (ib,ik) is at ib + nbranch*ik. */
+typedef struct ptg_spectrum {
+  int32_t nbranch, nkpoint;
+  double rtemp;             /* RTemp [K]                                        */
+  double vol;               /* vol                                              */
+  const double* omega;      /* rad/s (file value * 0.03 * 2*pi * 1e12)          */
+  const double* tau;        /* ps, as read                                      */
+  const double* vel;        /* m/s                                              */
+  const double* mfp;        /* as read (unused by the transport)                */
+  const double* weight;     /* k-point weight                                   */
+} ptg_spectrum;
+
+/*
+ * Built geometry: the flattened form of vgrain(0:...) (src/RTMCphon.f90:94-124).
+ * Grain 0 is the box (6 surfaces in the order x-,x+,y-,y+,z-,z+), grains
+ * 1..ngrain the .mcp grains, and for bricks the fill grain ngrain+1.
+ * Surfaces of grain g are [grain_begin[g], grain_begin[g+1]).
+ */
+typedef struct ptg_geometry {
+  double box[3];
+  double scope[2];
+  int32_t face_kind[6];
+  int32_t kind_grain;
+  int32_t ngrain;           /* .mcp grains                                      */
+  int32_t igrain_fill;      /* -1 (voronoi) or ngrain+1 (bricks)                */
+  int32_t nmaterial;
+  int32_t ngrain_total;     /* ngrain+1, plus 1 for the fill grain              */
+  int32_t nsurf;            /* all surfaces of all grains                       */
+  int32_t nvertex_total;    /* closed polygons: nvertex+1 entries per surface   */
+  const int32_t* grain_begin;       /* [ngrain_total+1]                         */
+  const int32_t* grain_incident;    /* [ngrain_total]                           */
+  const double* grain_generatrix;   /* [3*ngrain_total]                         */
+  const int32_t* shape;             /* [nsurf] PTG_SHAPE_*                      */
+  const int32_t* nvertex;           /* [nsurf]                                  */
+  const int32_t* vertex_begin;      /* [nsurf] offset (in vertices)             */
+  const double* vertex;             /* [3*nvertex_total]                        */
+  const double* normal;             /* [3*nsurf]                                */
+  const double* tangent;            /* [9*nsurf] tangent(:,1..3) column-major   */
+  const double* center;             /* [3*nsurf]                                */
+  const double* radius;             /* [nsurf]                                  */
+  const int32_t* kind_trans;        /* [nsurf] PTG_TRANS_*                      */
+  const double* specularity;        /* [nsurf]                                  */
+  const double* trans_param;        /* [nsurf] value (VALUE) or gamma           */
+  const int32_t* grain_inside;      /* [nsurf]                                  */
+  const int32_t* grain_outside;     /* [nsurf]                                  */
+  const int32_t* internal;          /* [nsurf] 0/1                              */
+  const int32_t* incident;          /* [nsurf] 0/1                              */
+  const int32_t* material1;         /* [nsurf]                                  */
+  const int32_t* material2;         /* [nsurf]                                  */
+} ptg_geometry;
+
+/* Handle options, fixed at ptg_create. Zero-initialise and set what you need. */
+typedef struct ptg_options {
+  int32_t device;           /* CUDA device ordinal                              */
+  int32_t block_size;       /* persistent kernel threads per block (0 = tuned)  */
+  int32_t blocks_per_sm;    /* persistent kernel residency (0 = occupancy)      */
+  int32_t regen_threshold;  /* idle lanes before a warp refills (0 = 1)         */
+  int32_t ref_quirks;       /* 1: a lost phonon also counts as transmitted      */
+                            /*    (src/RTMCphon.f90:1701 then :1833)            */
+  int32_t bvh_leaf;         /* BVH leaf size (0 = tuned)                        */
+  int64_t max_flights;      /* per-trajectory cap, lost when reached (0 = 2^31-1) */
+  double lost_limit;        /* PTG_ERR_LOST if lost/total exceeds it (0 = off)  */
+  int64_t chunk;            /* samples per work-queue chunk (0 = tuned)         */
+} ptg_options;
+
+/*
+ * One transport run.  Tasks are numbered
+ *   MATTHIESSEN / PER_MODE : task = ib + nb*(ik + nk*ia)
+ *   GRID                   : task = ib + nb*(ik + nk*(s + nmfp*ia))
+ * with ia in [0, nangle-2] (the last angle, pi/2, is never simulated,
+ * src/RTMCphon.f90:1576) and theta_ia = ia/(nangle-1) * pi/2
+ * (src/RTMCphon.f90:1554-1556).  Rank r of nranks runs the particles
+ * p = r, r+nranks, ... of every task (src/RTMCphon.f90:1627).
+ */
+typedef struct ptg_run {
+  int32_t kind_mfp;         /* PTG_MFP_*                                        */
+  int32_t nangle;           /* odd, >= 3 (Simpson)                              */
+  int64_t np;               /* particles per task                               */
+  int32_t nmfp;             /* GRID: number of grid points                      */
+  const double* mfp_grid_nm;/* GRID: [nmfp] ascending, > 0                      */
+  uint64_t seed;
+  int32_t stream;           /* 0..2^24-1, separates runs that share a seed      */
+  int32_t rank, nranks;     /* particle striding (nranks >= 1)                  */
+  int32_t precision;        /* PTG_PREC_FP32 or PTG_PREC_FP64                   */
+  double temperature;       /* param%temperature [K] (tau rescale, heat capacity) */
+  int32_t nbins;            /* per-frequency-bin outputs (0 = none)             */
+  double bin_omega_min, bin_omega_max;   /* rad/s                               */
+  double scatter_scale;     /* multiplies intrinsic scattering rates (0 = 1)    */
+} ptg_run;
+
+/* Results of ptg_kappa.  Pointers are caller-owned outputs (NULL = skip). */
+typedef struct ptg_kappa_out {
+  double kappa;             /* W m^-1 K^-1, sum of Thermal_conductivity         */
+  double kappa_stderr;
+  double* bin_T;            /* [nbins] flux-weighted <T> per frequency bin      */
+  double* bin_T_stderr;     /* [nbins]                                          */
+  double* emfp_nm;          /* [nbranch*nkpoint] effective MFP per mode [nm]    */
+  double* transmit;         /* [ntask_total + angle padding] see ptg_transmission */
+  uint64_t* counts;         /* [ntask] transmitted counts of this rank          */
+  uint64_t flights;         /* free flights simulated by this call              */
+  uint64_t lost;            /* lost phonons                                     */
+  uint64_t samples;         /* trajectories simulated                           */
+  double kernel_ms;         /* device time of the transport kernel(s)           */
+} ptg_kappa_out;
+
+/* Statistics of the last call on a handle. */
+typedef struct ptg_stats {
+  uint64_t flights, lost, samples, capped;
+  double kernel_ms;         /* CUDA-event time of the transport kernel          */
+  double reduce_ms;         /* CUDA-event time of the kappa reduction kernel    */
+  int32_t launches;         /* kernels launched by the call                     */
+  int32_t grid, block;      /* transport launch shape                           */
+  uint64_t h2d_bytes;       /* host-to-device bytes copied by the call          */
+  uint64_t d2h_bytes;       /* device-to-host bytes copied by the call          */
+} ptg_stats;
+
+typedef struct ptg_handle ptg_handle;
+typedef struct ptg_geombuf ptg_geombuf;
+
+/* ---- host-side geometry construction (no device needed) ---------------- */
+
+/* Builds the geometry as loadGeometry/setupBoxGrain/setupFillGrain do.
+   Replaces src/RTMCphon.f90:894-1491 (the part after the text parse). */
+int ptg_geometry_build(const ptg_model* model, const ptg_spectrum* spec,
+                       ptg_geombuf** out);
+const ptg_geometry* ptg_geombuf_view(const ptg_geombuf* buf);
+void ptg_geombuf_free(ptg_geombuf* buf);
+
+/* Parses a .mcp file (src/RTMCphon.f90:252-1251).  The returned buffer owns
+   the ptg_model arrays; anphon_name receives the first material name
+   (the reference loads Materials/<name>.anphon, :671). */
+typedef struct ptg_mcpbuf ptg_mcpbuf;
+int ptg_mcp_load(const char* path, ptg_mcpbuf** out);
+const ptg_model* ptg_mcpbuf_model(const ptg_mcpbuf* buf);
+int ptg_mcpbuf_info(const ptg_mcpbuf* buf, int64_t* np, int32_t* nangle,
+                    int32_t* kind_mfp, int32_t* nmfp, double* mfp_grid_nm,
+                    int32_t* particle_trace, char* material1, int32_t len);
+void ptg_mcpbuf_free(ptg_mcpbuf* buf);
+
+/* Reads / writes the .anphon mode table (src/RTMCphon.f90:661-733). */
+typedef struct ptg_anphonbuf ptg_anphonbuf;
+int ptg_anphon_load(const char* path, ptg_anphonbuf** out);
+const ptg_spectrum* ptg_anphonbuf_spectrum(const ptg_anphonbuf* buf);
+void ptg_anphonbuf_free(ptg_anphonbuf* buf);
+int ptg_anphon_write(const char* path, const ptg_spectrum* s);
+
+/* ---- device handle ------------------------------------------------------ */
+
+/* Uploads geometry and spectrum to the device and sizes the work buffers. */
+int ptg_create(const ptg_geometry* geom, const ptg_spectrum* spec,
+               const ptg_options* opt, ptg_handle** out);
+/* Replaces the spectrum (same nbranch, nkpoint). */
+int ptg_set_spectrum(ptg_handle* h, const ptg_spectrum* spec);
+void ptg_destroy(ptg_handle* h);
+const char* ptg_strerror(int status);
+
+/*
+ * The body of TransmissionFunction (src/RTMCphon.f90:1544-1604) for one gray
+ * mean free path: fills transmit(nbranch,nkpoint,nangle) column-major with
+ * (transmitted particles of this rank)/np, transmit(:,:,nangle) = 0, exactly
+ * what calcTransmit leaves before the MPI_Allreduce (:1584-1590).
+ * mfp_nm = 1e10 means ballistic (:1686-1690).  stderr_opt (same shape, may be
+ * NULL) receives sqrt(T(1-T)/np) with T the rank-local value.
+ * precision selects the kernel (PTG_PREC_FP32 / PTG_PREC_FP64).
+ */
+int ptg_transmission(ptg_handle* h, double mfp_nm, int32_t nangle, int64_t np,
+                     int32_t rank, int32_t nranks, uint64_t seed,
+                     int32_t precision, double* transmit, double* stderr_opt);
+
+/*
+ * Transport for every task of a run, then effectiveMFP (Simpson,
+ * src/RTMCphon.f90:2418-2451) and the kappa sum of fileoutput
+ * (:2645-2755) as an FP64 reduction on the device.  out->transmit, when set,
+ * has nb*nk*nmfp_eff*nangle entries laid out like the task numbering with
+ * the angle slowest (nmfp_eff = nmfp for GRID, else 1).
+ */
+int ptg_kappa(ptg_handle* h, const ptg_run* run, ptg_kappa_out* out);
+
+/*
+ * Host FP64 assembly of kappa from (all-reduced) transmitted counts, for a
+ * multi-rank caller that sums ptg_kappa_out.counts across ranks first, as the
+ * reference sums transmit with MPI_Allreduce (src/RTMCphon.f90:1587).
+ * counts has one entry per task (ptg_run numbering, angle nangle-1 excluded).
+ */
+int ptg_kappa_from_counts(const ptg_geometry* geom, const ptg_spectrum* spec,
+                          const ptg_run* run, const uint64_t* counts,
+                          ptg_kappa_out* out);
+
+/* Statistics of the last transport call on h. */
+int ptg_last_stats(const ptg_handle* h, ptg_stats* st);
+
+/* Debug / replay: runs the FP64 kernel for one task and writes, per particle,
+   the exit side (0 lost, 1 x-, 2 x+) and the number of free flights. */
+int ptg_replay_task(ptg_handle* h, const ptg_run* run, int64_t task,
+                    int32_t* end_side, uint32_t* flights, double* final_pos);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PTRANS_GPU_H */

@@ -1,0 +1,848 @@
+/*
+ * api.cpp - the C ABI of include/ptrans_gpu.h: device handles, task and
+ * work-queue construction, kernel launches and the FP64 kappa assembly.
+ *
+ * The transport entry points replace the body of TransmissionFunction
+ * (src/RTMCphon.f90:1544-1604); ptg_kappa additionally replaces effectiveMFP
+ * (:2418-2451) and the kappa sum of fileoutput (:2645-2755).
+ */
+#include <cuda_runtime.h>
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <new>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+#include "ptg_internal.h"
+
+namespace {
+
+/* Growable device buffer. */
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= cap) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = bytes < 256 ? 256 : bytes;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e == cudaSuccess) cap = want;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+  template <class T>
+  T* as() const { return static_cast<T*>(p); }
+};
+
+#define CU(x)                                  \
+  do {                                         \
+    cudaError_t e_ = (x);                      \
+    if (e_ != cudaSuccess) {                   \
+      h->last_error = cudaGetErrorString(e_);  \
+      return PTG_ERR_CUDA;                     \
+    }                                          \
+  } while (0)
+
+}  // namespace
+
+struct ptg_handle {
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  ptg_options opt;
+  ptg::GeomSoA geom;
+  ptg::SpecSoA spec;
+  std::string last_error;
+  ptg_stats last;
+  /* FP64 geometry */
+  std::vector<DevBuf*> owned;
+  ptg::Geo64 g64;
+  /* FP32 blob */
+  DevBuf blob;
+  ptg::GeoF32 g32;
+  size_t blob_bytes = 0;
+  /* work buffers */
+  DevBuf task, chunk, counts, lost, stats, queue;
+  /* reduction */
+  DevBuf red_coef, red_K, red_W, red_mfp, red_bin, red_grid, red_tc, red_kv, red_bw, red_bv,
+      red_emfp, red_trans, red_result;
+  ~ptg_handle() {
+    for (DevBuf* b : owned) { b->release(); delete b; }
+    DevBuf* all[] = {&blob, &task, &chunk, &counts, &lost, &stats, &queue, &red_coef, &red_K,
+                     &red_W, &red_mfp, &red_bin, &red_grid, &red_tc, &red_kv, &red_bw, &red_bv,
+                     &red_emfp, &red_trans, &red_result};
+    for (DevBuf* b : all) b->release();
+    for (cudaEvent_t e : ev) if (e) cudaEventDestroy(e);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+template <class T>
+int upload(ptg_handle* h, const std::vector<T>& v, const T** out) {
+  DevBuf* b = new DevBuf();
+  h->owned.push_back(b);
+  const size_t bytes = sizeof(T) * (v.size() ? v.size() : 1);
+  CU(b->ensure(bytes));
+  if (!v.empty()) CU(cudaMemcpy(b->p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+  *out = static_cast<const T*>(b->p);
+  return PTG_OK;
+}
+
+/* ---- FP32 geometry blob -------------------------------------------------- */
+
+inline float4 f4(double a, double b, double c, double d) {
+  return make_float4((float)a, (float)b, (float)c, (float)d);
+}
+inline float4 i4(int a, int b, int c, int d) {
+  float4 v;
+  memcpy(&v.x, &a, 4);
+  memcpy(&v.y, &b, 4);
+  memcpy(&v.z, &c, 4);
+  memcpy(&v.w, &d, 4);
+  return v;
+}
+
+int build_blob(ptg_handle* h) {
+  const ptg::GeomSoA& G = h->geom;
+  const int ns = G.nsurf(), ngt = G.ngrain_total();
+  std::vector<float4> hot(2 * (size_t)ns), cold(3 * (size_t)ns), edges;
+  std::vector<int> geom_id(ns);
+  for (int s = 0; s < ns; ++s) geom_id[s] = s;
+  /* a fill-grain quadric is the same physical surface as its brick's */
+  if (G.kind_grain == PTG_GRAIN_BRICKS && G.igrain_fill > 0) {
+    const int fb = G.grain_begin[G.igrain_fill], fe = G.grain_begin[G.igrain_fill + 1];
+    for (int s = fb; s < fe; ++s) {
+      if (G.shape[s] == PTG_SHAPE_POLYGON) continue;
+      for (int t = G.grain_begin[1]; t < fb; ++t) {
+        if (G.shape[t] == G.shape[s] && G.radius[t] == G.radius[s] &&
+            G.center[3 * t] == G.center[3 * s] && G.center[3 * t + 1] == G.center[3 * s + 1] &&
+            G.center[3 * t + 2] == G.center[3 * s + 2]) {
+          geom_id[s] = t;
+          break;
+        }
+      }
+    }
+  }
+  for (int g = 0; g < ngt; ++g) {
+    for (int s = G.grain_begin[g]; s < G.grain_begin[g + 1]; ++s) {
+      const double* n = &G.normal[3 * s];
+      const double* t = &G.tangent[9 * s];
+      const int meta = (G.kind_trans[s] & 0xff) | (G.grain_outside[s] << 8);
+      cold[3 * s + 0] = f4(t[0], t[1], t[2], G.specularity[s]);
+      cold[3 * s + 1] = f4(t[3], t[4], t[5], G.trans_param[s]);
+      cold[3 * s + 2] = f4(n[0], n[1], n[2], 0.0);
+      memcpy(&cold[3 * s + 2].w, &meta, 4);
+      const double* c = &G.center[3 * s];
+      if (G.shape[s] == PTG_SHAPE_POLYGON) {
+        const int nv = G.nvertex[s];
+        const double* v = &G.vertex[3 * (size_t)G.vertex_begin[s]];
+        /* winding normal: sum of the consecutive-triple cross products */
+        double wn[3] = {0, 0, 0};
+        for (int i = 0; i < nv; ++i) {
+          const double* p0 = v + 3 * i;
+          const double* p1 = v + 3 * ((i + 1) % nv);
+          const double* p2 = v + 3 * ((i + 2) % nv);
+          double a[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+          double b[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
+          wn[0] += a[1] * b[2] - a[2] * b[1];
+          wn[1] += a[2] * b[0] - a[0] * b[2];
+          wn[2] += a[0] * b[1] - a[1] * b[0];
+        }
+        double ln = sqrt(wn[0] * wn[0] + wn[1] * wn[1] + wn[2] * wn[2]);
+        if (!(ln > 0.0)) { h->last_error = "degenerate polygon"; return PTG_ERR_INVALID; }
+        for (int d = 0; d < 3; ++d) wn[d] /= ln;
+        const int e0 = (int)edges.size();
+        for (int i = 0; i < nv; ++i) {
+          const double* p0 = v + 3 * i;
+          const double* p1 = v + 3 * (i + 1);
+          double e[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+          double m[3] = {wn[1] * e[2] - wn[2] * e[1], wn[2] * e[0] - wn[0] * e[2],
+                         wn[0] * e[1] - wn[1] * e[0]};
+          double lm = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+          if (!(lm > 0.0)) { lm = 1.0; }
+          for (int d = 0; d < 3; ++d) m[d] /= lm;
+          edges.push_back(f4(m[0], m[1], m[2], m[0] * p0[0] + m[1] * p0[1] + m[2] * p0[2]));
+        }
+        const double d0 = n[0] * v[0] + n[1] * v[1] + n[2] * v[2];
+        hot[2 * s] = f4(n[0], n[1], n[2], d0);
+        hot[2 * s + 1] = i4(ptg::REC_POLY, e0, nv, geom_id[s]);
+      } else if (G.shape[s] == PTG_SHAPE_SPHERE) {
+        const int interior = (g != G.igrain_fill) ? ptg::REC_INTERIOR : 0;
+        hot[2 * s] = f4(c[0], c[1], c[2], G.radius[s]);
+        hot[2 * s + 1] = i4(ptg::REC_SPHERE | interior, 0, 0, geom_id[s]);
+      } else {
+        const int interior = (g != G.igrain_fill) ? ptg::REC_INTERIOR : 0;
+        hot[2 * s] = f4(c[0], c[1], G.radius[s], 0.0);
+        hot[2 * s + 1] = i4(ptg::REC_CYL | interior, 0, 0, geom_id[s]);
+      }
+    }
+  }
+  std::vector<int> cb(ngt + 1, 0), cand;
+  for (int g = 0; g < ngt; ++g) {
+    cb[g] = (int)cand.size();
+    if (g == 0) continue;
+    for (int s = G.grain_begin[g]; s < G.grain_begin[g + 1]; ++s)
+      if (G.internal[s]) cand.push_back(s);
+  }
+  cb[ngt] = (int)cand.size();
+  std::vector<float4> start;
+  for (int g = 1; g <= G.ngrain; ++g) {
+    if (!G.grain_incident[g]) continue;
+    if (G.kind_grain == PTG_GRAIN_VORONOI) {
+      float4 v = f4(G.grain_generatrix[3 * g], G.grain_generatrix[3 * g + 1],
+                    G.grain_generatrix[3 * g + 2], 0.0);
+      memcpy(&v.w, &g, 4);
+      start.push_back(v);
+    } else {
+      for (int s = G.grain_begin[g]; s < G.grain_begin[g + 1]; ++s)
+        if (G.incident[s] && G.shape[s] == PTG_SHAPE_POLYGON) start.push_back(i4(s, g, 0, 0));
+    }
+  }
+  auto units_of_ints = [](size_t n) { return (int)((n * 4 + 15) / 16); };
+  ptg::BlobLayout L;
+  L.hot = 0;
+  L.cold = L.hot + 2 * ns;
+  L.edge = L.cold + 3 * ns;
+  L.cand_begin = L.edge + (int)edges.size();
+  L.cand = L.cand_begin + units_of_ints(cb.size());
+  L.start = L.cand + units_of_ints(cand.size() ? cand.size() : 1);
+  L.total = L.start + (int)(start.size() ? start.size() : 1);
+  L.nstart = (int)start.size();
+  std::vector<float4> blob((size_t)L.total, make_float4(0, 0, 0, 0));
+  std::copy(hot.begin(), hot.end(), blob.begin() + L.hot);
+  std::copy(cold.begin(), cold.end(), blob.begin() + L.cold);
+  std::copy(edges.begin(), edges.end(), blob.begin() + L.edge);
+  memcpy(&blob[L.cand_begin], cb.data(), cb.size() * 4);
+  if (!cand.empty()) memcpy(&blob[L.cand], cand.data(), cand.size() * 4);
+  std::copy(start.begin(), start.end(), blob.begin() + L.start);
+  h->blob_bytes = blob.size() * 16;
+  CU(h->blob.ensure(h->blob_bytes));
+  CU(cudaMemcpy(h->blob.p, blob.data(), h->blob_bytes, cudaMemcpyHostToDevice));
+  ptg::GeoF32& g32 = h->g32;
+  g32.blob = h->blob.as<const float4>();
+  g32.lay = L;
+  for (int d = 0; d < 3; ++d) g32.box[d] = (float)G.box[d];
+  g32.scope[0] = (float)G.scope[0];
+  g32.scope[1] = (float)G.scope[1];
+  const double S = std::max(G.box[0], std::max(G.box[1], G.box[2]));
+  g32.eps = (float)(S * (1.0 / 1048576.0));
+  g32.periodic_mask = 0;
+  for (int f = 0; f < 6; ++f)
+    if (G.face_kind[f] == PTG_FACE_PERIODIC) g32.periodic_mask |= 1 << f;
+  g32.kind_grain = G.kind_grain;
+  g32.igrain_fill = G.igrain_fill;
+  g32.nmaterial = G.nmaterial;
+  g32.stage_smem = h->blob_bytes <= 96 * 1024 ? 1 : 0;
+  return PTG_OK;
+}
+
+int build_geo64(ptg_handle* h) {
+  const ptg::GeomSoA& G = h->geom;
+  ptg::Geo64& g = h->g64;
+  int st;
+  if ((st = upload(h, G.vertex, &g.vertex))) return st;
+  if ((st = upload(h, G.normal, &g.normal))) return st;
+  if ((st = upload(h, G.tangent, &g.tangent))) return st;
+  if ((st = upload(h, G.center, &g.center))) return st;
+  if ((st = upload(h, G.radius, &g.radius))) return st;
+  if ((st = upload(h, G.specularity, &g.spec))) return st;
+  if ((st = upload(h, G.trans_param, &g.tparam))) return st;
+  if ((st = upload(h, G.shape, &g.shape))) return st;
+  if ((st = upload(h, G.nvertex, &g.nvertex))) return st;
+  if ((st = upload(h, G.vertex_begin, &g.vbegin))) return st;
+  if ((st = upload(h, G.kind_trans, &g.kind_trans))) return st;
+  if ((st = upload(h, G.grain_outside, &g.gout))) return st;
+  if ((st = upload(h, G.internal, &g.internal))) return st;
+  if ((st = upload(h, G.incident, &g.incident))) return st;
+  if ((st = upload(h, G.grain_begin, &g.grain_begin))) return st;
+  if ((st = upload(h, G.grain_incident, &g.grain_incident))) return st;
+  if ((st = upload(h, G.grain_generatrix, &g.grain_gen))) return st;
+  for (int d = 0; d < 3; ++d) g.box[d] = G.box[d];
+  g.scope[0] = G.scope[0];
+  g.scope[1] = G.scope[1];
+  for (int f = 0; f < 6; ++f) g.face_kind[f] = G.face_kind[f];
+  g.kind_grain = G.kind_grain;
+  g.ngrain = G.ngrain;
+  g.igrain_fill = G.igrain_fill;
+  g.nmaterial = G.nmaterial;
+  g.max_omega = h->spec.max_omega;
+  return PTG_OK;
+}
+
+/* ---- one transport pass over a task list --------------------------------- */
+
+struct Transport {
+  int64_t ntask = 0;
+  int64_t np = 0, np_local = 0;
+  int32_t rank = 0, nranks = 1;
+  uint64_t seed = 0;
+  int32_t stream = 0;
+  int32_t precision = PTG_PREC_FP32;
+  const std::vector<ptg::TaskHost>* tasks = nullptr;
+};
+
+int run_transport(ptg_handle* h, const Transport& T) {
+  const int64_t ntask = T.ntask;
+  CU(cudaSetDevice(h->device));
+  CU(h->counts.ensure(sizeof(unsigned long long) * ntask));
+  CU(h->lost.ensure(sizeof(unsigned long long) * ntask));
+  CU(h->stats.ensure(sizeof(unsigned long long) * 4));
+  CU(h->queue.ensure(sizeof(int) * 4));
+  CU(cudaMemsetAsync(h->counts.p, 0, sizeof(unsigned long long) * ntask, h->stream));
+  CU(cudaMemsetAsync(h->lost.p, 0, sizeof(unsigned long long) * ntask, h->stream));
+  CU(cudaMemsetAsync(h->stats.p, 0, sizeof(unsigned long long) * 4, h->stream));
+  CU(cudaMemsetAsync(h->queue.p, 0, sizeof(int) * 4, h->stream));
+  const int64_t maxf = h->opt.max_flights > 0 ? h->opt.max_flights : 2147483647LL;
+  memset(&h->last, 0, sizeof(h->last));
+  if (T.precision == PTG_PREC_FP64) {
+    std::vector<ptg::Task64> t64(ntask);
+    for (int64_t i = 0; i < ntask; ++i) {
+      const ptg::TaskHost& th = (*T.tasks)[i];
+      t64[i] = {th.lambda, th.cth, th.sth, th.omega};
+    }
+    CU(h->task.ensure(sizeof(ptg::Task64) * ntask));
+    CU(cudaMemcpyAsync(h->task.p, t64.data(), sizeof(ptg::Task64) * ntask, cudaMemcpyHostToDevice,
+                       h->stream));
+    CU(cudaStreamSynchronize(h->stream));  /* t64 is a local buffer */
+    h->last.h2d_bytes += sizeof(ptg::Task64) * ntask;
+    ptg::Run64 r;
+    memset(&r, 0, sizeof(r));
+    r.task = h->task.as<const ptg::Task64>();
+    r.ntask = ntask;
+    r.np = T.np;
+    r.np_local = T.np_local;
+    r.rank = T.rank;
+    r.nranks = T.nranks;
+    r.k0 = (uint32_t)T.seed;
+    r.k1 = (uint32_t)(T.seed >> 32);
+    r.c1 = ((uint32_t)T.stream) << 8;
+    r.max_flights = maxf;
+    r.ref_quirks = h->opt.ref_quirks;
+    r.counts = h->counts.as<unsigned long long>();
+    r.lost = h->lost.as<unsigned long long>();
+    r.stats = h->stats.as<unsigned long long>();
+    r.replay_task = -1;
+    CU(cudaEventRecord(h->ev[0], h->stream));
+    int grid = 0, block = 0;
+    CU(ptg::launch_plain_fp64(h->g64, r, h->stream, &grid, &block));
+    CU(cudaEventRecord(h->ev[1], h->stream));
+    h->last.grid = grid;
+    h->last.block = block;
+    h->last.launches = 1;
+  } else {
+    std::vector<float4> t32(ntask);
+    std::vector<int64_t> order;
+    order.reserve(ntask);
+    for (int64_t i = 0; i < ntask; ++i) {
+      const ptg::TaskHost& th = (*T.tasks)[i];
+      float lam = th.lambda == 1.0e10 ? INFINITY : (float)th.lambda;
+      if (!(th.lambda > 0.0)) lam = 0.0f;
+      t32[i] = make_float4(lam, (float)th.cth, (float)th.sth,
+                           (float)(th.omega / h->spec.max_omega));
+      if (th.lambda > 0.0) order.push_back(i);
+    }
+    /* longest expected trajectories first: small mean free paths first */
+    std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
+      return (*T.tasks)[a].lambda < (*T.tasks)[b].lambda;
+    });
+    const int64_t csz = h->opt.chunk > 0 ? h->opt.chunk : 64;
+    std::vector<int4> chunks;
+    for (int64_t t : order) {
+      for (int64_t j = 0; j < T.np_local; j += csz) {
+        const int64_t cnt = std::min(csz, T.np_local - j);
+        chunks.push_back(make_int4((int)t, (int)j, (int)cnt, 0));
+      }
+    }
+    if (chunks.size() > 2147483647ull) { h->last_error = "too many chunks"; return PTG_ERR_INVALID; }
+    CU(h->task.ensure(sizeof(float4) * ntask));
+    CU(cudaMemcpyAsync(h->task.p, t32.data(), sizeof(float4) * ntask, cudaMemcpyHostToDevice,
+                       h->stream));
+    CU(h->chunk.ensure(sizeof(int4) * (chunks.size() + 1)));
+    if (!chunks.empty())
+      CU(cudaMemcpyAsync(h->chunk.p, chunks.data(), sizeof(int4) * chunks.size(),
+                         cudaMemcpyHostToDevice, h->stream));
+    CU(cudaStreamSynchronize(h->stream));  /* t32 and chunks are local buffers */
+    h->last.h2d_bytes += sizeof(float4) * ntask + sizeof(int4) * chunks.size();
+    ptg::RunF32 r;
+    memset(&r, 0, sizeof(r));
+    r.task = h->task.as<const float4>();
+    r.chunk = h->chunk.as<const int4>();
+    r.nchunk = (int32_t)chunks.size();
+    r.np = T.np;
+    r.rank = T.rank;
+    r.nranks = T.nranks;
+    r.k0 = (uint32_t)T.seed;
+    r.k1 = (uint32_t)(T.seed >> 32);
+    r.c1 = ((uint32_t)T.stream) << 8;
+    r.max_flights = (uint32_t)std::min<int64_t>(maxf, 4294967295LL);
+    r.ref_quirks = h->opt.ref_quirks;
+    int rt = h->opt.regen_threshold;
+    r.regen_threshold = rt < 1 ? 1 : (rt > 32 ? 32 : rt);
+    r.counts = h->counts.as<unsigned long long>();
+    r.lost = h->lost.as<unsigned long long>();
+    r.stats = h->stats.as<unsigned long long>();
+    r.queue = h->queue.as<int>();
+    const int block = 256;
+    const size_t smem = h->g32.stage_smem ? h->blob_bytes : 0;
+    int bps = 0;
+    CU(ptg::persistent_occupancy(block, smem, &bps));
+    if (h->opt.blocks_per_sm > 0 && h->opt.blocks_per_sm < bps) bps = h->opt.blocks_per_sm;
+    if (bps < 1) bps = 1;
+    const int grid = h->num_sms * bps;
+    CU(cudaEventRecord(h->ev[0], h->stream));
+    if (r.nchunk > 0) CU(ptg::launch_persistent_fp32(h->g32, r, grid, block, smem, h->stream));
+    CU(cudaEventRecord(h->ev[1], h->stream));
+    h->last.grid = grid;
+    h->last.block = block;
+    h->last.launches = 1;
+  }
+  return PTG_OK;
+}
+
+int finish_stats(ptg_handle* h) {
+  unsigned long long st[4];
+  int qerr[4];
+  CU(cudaMemcpyAsync(st, h->stats.p, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaMemcpyAsync(qerr, h->queue.p, sizeof(qerr), cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  float ms = 0.f;
+  CU(cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]));
+  h->last.d2h_bytes += sizeof(st) + sizeof(qerr);
+  h->last.flights = st[0];
+  h->last.lost = st[1];
+  h->last.capped = st[2];
+  h->last.samples = st[3];
+  h->last.kernel_ms = ms;
+  if (qerr[1] != 0) { h->last_error = "shared-memory staging wait timed out"; return PTG_ERR_TIMEOUT; }
+  return PTG_OK;
+}
+
+int64_t np_local_of(int64_t np, int32_t rank, int32_t nranks) {
+  return np > rank ? (np - rank + nranks - 1) / nranks : 0;
+}
+
+int check_lost(ptg_handle* h) {
+  if (h->opt.lost_limit > 0.0 && h->last.samples > 0 &&
+      (double)h->last.lost > h->opt.lost_limit * (double)h->last.samples) {
+    h->last_error = "lost-phonon fraction above the limit";
+    return PTG_ERR_LOST;
+  }
+  return PTG_OK;
+}
+
+}  // namespace
+
+/* ========================================================================= */
+extern "C" {
+
+const char* ptg_strerror(int status) {
+  switch (status) {
+    case PTG_OK: return "ok";
+    case PTG_ERR_INVALID: return "invalid argument or inconsistent input";
+    case PTG_ERR_CUDA: return "CUDA runtime error";
+    case PTG_ERR_NO_DEVICE: return "no usable sm_100 CUDA device";
+    case PTG_ERR_TIMEOUT: return "a bounded device wait timed out";
+    case PTG_ERR_LOST: return "lost-phonon fraction above the limit";
+    case PTG_ERR_NOMEM: return "out of memory";
+    case PTG_ERR_IO: return "file missing or malformed";
+    case PTG_ERR_UNSUPPORTED: return "unsupported combination";
+  }
+  return "unknown status";
+}
+
+int ptg_create(const ptg_geometry* geom, const ptg_spectrum* spec, const ptg_options* opt,
+               ptg_handle** out) {
+  if (!out) return PTG_ERR_INVALID;
+  *out = nullptr;
+  ptg_handle* h = new (std::nothrow) ptg_handle();
+  if (!h) return PTG_ERR_NOMEM;
+  memset(&h->opt, 0, sizeof(h->opt));
+  if (opt) h->opt = *opt;
+  memset(&h->last, 0, sizeof(h->last));
+  std::string why;
+  int st = ptg::copy_geometry(geom, &h->geom, &why);
+  if (st == PTG_OK) st = ptg::copy_spectrum(spec, &h->spec, &why);
+  if (st != PTG_OK) { delete h; return st; }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0 || h->opt.device < 0 ||
+      h->opt.device >= ndev) {
+    cudaGetLastError();
+    delete h;
+    return PTG_ERR_NO_DEVICE;
+  }
+  h->device = h->opt.device;
+  cudaDeviceProp prop;
+  if (cudaSetDevice(h->device) != cudaSuccess ||
+      cudaGetDeviceProperties(&prop, h->device) != cudaSuccess || prop.major != 10) {
+    cudaGetLastError();
+    delete h;
+    return PTG_ERR_NO_DEVICE;
+  }
+  h->num_sms = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete h;
+    return PTG_ERR_CUDA;
+  }
+  for (auto& e : h->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) { delete h; return PTG_ERR_CUDA; }
+  st = build_geo64(h);
+  if (st == PTG_OK) st = build_blob(h);
+  if (st != PTG_OK) { delete h; return st; }
+  *out = h;
+  return PTG_OK;
+}
+
+int ptg_set_spectrum(ptg_handle* h, const ptg_spectrum* spec) {
+  if (!h || !spec) return PTG_ERR_INVALID;
+  if (spec->nbranch != h->spec.nb || spec->nkpoint != h->spec.nk) return PTG_ERR_INVALID;
+  std::string why;
+  ptg::SpecSoA s;
+  int st = ptg::copy_spectrum(spec, &s, &why);
+  if (st != PTG_OK) return st;
+  h->spec = s;
+  h->g64.max_omega = h->spec.max_omega;
+  return PTG_OK;
+}
+
+void ptg_destroy(ptg_handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  delete h;
+}
+
+int ptg_transmission(ptg_handle* h, double mfp_nm, int32_t nangle, int64_t np, int32_t rank,
+                     int32_t nranks, uint64_t seed, int32_t precision, double* transmit,
+                     double* stderr_opt) {
+  if (!h || !transmit) return PTG_ERR_INVALID;
+  if (nangle < 2 || np < 1 || nranks < 1 || rank < 0 || rank >= nranks) return PTG_ERR_INVALID;
+  if (precision != PTG_PREC_FP32 && precision != PTG_PREC_FP64) return PTG_ERR_INVALID;
+  if (!(mfp_nm > 0.0)) return PTG_ERR_INVALID;
+  const int64_t nm = (int64_t)h->spec.nb * h->spec.nk;
+  const int64_t ntask = nm * (nangle - 1);
+  std::vector<ptg::TaskHost> tasks(ntask);
+  const double half_pi = 3.14159265358979323846 * 0.5;
+  for (int64_t t = 0; t < ntask; ++t) {
+    const int64_t m = t % nm, ia = t / nm;
+    const double theta = 0.0 + (double)ia / (double)(nangle - 1) * half_pi;
+    tasks[t] = {mfp_nm, cos(theta), sin(theta), h->spec.omega[m]};
+  }
+  Transport T;
+  T.ntask = ntask;
+  T.np = np;
+  T.np_local = np_local_of(np, rank, nranks);
+  if (T.np_local > 2147483647LL) return PTG_ERR_INVALID;
+  T.rank = rank;
+  T.nranks = nranks;
+  T.seed = seed;
+  T.precision = precision;
+  T.tasks = &tasks;
+  int st = run_transport(h, T);
+  if (st != PTG_OK) return st;
+  std::vector<unsigned long long> cnt(ntask);
+  CU(cudaMemcpyAsync(cnt.data(), h->counts.p, sizeof(unsigned long long) * ntask,
+                     cudaMemcpyDeviceToHost, h->stream));
+  h->last.d2h_bytes += sizeof(unsigned long long) * ntask;
+  st = finish_stats(h);
+  if (st != PTG_OK) return st;
+  for (int64_t t = 0; t < nm * nangle; ++t) {
+    double v = 0.0;
+    if (t < ntask) v = (double)cnt[t] / (double)np;
+    transmit[t] = v;
+    if (stderr_opt) stderr_opt[t] = sqrt(v * (1.0 - v) / (double)np);
+  }
+  return check_lost(h);
+}
+
+int ptg_kappa(ptg_handle* h, const ptg_run* run, ptg_kappa_out* out) {
+  if (!h || !run || !out) return PTG_ERR_INVALID;
+  std::string why;
+  if (!ptg::run_valid(h->spec, run, &why)) { h->last_error = why; return PTG_ERR_INVALID; }
+  if (run->precision != PTG_PREC_FP32 && run->precision != PTG_PREC_FP64) return PTG_ERR_INVALID;
+  const int ns = run->kind_mfp == PTG_MFP_GRID ? run->nmfp : 1;
+  if (ns > 64) { h->last_error = "at most 64 grid MFPs"; return PTG_ERR_UNSUPPORTED; }
+  std::vector<ptg::TaskHost> tasks;
+  ptg::run_tasks(h->spec, run, &tasks);
+  Transport T;
+  T.ntask = (int64_t)tasks.size();
+  T.np = run->np;
+  T.np_local = np_local_of(run->np, run->rank, run->nranks);
+  if (T.np_local > 2147483647LL) return PTG_ERR_INVALID;
+  T.rank = run->rank;
+  T.nranks = run->nranks;
+  T.seed = run->seed;
+  T.stream = run->stream;
+  T.precision = run->precision;
+  T.tasks = &tasks;
+  int st = run_transport(h, T);
+  if (st != PTG_OK) return st;
+  /* FP64 reduction on the device */
+  const int64_t nm = h->spec.nmode();
+  ptg::ModeConst mc;
+  ptg::mode_constants(h->spec, run, &mc);
+  std::vector<double> coef;
+  double dS = 0.0;
+  ptg::simpson_weights(run->nangle, h->geom.box[0], &coef, &dS);
+  const int nbins = run->nbins;
+  CU(h->red_coef.ensure(sizeof(double) * coef.size()));
+  CU(h->red_K.ensure(sizeof(double) * nm));
+  CU(h->red_W.ensure(sizeof(double) * nm));
+  CU(h->red_mfp.ensure(sizeof(double) * nm));
+  CU(h->red_bin.ensure(sizeof(int) * nm));
+  CU(h->red_grid.ensure(sizeof(double) * ns));
+  CU(h->red_tc.ensure(sizeof(double) * nm));
+  CU(h->red_kv.ensure(sizeof(double) * nm));
+  CU(h->red_bw.ensure(sizeof(double) * nm));
+  CU(h->red_bv.ensure(sizeof(double) * nm));
+  CU(h->red_emfp.ensure(sizeof(double) * nm));
+  CU(h->red_trans.ensure(sizeof(double) * nm * ns * run->nangle));
+  CU(h->red_result.ensure(sizeof(double) * (2 + 3 * (size_t)nbins)));
+  cudaStream_t s = h->stream;
+  CU(cudaMemcpyAsync(h->red_coef.p, coef.data(), sizeof(double) * coef.size(), cudaMemcpyHostToDevice, s));
+  CU(cudaMemcpyAsync(h->red_K.p, mc.K.data(), sizeof(double) * nm, cudaMemcpyHostToDevice, s));
+  CU(cudaMemcpyAsync(h->red_W.p, mc.W.data(), sizeof(double) * nm, cudaMemcpyHostToDevice, s));
+  CU(cudaMemcpyAsync(h->red_mfp.p, mc.mfp_m.data(), sizeof(double) * nm, cudaMemcpyHostToDevice, s));
+  CU(cudaMemcpyAsync(h->red_bin.p, mc.bin.data(), sizeof(int) * nm, cudaMemcpyHostToDevice, s));
+  if (run->kind_mfp == PTG_MFP_GRID)
+    CU(cudaMemcpyAsync(h->red_grid.p, run->mfp_grid_nm, sizeof(double) * ns, cudaMemcpyHostToDevice, s));
+  h->last.h2d_bytes += sizeof(double) * (coef.size() + 3 * (size_t)nm) + sizeof(int) * nm +
+                       (run->kind_mfp == PTG_MFP_GRID ? sizeof(double) * ns : 0);
+  ptg::ReduceIn in;
+  memset(&in, 0, sizeof(in));
+  in.counts = h->counts.as<const unsigned long long>();
+  in.nmode = nm;
+  in.nangle = run->nangle;
+  in.ns = ns;
+  in.kind_mfp = run->kind_mfp;
+  in.nbins = nbins;
+  in.np = (double)run->np;
+  in.dS = dS;
+  in.tnorm = 0.75 * h->geom.box[0];
+  in.coef = h->red_coef.as<const double>();
+  in.K = h->red_K.as<const double>();
+  in.W = h->red_W.as<const double>();
+  in.mfp_m = h->red_mfp.as<const double>();
+  in.bin = h->red_bin.as<const int>();
+  in.grid = h->red_grid.as<const double>();
+  in.tc = h->red_tc.as<double>();
+  in.kv = h->red_kv.as<double>();
+  in.bw = h->red_bw.as<double>();
+  in.bv = h->red_bv.as<double>();
+  in.emfp_nm = h->red_emfp.as<double>();
+  in.transmit = h->red_trans.as<double>();
+  in.result = h->red_result.as<double>();
+  CU(cudaEventRecord(h->ev[2], s));
+  CU(ptg::launch_kappa_reduce(in, s));
+  CU(cudaEventRecord(h->ev[3], s));
+  std::vector<double> res(2 + 3 * (size_t)nbins);
+  CU(cudaMemcpyAsync(res.data(), h->red_result.p, sizeof(double) * res.size(), cudaMemcpyDeviceToHost, s));
+  if (out->emfp_nm)
+    CU(cudaMemcpyAsync(out->emfp_nm, h->red_emfp.p, sizeof(double) * nm, cudaMemcpyDeviceToHost, s));
+  if (out->transmit)
+    CU(cudaMemcpyAsync(out->transmit, h->red_trans.p, sizeof(double) * nm * ns * run->nangle,
+                       cudaMemcpyDeviceToHost, s));
+  if (out->counts)
+    CU(cudaMemcpyAsync(out->counts, h->counts.p, sizeof(unsigned long long) * T.ntask,
+                       cudaMemcpyDeviceToHost, s));
+  h->last.d2h_bytes += sizeof(double) * res.size() + (out->emfp_nm ? sizeof(double) * nm : 0) +
+                       (out->transmit ? sizeof(double) * nm * ns * run->nangle : 0) +
+                       (out->counts ? sizeof(unsigned long long) * T.ntask : 0);
+  st = finish_stats(h);
+  if (st != PTG_OK) return st;
+  float rms = 0.f;
+  CU(cudaEventElapsedTime(&rms, h->ev[2], h->ev[3]));
+  h->last.reduce_ms = rms;
+  h->last.launches += 2;
+  out->kappa = res[0];
+  out->kappa_stderr = sqrt(res[1]);
+  for (int b = 0; b < nbins; ++b) {
+    const double sw = res[2 + 3 * b], swt = res[3 + 3 * b], sv = res[4 + 3 * b];
+    if (out->bin_T) out->bin_T[b] = sw > 0 ? swt / sw : 0.0;
+    if (out->bin_T_stderr) out->bin_T_stderr[b] = sw > 0 ? sqrt(sv) / sw : 0.0;
+  }
+  out->flights = h->last.flights;
+  out->lost = h->last.lost;
+  out->samples = h->last.samples;
+  out->kernel_ms = h->last.kernel_ms;
+  return check_lost(h);
+}
+
+int ptg_kappa_from_counts(const ptg_geometry* geom, const ptg_spectrum* spec, const ptg_run* run,
+                          const uint64_t* counts, ptg_kappa_out* out) {
+  if (!geom || !spec || !run || !counts || !out) return PTG_ERR_INVALID;
+  ptg::SpecSoA S;
+  std::string why;
+  if (ptg::copy_spectrum(spec, &S, &why) != PTG_OK) return PTG_ERR_INVALID;
+  if (!ptg::run_valid(S, run, &why)) return PTG_ERR_INVALID;
+  const int ns = run->kind_mfp == PTG_MFP_GRID ? run->nmfp : 1;
+  const int na = run->nangle;
+  const int64_t nm = S.nmode();
+  ptg::ModeConst mc;
+  ptg::mode_constants(S, run, &mc);
+  std::vector<double> coef;
+  double dS = 0.0;
+  ptg::simpson_weights(na, geom->box[0], &coef, &dS);
+  const double tnorm = 0.75 * geom->box[0];
+  const double np = (double)run->np;
+  double kappa = 0.0, kvar = 0.0;
+  std::vector<double> sw(run->nbins, 0.0), swt(run->nbins, 0.0), sv(run->nbins, 0.0);
+  std::vector<double> Sv(ns), Vv(ns), dE(ns);
+  for (int64_t m = 0; m < nm; ++m) {
+    for (int s = 0; s < ns; ++s) {
+      double acc = 0.0, var = 0.0;
+      for (int ia = 0; ia < na - 1; ++ia) {
+        const int64_t task = m + nm * (s + (int64_t)ns * ia);
+        const double tr = (double)counts[task] / np;
+        acc += coef[ia] * tr;
+        var += coef[ia] * coef[ia] * (tr * (1.0 - tr) / np);
+        if (out->transmit) out->transmit[task] = tr;
+      }
+      if (out->transmit) out->transmit[m + nm * (s + (int64_t)ns * (na - 1))] = 0.0;
+      Sv[s] = acc * dS;
+      Vv[s] = var * dS * dS;
+      dE[s] = 0.0;
+    }
+    const double mf = mc.mfp_m[m];
+    double E;
+    if (run->kind_mfp == PTG_MFP_MATTHIESSEN) {
+      if (mf == 0.0) { E = Sv[0] * 1.0e-9; dE[0] = 1.0e-9; }
+      else {
+        const double sm = Sv[0] * 1.0e-9;
+        E = 1.0 / (1.0 / mf + 1.0 / sm);
+        dE[0] = (sm > 0.0) ? 1.0e-9 * (E * E) / (sm * sm) : 1.0e-9;
+      }
+    } else if (run->kind_mfp == PTG_MFP_PER_MODE) {
+      E = Sv[0] * 1.0e-9;
+      dE[0] = 1.0e-9;
+    } else {
+      const double* g = run->mfp_grid_nm;
+      if (mf < g[0] * 1.0e-9) {
+        E = Sv[0] * 1.0e-9 * mf / (g[0] * 1.0e-9);
+        dE[0] = 1.0e-9 * mf / (g[0] * 1.0e-9);
+      } else if (mf > g[ns - 1] * 1.0e-9) {
+        E = Sv[ns - 1] * 1.0e-9;
+        dE[ns - 1] = 1.0e-9;
+      } else {
+        E = Sv[ns - 1] * 1.0e-9;
+        dE[ns - 1] = 1.0e-9;
+        for (int s = 0; s < ns - 1; ++s) {
+          if (g[s] * 1.0e-9 <= mf && mf < g[s + 1] * 1.0e-9) {
+            const double ip = (mf - g[s] * 1.0e-9) / ((g[s + 1] - g[s]) * 1.0e-9);
+            E = Sv[s] * 1.0e-9 * (1.0 - ip) + Sv[s + 1] * 1.0e-9 * ip;
+            dE[ns - 1] = 0.0;
+            dE[s] = 1.0e-9 * (1.0 - ip);
+            dE[s + 1] = 1.0e-9 * ip;
+            break;
+          }
+        }
+      }
+    }
+    kappa += mc.K[m] * E;
+    for (int s = 0; s < ns; ++s) {
+      const double gk = mc.K[m] * dE[s];
+      kvar += gk * gk * Vv[s];
+    }
+    if (out->emfp_nm) out->emfp_nm[m] = E * 1.0e9;
+    if (run->nbins > 0 && mc.bin[m] >= 0) {
+      double tm, vm = 0.0;
+      if (run->kind_mfp == PTG_MFP_MATTHIESSEN) {
+        tm = Sv[0] / tnorm;
+        vm = Vv[0] / (tnorm * tnorm);
+      } else {
+        tm = E * 1.0e9 / tnorm;
+        for (int s = 0; s < ns; ++s) {
+          const double gk = dE[s] * 1.0e9 / tnorm;
+          vm += gk * gk * Vv[s];
+        }
+      }
+      const int b = mc.bin[m];
+      sw[b] += mc.W[m];
+      swt[b] += mc.W[m] * tm;
+      sv[b] += mc.W[m] * mc.W[m] * vm;
+    }
+  }
+  out->kappa = kappa;
+  out->kappa_stderr = sqrt(kvar);
+  for (int b = 0; b < run->nbins; ++b) {
+    if (out->bin_T) out->bin_T[b] = sw[b] > 0 ? swt[b] / sw[b] : 0.0;
+    if (out->bin_T_stderr) out->bin_T_stderr[b] = sw[b] > 0 ? sqrt(sv[b]) / sw[b] : 0.0;
+  }
+  return PTG_OK;
+}
+
+int ptg_last_stats(const ptg_handle* h, ptg_stats* st) {
+  if (!h || !st) return PTG_ERR_INVALID;
+  *st = h->last;
+  return PTG_OK;
+}
+
+int ptg_replay_task(ptg_handle* h, const ptg_run* run, int64_t task, int32_t* end_side,
+                    uint32_t* flights, double* final_pos) {
+  if (!h || !run || !end_side || !flights || !final_pos) return PTG_ERR_INVALID;
+  std::string why;
+  if (!ptg::run_valid(h->spec, run, &why)) return PTG_ERR_INVALID;
+  std::vector<ptg::TaskHost> tasks;
+  ptg::run_tasks(h->spec, run, &tasks);
+  if (task < 0 || task >= (int64_t)tasks.size()) return PTG_ERR_INVALID;
+  const int64_t npl = np_local_of(run->np, run->rank, run->nranks);
+  CU(cudaSetDevice(h->device));
+  const int64_t ntask = (int64_t)tasks.size();
+  std::vector<ptg::Task64> t64(ntask);
+  for (int64_t i = 0; i < ntask; ++i) t64[i] = {tasks[i].lambda, tasks[i].cth, tasks[i].sth, tasks[i].omega};
+  DevBuf dt, de, df, dp, dc, dl, ds;
+  int st = PTG_OK;
+  do {
+    if (dt.ensure(sizeof(ptg::Task64) * ntask) || de.ensure(sizeof(int) * npl) ||
+        df.ensure(sizeof(unsigned) * npl) || dp.ensure(sizeof(double) * 3 * npl) ||
+        dc.ensure(sizeof(unsigned long long) * ntask) || dl.ensure(sizeof(unsigned long long) * ntask) ||
+        ds.ensure(sizeof(unsigned long long) * 4)) { st = PTG_ERR_CUDA; break; }
+    cudaMemcpy(dt.p, t64.data(), sizeof(ptg::Task64) * ntask, cudaMemcpyHostToDevice);
+    cudaMemset(dc.p, 0, sizeof(unsigned long long) * ntask);
+    cudaMemset(dl.p, 0, sizeof(unsigned long long) * ntask);
+    cudaMemset(ds.p, 0, sizeof(unsigned long long) * 4);
+    ptg::Run64 r;
+    memset(&r, 0, sizeof(r));
+    r.task = dt.as<const ptg::Task64>();
+    r.ntask = ntask;
+    r.np = run->np;
+    r.np_local = npl;
+    r.rank = run->rank;
+    r.nranks = run->nranks;
+    r.k0 = (uint32_t)run->seed;
+    r.k1 = (uint32_t)(run->seed >> 32);
+    r.c1 = ((uint32_t)run->stream) << 8;
+    r.max_flights = h->opt.max_flights > 0 ? h->opt.max_flights : 2147483647LL;
+    r.ref_quirks = h->opt.ref_quirks;
+    r.counts = dc.as<unsigned long long>();
+    r.lost = dl.as<unsigned long long>();
+    r.stats = ds.as<unsigned long long>();
+    r.replay_task = task;
+    r.end_side = de.as<int>();
+    r.flights = df.as<unsigned>();
+    r.final_pos = dp.as<double>();
+    if (ptg::launch_plain_fp64(h->g64, r, h->stream, nullptr, nullptr) != cudaSuccess ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess) { st = PTG_ERR_CUDA; break; }
+    cudaMemcpy(end_side, de.p, sizeof(int) * npl, cudaMemcpyDeviceToHost);
+    cudaMemcpy(flights, df.p, sizeof(unsigned) * npl, cudaMemcpyDeviceToHost);
+    if (cudaMemcpy(final_pos, dp.p, sizeof(double) * 3 * npl, cudaMemcpyDeviceToHost) != cudaSuccess)
+      st = PTG_ERR_CUDA;
+  } while (0);
+  DevBuf* all[] = {&dt, &de, &df, &dp, &dc, &dl, &ds};
+  for (DevBuf* b : all) b->release();
+  return st;
+}
+
+}  // extern "C"

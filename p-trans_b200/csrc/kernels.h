@@ -1,0 +1,150 @@
+/*
+ * kernels.h - device data layouts and host-callable launchers of the
+ * transport and reduction kernels.
+ */
+#ifndef PTG_KERNELS_H
+#define PTG_KERNELS_H
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ptg {
+
+/* ---------------- plain FP64 kernel ------------------------------------- */
+
+/* Built geometry in device memory, FP64 structure of arrays (the
+   ptg_geometry fields the transport reads). */
+struct Geo64 {
+  const double* vertex;      /* closed polygons, 3 per vertex        */
+  const double* normal;      /* 3 per surface                        */
+  const double* tangent;     /* 9 per surface, column-major          */
+  const double* center;      /* 3 per surface                        */
+  const double* radius;
+  const double* spec;
+  const double* tparam;
+  const int* shape;
+  const int* nvertex;
+  const int* vbegin;
+  const int* kind_trans;
+  const int* gout;
+  const int* internal;
+  const int* incident;
+  const int* grain_begin;
+  const int* grain_incident;
+  const double* grain_gen;   /* 3 per grain                          */
+  double box[3];
+  double scope[2];
+  int face_kind[6];
+  int kind_grain, ngrain, igrain_fill, nmaterial;
+  double max_omega;
+};
+
+/* Per task: lambda [nm] (1e10 ballistic, <= 0 skipped), cos/sin of the
+   incident angle, mode omega. */
+struct Task64 {
+  double lambda, cth, sth, omega;
+};
+
+struct Run64 {
+  const Task64* task;
+  int64_t ntask;
+  int64_t np;                 /* particles per task (all ranks)          */
+  int64_t np_local;           /* particles of this rank per task         */
+  int32_t rank, nranks;
+  uint32_t k0, k1, c1;        /* Philox key and stream word              */
+  int64_t max_flights;
+  int32_t ref_quirks;
+  unsigned long long* counts; /* [ntask]                                 */
+  unsigned long long* lost;   /* [ntask]                                 */
+  unsigned long long* stats;  /* flights, lost, capped, samples          */
+  /* replay of one task (replay_task >= 0) */
+  int64_t replay_task;
+  int* end_side;
+  unsigned* flights;
+  double* final_pos;
+};
+
+cudaError_t launch_plain_fp64(const Geo64& g, const Run64& r, cudaStream_t st, int* grid,
+                              int* block);
+
+/* ---------------- persistent FP32 kernel -------------------------------- */
+
+/* Surface record types in the FP32 blob. */
+enum { REC_POLY = 1, REC_SPHERE = 2, REC_CYL = 3 };
+enum { REC_INTERIOR = 1 << 8 };
+
+/* Offsets (in 16-byte units) of the sections of the FP32 geometry blob. */
+struct BlobLayout {
+  int hot;          /* float4[2*nsurf]: A = shape data, B = int4 (type, e0, ne, geom) */
+  int cold;         /* float4[3*nsurf]: (t1,spec) (t2,tparam) (n, kind|gout<<8)      */
+  int edge;         /* float4[nedge]  : in-plane inward edge normal m, m.v           */
+  int cand_begin;   /* int[ngrain_total+1]                                           */
+  int cand;         /* int[ncand]                                                    */
+  int start;        /* voronoi: float4 (generatrix, grain); bricks: int2 (surf, grain) */
+  int total;        /* blob size in 16-byte units                                    */
+  int nstart;
+};
+
+struct GeoF32 {
+  const float4* blob;  /* device blob (global memory)                    */
+  BlobLayout lay;
+  float box[3];
+  float scope[2];
+  float eps;           /* absolute geometric tolerance [nm]              */
+  int periodic_mask;   /* bit f set: box face f is periodic              */
+  int kind_grain, igrain_fill, nmaterial;
+  int stage_smem;      /* 1: copy the blob to shared memory (bulk copy)  */
+};
+
+/* Per task (FP32): lambda (inf = ballistic, <= 0 skipped), cos, sin, omega/max_omega */
+struct RunF32 {
+  const float4* task;
+  const int4* chunk;          /* (task, first local particle, count, 0) in LPT order */
+  int32_t nchunk;
+  int64_t np;
+  int32_t rank, nranks;
+  uint32_t k0, k1, c1;
+  uint32_t max_flights;
+  int32_t ref_quirks;
+  int32_t regen_threshold;
+  unsigned long long* counts;
+  unsigned long long* lost;
+  unsigned long long* stats;  /* flights, lost, capped, samples */
+  int* queue;                 /* [0] next chunk, [1] error flags */
+};
+
+cudaError_t launch_persistent_fp32(const GeoF32& g, const RunF32& r, int grid, int block,
+                                   size_t smem, cudaStream_t st);
+/* Residency of the persistent kernel for a block size and shared memory. */
+cudaError_t persistent_occupancy(int block, size_t smem, int* blocks_per_sm);
+
+/* ---------------- FP64 kappa reduction ---------------------------------- */
+
+struct ReduceIn {
+  const unsigned long long* counts;  /* [ntask]                          */
+  int64_t nmode;
+  int32_t nangle, ns, kind_mfp, nbins;
+  double np;                         /* particles per task                */
+  double dS;                         /* Simpson step * 1.5 * Lx           */
+  double tnorm;                      /* 0.75 * Lx                         */
+  const double* coef;                /* [nangle] Simpson c_a sin cos      */
+  const double* K;                   /* [nmode]                           */
+  const double* W;                   /* [nmode]                           */
+  const double* mfp_m;               /* [nmode] bulk MFP [m]              */
+  const int* bin;                    /* [nmode]                           */
+  const double* grid;                /* [ns] (GRID)                       */
+  /* scratch and outputs */
+  double* tc;                        /* [nmode] kappa per mode            */
+  double* kv;                        /* [nmode] kappa variance per mode   */
+  double* bw;                        /* [nmode] W * <T>                   */
+  double* bv;                        /* [nmode] W^2 var<T>                */
+  double* emfp_nm;                   /* [nmode]                           */
+  double* transmit;                  /* [nmode*ns*nangle] or null         */
+  double* result;                    /* [2 + 3*nbins]: kappa, var, (sumW, sumWT, sumW2V) per bin */
+};
+
+cudaError_t launch_kappa_reduce(const ReduceIn& in, cudaStream_t st);
+
+}  // namespace ptg
+
+#endif

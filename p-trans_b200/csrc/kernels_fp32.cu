@@ -1,0 +1,467 @@
+/*
+ * kernels_fp32.cu - persistent FP32 transport kernel.
+ *
+ * Same physics and random-number counters as the reference's calcTransmit
+ * (src/RTMCphon.f90:1608-2414), restructured for the GPU:
+ *   - one resident grid; every warp pulls work chunks (task, particle range)
+ *     from an atomic queue ordered longest-expected-trajectory first, and a
+ *     lane whose phonon has left the box is refilled at once from the warp's
+ *     chunk (ballot + popc ranking), so warps stay full while trajectory
+ *     lengths differ by orders of magnitude;
+ *   - phonon state lives in registers for the whole trajectory;
+ *   - geometry (surface records, polygon edge planes, per-grain candidate
+ *     lists) is one blob copied into shared memory by a bulk asynchronous copy
+ *     when it fits, else read through the read-only path;
+ *   - the box grain is an axis-aligned slab test (its six faces are the
+ *     reference's box quads, src/RTMCphon.f90:1253-1332);
+ *   - intersection is FP32 with an absolute tolerance eps: planes accept
+ *     t >= -eps and edge planes accept points within eps, so neighbouring
+ *     facets overlap and no ray leaks through a shared edge; quadrics use the
+ *     stable quadratic roots, the far root from the inside, and exclude the
+ *     surface just left from the outside, which replaces the reference's
+ *     absolute 1e-7 nm nudge (src/RTMCphon.f90:1779);
+ *   - one Philox4x32-10 block per free flight supplies the four uniforms of
+ *     any event; tallies are integer, aggregated per warp by task
+ *     (match_any) before one atomic.
+ */
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "kernels.h"
+#include "philox.cuh"
+
+namespace ptg {
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int kBlock = 256;
+
+struct Geo {
+  const float4* base;   /* blob in shared or global memory */
+  BlobLayout lay;
+  __device__ __forceinline__ float4 hotA(int s) const { return base[lay.hot + 2 * s]; }
+  __device__ __forceinline__ int4 hotB(int s) const {
+    const float4 v = base[lay.hot + 2 * s + 1];
+    return make_int4(__float_as_int(v.x), __float_as_int(v.y), __float_as_int(v.z),
+                     __float_as_int(v.w));
+  }
+  __device__ __forceinline__ float4 cold(int s, int i) const { return base[lay.cold + 3 * s + i]; }
+  __device__ __forceinline__ float4 edge(int e) const { return base[lay.edge + e]; }
+  __device__ __forceinline__ int cand_begin(int g) const {
+    return reinterpret_cast<const int*>(base + lay.cand_begin)[g];
+  }
+  __device__ __forceinline__ int cand(int k) const {
+    return reinterpret_cast<const int*>(base + lay.cand)[k];
+  }
+  __device__ __forceinline__ float4 start(int i) const { return base[lay.start + i]; }
+};
+
+__device__ __forceinline__ bool inside_edges(const Geo& G, int e0, int ne, float x, float y,
+                                             float z, float eps) {
+  for (int e = 0; e < ne; ++e) {
+    const float4 m = G.edge(e0 + e);
+    if (fmaf(m.x, x, fmaf(m.y, y, m.z * z)) < m.w - eps) return false;
+  }
+  return true;
+}
+
+/* Nearest surface among the candidates of a grain (not the box). */
+__device__ __forceinline__ void scan_grain(const Geo& G, int grain, float px, float py, float pz,
+                                           float dx, float dy, float dz, int last_geom, float eps,
+                                           float zmax, float& tb, int& sb) {
+  const int kb = G.cand_begin(grain), ke = G.cand_begin(grain + 1);
+  for (int k = kb; k < ke; ++k) {
+    const int s = G.cand(k);
+    const float4 A = G.hotA(s);
+    const int4 B = G.hotB(s);
+    const int type = B.x & 0xff;
+    if (type == REC_POLY) {
+      const float cosa = fmaf(A.x, dx, fmaf(A.y, dy, A.z * dz));
+      if (cosa <= 0.0f) continue;
+      const float t = __fdividef(A.w - fmaf(A.x, px, fmaf(A.y, py, A.z * pz)), cosa);
+      if (!(t >= -eps) || !(t < tb)) continue;
+      const float hx = fmaf(t, dx, px), hy = fmaf(t, dy, py), hz = fmaf(t, dz, pz);
+      if (!inside_edges(G, B.y, B.z, hx, hy, hz, eps)) continue;
+      tb = fmaxf(t, 0.0f);
+      sb = s;
+    } else {
+      const bool interior = (B.x & REC_INTERIOR) != 0;
+      if (!interior && B.w == last_geom) continue;
+      float wx = A.x - px, wy = A.y - py, wz, a, b, c, r;
+      if (type == REC_SPHERE) {
+        wz = A.z - pz;
+        r = A.w;
+        a = 1.0f;
+        b = fmaf(wx, dx, fmaf(wy, dy, wz * dz));
+        c = fmaf(wx, wx, fmaf(wy, wy, wz * wz)) - r * r;
+      } else {
+        r = A.z;
+        a = fmaf(dx, dx, dy * dy);
+        if (!(a > 0.0f)) continue;
+        b = fmaf(wx, dx, wy * dy);
+        c = fmaf(wx, wx, wy * wy) - r * r;
+      }
+      /* roots of a t^2 - 2 b t + c = 0 */
+      const float disc = fmaf(b, b, -a * c);
+      if (!(disc >= 0.0f)) continue;
+      const float sq = sqrtf(disc);
+      float t;
+      if (interior) {
+        /* far root (b + sq)/a, written without cancellation */
+        t = (b >= 0.0f) ? __fdividef(b + sq, a) : __fdividef(-c, sq - b);
+      } else {
+        /* near root (b - sq)/a = c / (b + sq), valid when approaching */
+        if (!(b > 0.0f)) continue;
+        t = __fdividef(c, b + sq);
+        if (!(t >= -eps)) continue;
+      }
+      if (!(t < tb)) continue;
+      if (type == REC_CYL) {
+        const float hz = fmaf(t, dz, pz);
+        if (hz < 0.0f || hz > zmax) continue;
+      }
+      tb = fmaxf(t, 0.0f);
+      sb = s;
+    }
+  }
+}
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+__device__ __forceinline__ void warp_add_by_task(bool pred, int task, unsigned long long* arr) {
+  const unsigned m = __ballot_sync(FULL, pred);
+  if (pred) {
+    const unsigned peers = __match_any_sync(m, task);
+    if ((threadIdx.x & 31) == __ffs(peers) - 1)
+      atomicAdd(arr + task, (unsigned long long)__popc(peers));
+  }
+}
+
+/* Copies the geometry blob into shared memory with one bulk asynchronous
+   copy completed on an mbarrier.  The wait is bounded; on timeout the block
+   records an error and falls back to the global copy. */
+__device__ bool stage_blob(const float4* gblob, float4* sblob, int units, int* err) {
+  __shared__ alignas(8) unsigned long long bar;
+  const unsigned bar_a = (unsigned)__cvta_generic_to_shared(&bar);
+  const unsigned dst_a = (unsigned)__cvta_generic_to_shared(sblob);
+  const unsigned bytes = (unsigned)units * 16u;
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            dst_a),
+        "l"(gblob), "r"(bytes), "r"(bar_a)
+        : "memory");
+  }
+  unsigned done = 0;
+  for (int it = 0; it < (1 << 20) && !done; ++it) {
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(bar_a)
+        : "memory");
+  }
+  const int ok = __syncthreads_and((int)done);
+  if (!ok && threadIdx.x == 0) atomicOr(err, 1);
+  return ok != 0;
+}
+
+__global__ void __launch_bounds__(kBlock, 4) k_persistent(GeoF32 gp, RunF32 r) {
+  extern __shared__ float4 sblob[];
+  Geo G;
+  G.lay = gp.lay;
+  G.base = gp.blob;
+  if (gp.stage_smem) {
+    if (stage_blob(gp.blob, sblob, gp.lay.total, r.queue + 1)) G.base = sblob;
+  }
+  const int lane = threadIdx.x & 31;
+  const float X = gp.box[0], Y = gp.box[1], Z = gp.box[2];
+  const float eps = gp.eps;
+  const Key2 key = {r.k0, r.k1};
+
+  /* warp-uniform chunk cursor */
+  int ch_task = -1, ch_next = 0, ch_left = 0;
+  bool queue_done = false;
+
+  /* lane state */
+  bool alive = false;
+  float px = 0, py = 0, pz = 0, dx = 1, dy = 0, dz = 0, fp = 0, lam = 0, omr = 0;
+  int grain = 0, last_geom = -1, task = 0;
+  uint32_t slo = 0, shi = 0, flight = 0;
+  unsigned long long my_flights = 0, my_samples = 0, my_capped = 0, my_lost = 0;
+
+  while (true) {
+    /* ---- refill idle lanes from the warp's chunk ---------------------- */
+    unsigned idle = __ballot_sync(FULL, !alive);
+    if (!queue_done && idle &&
+        (__popc(idle) >= r.regen_threshold || idle == FULL)) {
+      while (idle && !queue_done) {
+        if (ch_left == 0) {
+          int c = 0;
+          if (lane == 0) c = atomicAdd(r.queue, 1);
+          c = __shfl_sync(FULL, c, 0);
+          if (c >= r.nchunk) { queue_done = true; break; }
+          const int4 q = r.chunk[c];
+          ch_task = q.x; ch_next = q.y; ch_left = q.z;
+        }
+        const int take = min(__popc(idle), ch_left);
+        const int rank = __popc(idle & lanemask_lt());
+        if (((idle >> lane) & 1u) && rank < take) {
+          const int64_t p = (int64_t)r.rank + (int64_t)(ch_next + rank) * r.nranks;
+          const uint64_t sample = (uint64_t)ch_task * (uint64_t)r.np + (uint64_t)p;
+          task = ch_task;
+          slo = (uint32_t)sample;
+          shi = (uint32_t)(sample >> 32);
+          const float4 T = r.task[task];
+          lam = T.x;
+          omr = T.w;
+          /* emission: createRandomPosition / createRandomDirectionPhi,
+             src/RTMCphon.f90:1845-1871; flight 0 draws y, z, phi, free path */
+          const uint4 R0 = philox10(0u, r.c1, slo, shi, key);
+          px = 0.0f;
+          py = u23f(R0.x) * Y * gp.scope[0];
+          pz = u23f(R0.y) * Z * gp.scope[1];
+          float sp, cp;
+          sincospif(2.0f * u23f(R0.z), &sp, &cp);
+          dx = T.y;
+          dy = T.z * cp;
+          dz = T.z * sp;
+          fp = isinf(lam) ? lam : -lam * __logf(u23f(R0.w));
+          /* start grain: nearest incident generatrix (voronoi,
+             src/RTMCphon.f90:2100-2118) or the last incident polygon
+             containing the point, else the fill grain (bricks, :2131-2163) */
+          grain = 0;
+          if (gp.kind_grain == 1) {
+            float dmin = 3.0e38f;
+            for (int i = 0; i < gp.lay.nstart; ++i) {
+              const float4 s = G.start(i);
+              const float a = px - s.x, b = py - s.y, c = pz - s.z;
+              const float d2 = fmaf(a, a, fmaf(b, b, c * c));
+              if (d2 < dmin) { dmin = d2; grain = __float_as_int(s.w); }
+            }
+          } else {
+            grain = gp.igrain_fill;
+            for (int i = 0; i < gp.lay.nstart; ++i) {
+              const float4 s = G.start(i);
+              const int sid = __float_as_int(s.x);
+              const int4 B = G.hotB(sid);
+              if (inside_edges(G, B.y, B.z, px, py, pz, 0.0f)) grain = __float_as_int(s.y);
+            }
+          }
+          last_geom = -1;
+          flight = 0;
+          alive = true;
+          my_samples += 1;
+        }
+        ch_next += take;
+        ch_left -= take;
+        idle = __ballot_sync(FULL, !alive);
+      }
+    }
+    if (!__any_sync(FULL, alive)) {
+      if (queue_done) break;
+      continue;
+    }
+
+    /* ---- one free flight ------------------------------------------------ */
+    int end_side = -1;  /* -1 still running, 0 lost, 1 x-, 2 x+ */
+    if (alive) {
+      if (!(px >= -eps && px <= X + eps && py >= -eps && py <= Y + eps && pz >= -eps &&
+            pz <= Z + eps)) {
+        end_side = 0;
+      } else if (flight >= r.max_flights) {
+        end_side = 0;
+        my_capped += 1;
+      } else {
+        ++flight;
+        const uint4 R = philox10(flight, r.c1, slo, shi, key);
+        /* slab exit of the box grain */
+        float tb = 3.0e38f;
+        int sb = -1;
+        if (dx > 0.0f) { tb = __fdividef(X - px, dx); sb = 1; }
+        else if (dx < 0.0f) { tb = __fdividef(-px, dx); sb = 0; }
+        if (dy != 0.0f) {
+          const float t = __fdividef((dy > 0.0f ? Y : 0.0f) - py, dy);
+          if (t < tb) { tb = t; sb = dy > 0.0f ? 3 : 2; }
+        }
+        if (dz != 0.0f) {
+          const float t = __fdividef((dz > 0.0f ? Z : 0.0f) - pz, dz);
+          if (t < tb) { tb = t; sb = dz > 0.0f ? 5 : 4; }
+        }
+        tb = fmaxf(tb, 0.0f);
+        if (grain > 0) scan_grain(G, grain, px, py, pz, dx, dy, dz, last_geom, eps, Z, tb, sb);
+
+        const float u0 = u23f(R.x), u1 = u23f(R.y), u2 = u23f(R.z), u3 = u23f(R.w);
+        if (fp < tb) {
+          /* intrinsic scattering: isotropic direction, new free path */
+          px = fmaf(fp, dx, px);
+          py = fmaf(fp, dy, py);
+          pz = fmaf(fp, dz, pz);
+          const float ct = fmaf(u0, 2.0f, -1.0f);
+          const float st = sqrtf(fmaxf(0.0f, fmaf(-ct, ct, 1.0f)));
+          float sp, cp;
+          sincospif(2.0f * u1, &sp, &cp);
+          dx = ct;
+          dy = st * cp;
+          dz = st * sp;
+          fp = -lam * __logf(u2);
+          last_geom = -1;
+        } else {
+          px = fmaf(tb, dx, px);
+          py = fmaf(tb, dy, py);
+          pz = fmaf(tb, dz, pz);
+          fp -= tb;
+          if (sb == 0) {
+            end_side = 1;
+          } else if (sb == 1) {
+            end_side = 2;
+          } else if (sb < 6 && ((gp.periodic_mask >> sb) & 1)) {
+            const int ax = sb >> 1;
+            const float L = ax == 1 ? Y : Z;
+            const float sg = (sb & 1) ? -L : L;
+            if (ax == 1) py += sg; else pz += sg;
+            last_geom = -1;
+          } else {
+            /* surface event: determinSpecular, reflectSpecular /
+               reflectDiffusive, determinTransmit (src/RTMCphon.f90:2225-2413) */
+            const float4 C0 = G.cold(sb, 0), C1 = G.cold(sb, 1), C2 = G.cold(sb, 2);
+            const int meta = __float_as_int(C2.w);
+            const int kind = meta & 0xff;
+            float thr = 0.0f;
+            if (kind == 1) {
+              thr = C1.w;
+            } else if (kind == 2 || kind == 3) {
+              if (gp.nmaterial == 1) {
+                thr = __frcp_rn(fmaf(C1.w, omr, 1.0f));
+              } else {
+                const uint4 R2 = philox10(flight, r.c1 | 1u, slo, shi, key);
+                const float t11 = __frcp_rn(C1.w + 1.0f);
+                thr = fmaf(u23f(R2.x), 1.0f - t11, t11);
+              }
+            }
+            /* surface normal at the hit point and surface frame */
+            float nx, ny, nz, ax1, ay1, az1, ax2, ay2, az2;
+            const int4 B = G.hotB(sb);
+            const int type = B.x & 0xff;
+            if (type == REC_POLY) {
+              nx = C2.x; ny = C2.y; nz = C2.z;
+              ax1 = C0.x; ay1 = C0.y; az1 = C0.z;
+              ax2 = C1.x; ay2 = C1.y; az2 = C1.z;
+            } else {
+              const float4 A = G.hotA(sb);
+              float rx = px - A.x, ry = py - A.y, rz = (type == REC_SPHERE) ? pz - A.z : 0.0f;
+              const float inv = rsqrtf(fmaf(rx, rx, fmaf(ry, ry, rz * rz)));
+              nx = rx * inv; ny = ry * inv; nz = rz * inv;
+              const float q2 = fmaf(nx, nx, ny * ny);
+              if (q2 > 1.0e-12f) {
+                const float q = rsqrtf(q2);
+                ax2 = -ny * q; ay2 = nx * q; az2 = 0.0f;
+              } else {
+                ax2 = 0.0f; ay2 = 1.0f; az2 = 0.0f;
+              }
+              /* t1 = t2 x n */
+              ax1 = ay2 * nz - az2 * ny;
+              ay1 = az2 * nx - ax2 * nz;
+              az1 = ax2 * ny - ay2 * nx;
+              if (q2 <= 1.0e-12f) { ax1 = 1.0f; ay1 = 0.0f; az1 = 0.0f; }
+            }
+            /* tmpNormal oriented along the incoming direction */
+            const float dn0 = fmaf(nx, dx, fmaf(ny, dy, nz * dz));
+            const float on = dn0 < 0.0f ? -1.0f : 1.0f;
+            bool transmitted = false;
+            if (u0 <= C0.w) {
+              if (u1 <= thr) {
+                transmitted = true;
+              } else {
+                const float k2 = 2.0f * dn0;
+                dx = fmaf(-k2, nx, dx);
+                dy = fmaf(-k2, ny, dy);
+                dz = fmaf(-k2, nz, dz);
+                const float inv = rsqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+                dx *= inv; dy *= inv; dz *= inv;
+              }
+            } else {
+              const float sint = sqrtf(u1);
+              const float cost = sqrtf(fmaxf(0.0f, 1.0f - u1));
+              float sp, cp;
+              sincospif(2.0f * u2, &sp, &cp);
+              const float a = sint * cp, b = sint * sp;
+              float vx = fmaf(ax1, a, fmaf(ax2, b, nx * cost));
+              float vy = fmaf(ay1, a, fmaf(ay2, b, ny * cost));
+              float vz = fmaf(az1, a, fmaf(az2, b, nz * cost));
+              /* Lambertian into the incidence side, then optionally through */
+              const float s = on * fmaf(vx, nx, fmaf(vy, ny, vz * nz));
+              float sg = s > 0.0f ? -1.0f : 1.0f;
+              if (u3 <= thr) { sg = -sg; transmitted = true; }
+              dx = sg * vx; dy = sg * vy; dz = sg * vz;
+            }
+            if (transmitted) grain = meta >> 8;
+            last_geom = B.w;
+          }
+          if (end_side < 0 && fp < 1.0e-10f) {
+            const uint4 R2 = philox10(flight, r.c1 | 1u, slo, shi, key);
+            fp = -lam * __logf(u23f(R2.y));
+          }
+        }
+      }
+    }
+    /* ---- tallies ------------------------------------------------------- */
+    const bool fin = alive && end_side >= 0;
+    const bool trans = fin && (end_side == 2 || (end_side == 0 && r.ref_quirks));
+    const bool lostp = fin && end_side == 0;
+    warp_add_by_task(trans, task, r.counts);
+    warp_add_by_task(lostp, task, r.lost);
+    if (fin) {
+      my_flights += flight;
+      my_lost += lostp ? 1 : 0;
+      alive = false;
+    }
+  }
+  /* block-wide totals */
+  unsigned long long v0 = my_flights, v1 = my_lost, v2 = my_capped, v3 = my_samples;
+  for (int o = 16; o > 0; o >>= 1) {
+    v0 += __shfl_xor_sync(FULL, v0, o);
+    v1 += __shfl_xor_sync(FULL, v1, o);
+    v2 += __shfl_xor_sync(FULL, v2, o);
+    v3 += __shfl_xor_sync(FULL, v3, o);
+  }
+  if (lane == 0) {
+    if (v0) atomicAdd(r.stats + 0, v0);
+    if (v1) atomicAdd(r.stats + 1, v1);
+    if (v2) atomicAdd(r.stats + 2, v2);
+    if (v3) atomicAdd(r.stats + 3, v3);
+  }
+}
+
+}  // namespace
+
+cudaError_t persistent_occupancy(int block, size_t smem, int* bps) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_persistent, block, smem);
+}
+
+cudaError_t launch_persistent_fp32(const GeoF32& g, const RunF32& r, int grid, int block,
+                                   size_t smem, cudaStream_t st) {
+  if (block != kBlock) return cudaErrorInvalidConfiguration;
+  if (smem > 48 * 1024) {
+    cudaError_t e =
+        cudaFuncSetAttribute(k_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  k_persistent<<<grid, block, smem, st>>>(g, r);
+  return cudaGetLastError();
+}
+
+}  // namespace ptg

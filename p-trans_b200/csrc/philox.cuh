@@ -1,0 +1,53 @@
+/*
+ * philox.cuh - counter-based Philox4x32-10 (Salmon, Moraes, Dror, Shaw,
+ * "Parallel random numbers: as easy as 1, 2, 3", SC'11) for the transport
+ * kernels.  Counter layout (include/ptrans_gpu.h):
+ *   c0 = flight_no, c1 = sub | stream << 8, c2 = lo32(sample), c3 = hi32(sample)
+ *   key = (lo32(seed), hi32(seed)).
+ */
+#ifndef PTG_PHILOX_CUH
+#define PTG_PHILOX_CUH
+
+#include <stdint.h>
+
+namespace ptg {
+
+struct Key2 {
+  uint32_t k0, k1;
+};
+
+__device__ __forceinline__ uint4 philox10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                          Key2 k) {
+  uint32_t k0 = k.k0, k1 = k.k1;
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint32_t lo0 = 0xD2511F53u * c0;
+    const uint32_t hi0 = __umulhi(0xD2511F53u, c0);
+    const uint32_t lo1 = 0xCD9E8D57u * c2;
+    const uint32_t hi1 = __umulhi(0xCD9E8D57u, c2);
+    const uint32_t n0 = hi1 ^ c1 ^ k0;
+    const uint32_t n2 = hi0 ^ c3 ^ k1;
+    c0 = n0;
+    c1 = lo1;
+    c2 = n2;
+    c3 = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return make_uint4(c0, c1, c2, c3);
+}
+
+/* (k + 0.5) * 2^-52 from the top 52 bits of (a,b): open interval (0,1). */
+__device__ __forceinline__ double u52d(uint32_t a, uint32_t b) {
+  const uint64_t k = ((uint64_t)a << 20) | (uint64_t)(b >> 12);
+  return ((double)k + 0.5) * (1.0 / 4503599627370496.0);
+}
+
+/* (k + 0.5) * 2^-23 from the top 23 bits of a: open interval (0,1). */
+__device__ __forceinline__ float u23f(uint32_t a) {
+  return ((float)(a >> 9) + 0.5f) * (1.0f / 8388608.0f);
+}
+
+}  // namespace ptg
+
+#endif

@@ -1,0 +1,72 @@
+/*
+ * ptg_internal.h - host-side types shared by the C ABI implementation and the
+ * kernel launchers of the B200 RTMC phonon transport library.
+ */
+#ifndef PTG_INTERNAL_H
+#define PTG_INTERNAL_H
+
+#include <stdint.h>
+#include <string>
+#include <vector>
+
+#include "../../include/ptrans_gpu.h"
+
+namespace ptg {
+
+/* Owning, structure-of-arrays copy of a built geometry (ptg_geometry). */
+struct GeomSoA {
+  double box[3] = {0, 0, 0};
+  double scope[2] = {1, 1};
+  int32_t face_kind[6] = {0, 0, 0, 0, 0, 0};
+  int32_t kind_grain = PTG_GRAIN_VORONOI, ngrain = 0, igrain_fill = -1, nmaterial = 1;
+  std::vector<int32_t> grain_begin, grain_incident;
+  std::vector<double> grain_generatrix;
+  std::vector<int32_t> shape, nvertex, vertex_begin, kind_trans, grain_inside, grain_outside,
+      internal, incident, material1, material2;
+  std::vector<double> vertex, normal, tangent, center, radius, specularity, trans_param;
+  ptg_geometry view;  /* points into the vectors above */
+
+  int32_t nsurf() const { return (int32_t)shape.size(); }
+  int32_t ngrain_total() const { return (int32_t)grain_incident.size(); }
+  void make_view();
+};
+
+/* Copies a caller-provided ptg_geometry after validating it. */
+int copy_geometry(const ptg_geometry* g, GeomSoA* out, std::string* why);
+/* Builds from the raw model (src/RTMCphon.f90:894-1491). */
+int build_geometry(const ptg_model* m, GeomSoA* out, std::string* why);
+
+/* Spectrum copy with the derived per-mode quantities. */
+struct SpecSoA {
+  int32_t nb = 0, nk = 0;
+  double rtemp = 300, vol = 1, max_omega = 1;
+  std::vector<double> omega, tau, vel, mfp, weight;
+  int nmode() const { return nb * nk; }
+};
+int copy_spectrum(const ptg_spectrum* s, SpecSoA* out, std::string* why);
+
+/* Per-task description shared by the launchers. */
+struct TaskHost {
+  double lambda;  /* nm; 1e10 ballistic; <= 0 not simulated */
+  double cth, sth;
+  double omega;
+};
+
+/* Numbering helpers for ptg_run (include/ptrans_gpu.h). */
+int64_t run_ntask(const SpecSoA& s, const ptg_run* r);
+bool run_valid(const SpecSoA& s, const ptg_run* r, std::string* why);
+void run_tasks(const SpecSoA& s, const ptg_run* r, std::vector<TaskHost>* tasks);
+
+/* Host FP64 kappa assembly (effectiveMFP + fileoutput kappa sum). */
+struct ModeConst {
+  std::vector<double> K;      /* C*w*v/(3*vol*nqfbz): kappa per unit EMFP [m] */
+  std::vector<double> W;      /* C*w*v: flux weight of the per-bin averages    */
+  std::vector<double> mfp_m;  /* bulk MFP [m] after the tau rescale            */
+  std::vector<int32_t> bin;   /* frequency bin or -1                           */
+};
+void mode_constants(const SpecSoA& s, const ptg_run* r, ModeConst* mc);
+void simpson_weights(int nangle, double box_x, std::vector<double>* coef, double* dS);
+
+}  // namespace ptg
+
+#endif

@@ -1,0 +1,178 @@
+"""GPU parity of the CUDA path against the CPU FP64 oracle, through the C ABI.
+
+- The plain FP64 kernel replays the oracle bit for bit: same exit side, same
+  number of free flights and the same final position for every particle, and
+  identical transmitted counts per task (integer tallies: exact).
+- The persistent FP32 kernel draws the same kind of trajectories with FP32
+  geometry; its per-task and per-mode transmissions and kappa agree with the
+  oracle within the combined binomial confidence interval (|z| bounds written
+  in each test).
+- The device FP64 reduction gives the host assembly's kappa to 1e-12.
+"""
+import numpy as np
+import pytest
+
+from ptrans_b200 import abi as A
+from ptrans_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def geometries():
+    return {
+        "nanowire_diffuse": synth.nanowire(length=300.0, width=60.0, height=50.0, p_side=0.0),
+        "nanowire_mixed": synth.nanowire(length=300.0, width=60.0, height=50.0, p_side=0.6),
+        "film_periodic": synth.film_with_holes(lx=300.0, ly=300.0, lz=145.0, seed=2),
+        "film_mirror_transmit": synth.film_with_holes(seed=3, periodic_y=False, p_hole=0.3, t_hole=0.4, p_z=0.5),
+        "spheres": synth.spheres_in_box(l=200.0, centres=((70, 90, 100), (140, 110, 90)), radii=(35, 40),
+                                        t=0.5, p=0.3, p_wall=0.2),
+        "brick_quads": synth.brick_box(t=0.5, p=0.3, p_wall=0.1),
+        "brick_tris": synth.brick_box(t=0.7, p=0.0, p_wall=0.5, triangles=True),
+    }
+
+
+def setup(name, nmode=6, seed=1):
+    m = geometries()[name]
+    spec = synth.spectrum(nmode, seed=seed, mfp_lo=5e-9, mfp_hi=2e-6)
+    gb = A.GeomBuf(m)
+    return m, spec, gb
+
+
+@pytest.mark.parametrize("name", list(geometries()))
+def test_fp64_replay_is_bit_exact(orc, name):
+    m, spec, gb = setup(name)
+    o = orc.Oracle(model=m, spectrum=spec)
+    run = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=7, np_=64, seed=12345, stream=3,
+                     precision=A.PREC_FP64)
+    with A.Handle(gb.view, spec) as h:
+        for task in (0, 5, 13, 20, 35):
+            es_g, fl_g, fp_g = h.replay_task(run, task)
+            es_o, fl_o, fp_o = o.replay(run, task)
+            np.testing.assert_array_equal(es_g, es_o)
+            np.testing.assert_array_equal(fl_g, fl_o)
+            np.testing.assert_array_equal(fp_g, fp_o)
+
+
+@pytest.mark.parametrize("name", ["nanowire_diffuse", "film_periodic", "spheres", "brick_tris"])
+def test_fp64_counts_equal_oracle(orc, name):
+    m, spec, gb = setup(name, nmode=10)
+    o = orc.Oracle(model=m, spectrum=spec)
+    run = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=9, np_=200, seed=7, precision=A.PREC_FP64,
+                     nbins=4, bin_omega=(0.0, float(spec.omega.max())))
+    cnt_o, lost_o, res_o = o.counts(run)
+    ko = o.kappa(run, cnt_o)
+    with A.Handle(gb.view, spec) as h:
+        kg = h.kappa(run, want_counts=True, want_transmit=True)
+    np.testing.assert_array_equal(kg["counts"], cnt_o)
+    assert kg["flights"] == res_o["flights"]
+    assert kg["lost"] == res_o["lost"]
+    assert kg["kappa"] == pytest.approx(ko["kappa"], rel=1e-12)
+    np.testing.assert_allclose(kg["emfp_nm"], ko["emfp_nm"], rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(kg["bin_T"], ko["bin_T"], rtol=1e-12, atol=1e-15)
+    np.testing.assert_allclose(kg["transmit"], ko["transmit"], rtol=0, atol=0)
+
+
+def test_transmission_function_layout_and_ranks(orc):
+    """ptg_transmission fills transmit(nb,nk,nangle) with count/np per rank,
+    transmit(:,:,nangle) = 0; summing the ranks gives the single-rank result
+    (the reference's MPI_Allreduce, src/RTMCphon.f90:1584-1590)."""
+    m, spec, gb = setup("film_mirror_transmit", nmode=5)
+    o = orc.Oracle(model=m, spectrum=spec)
+    run = A.make_run(kind_mfp=A.MFP_GRID, nangle=7, np_=150, seed=99, mfp_grid=[40.0])
+    cnt_o, _, _ = o.counts(run)
+    with A.Handle(gb.view, spec) as h:
+        t1, e1 = h.transmission(40.0, 7, 150, seed=99, precision=A.PREC_FP64)
+        t_r0, _ = h.transmission(40.0, 7, 150, rank=0, nranks=2, seed=99, precision=A.PREC_FP64)
+        t_r1, _ = h.transmission(40.0, 7, 150, rank=1, nranks=2, seed=99, precision=A.PREC_FP64)
+    ref = (cnt_o / 150.0).reshape(6, 5)  # (angle, mode) with nbranch = 1
+    np.testing.assert_array_equal(t1[0, :, :6].T, ref)
+    assert np.all(t1[:, :, 6] == 0.0)
+    np.testing.assert_allclose(t_r0 + t_r1, t1, rtol=0, atol=1e-15)
+    np.testing.assert_allclose(e1, np.sqrt(t1 * (1 - t1) / 150.0))
+
+
+def _z(c1, c2, n):
+    p1, p2 = c1 / n, c2 / n
+    var = (p1 * (1 - p1) + p2 * (1 - p2)) / n
+    return (p1 - p2) / np.sqrt(np.maximum(var, 0.5 / n / n))
+
+
+@pytest.mark.parametrize("name", ["nanowire_diffuse", "film_periodic", "film_mirror_transmit", "spheres",
+                                  "brick_quads", "brick_tris"])
+def test_fp32_statistical_parity(orc, name):
+    """Per-mode transmission sums and kappa of the FP32 kernel vs the oracle:
+    every |z| < 5 and the kappa difference within 4 combined standard errors."""
+    m, spec, gb = setup(name, nmode=24, seed=5)
+    o = orc.Oracle(model=m, spectrum=spec)
+    np_ = 2000
+    run64 = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=9, np_=np_, seed=1, nbins=4,
+                       bin_omega=(0.0, float(spec.omega.max())))
+    cnt_o, lost_o, _ = o.counts(run64)
+    ko = o.kappa(run64, cnt_o)
+    run32 = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=9, np_=np_, seed=2, nbins=4,
+                       bin_omega=(0.0, float(spec.omega.max())), precision=A.PREC_FP32)
+    with A.Handle(gb.view, spec) as h:
+        kg = h.kappa(run32, want_counts=True)
+    assert kg["lost"] <= max(2, 1e-4 * kg["samples"])
+    z = _z(kg["counts"].astype(float), cnt_o.astype(float), np_)
+    assert np.max(np.abs(z)) < 5.0, np.max(np.abs(z))
+    se = np.hypot(kg["kappa_stderr"], ko["kappa_stderr"])
+    assert abs(kg["kappa"] - ko["kappa"]) < 4 * se + 1e-12 * abs(ko["kappa"]), (kg["kappa"], ko["kappa"], se)
+    seb = np.hypot(kg["bin_T_stderr"], ko["bin_T_stderr"])
+    assert np.all(np.abs(kg["bin_T"] - ko["bin_T"]) < 4 * seb + 1e-12)
+
+
+def test_device_reduction_matches_host_assembly():
+    m, spec, gb = setup("film_periodic", nmode=30)
+    run = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=11, np_=300, seed=4, nbins=6,
+                     bin_omega=(0.0, float(spec.omega.max())))
+    with A.Handle(gb.view, spec) as h:
+        kg = h.kappa(run, want_counts=True)
+    kh = A.kappa_from_counts(gb.view, spec, run, kg["counts"])
+    assert kg["kappa"] == pytest.approx(kh["kappa"], rel=1e-12)
+    assert kg["kappa_stderr"] == pytest.approx(kh["kappa_stderr"], rel=1e-10)
+    np.testing.assert_allclose(kg["bin_T"], kh["bin_T"], rtol=1e-12, atol=1e-15)
+    np.testing.assert_allclose(kg["emfp_nm"], kh["emfp_nm"], rtol=1e-12)
+
+
+@pytest.mark.parametrize("prec", [A.PREC_FP32, A.PREC_FP64])
+def test_ballistic_specular_duct_transmits_everything(prec):
+    m = synth.nanowire(length=500.0, width=50.0, height=50.0, p_side=1.0)
+    spec = synth.spectrum(4, seed=0)
+    gb = A.GeomBuf(m)
+    run = A.make_run(kind_mfp=A.MFP_MATTHIESSEN, nangle=11, np_=500, seed=3, precision=prec)
+    with A.Handle(gb.view, spec) as h:
+        k = h.kappa(run, want_counts=True)
+    assert np.all(k["counts"] == 500)
+    assert k["lost"] == 0
+
+
+@pytest.mark.parametrize("prec", [A.PREC_FP32, A.PREC_FP64])
+def test_lost_phonons_with_flight_cap(orc, prec):
+    m, spec, gb = setup("nanowire_diffuse", nmode=3)
+    run = A.make_run(kind_mfp=A.MFP_MATTHIESSEN, nangle=5, np_=300, seed=5, precision=prec)
+    with A.Handle(gb.view, spec, max_flights=1) as h:
+        a = h.kappa(run, want_counts=True)
+        sa = h.stats()
+    with A.Handle(gb.view, spec, max_flights=1, ref_quirks=1) as h:
+        b = h.kappa(run, want_counts=True)
+    assert sa["capped"] > 0 and a["lost"] == sa["capped"]
+    assert int(b["counts"].sum()) == int(a["counts"].sum()) + a["lost"]
+    with A.Handle(gb.view, spec, max_flights=1, lost_limit=1e-3) as h:
+        with pytest.raises(A.PtgError) as e:
+            h.kappa(run)
+        assert e.value.status == A.PTG_ERR_LOST
+
+
+def test_rank_partition_is_exact_fp32():
+    """Counts of two FP32 ranks sum to the single-rank counts exactly: every
+    trajectory depends only on its Philox counter."""
+    m, spec, gb = setup("film_periodic", nmode=8)
+    kw = dict(kind_mfp=A.MFP_PER_MODE, nangle=7, np_=301, seed=8, precision=A.PREC_FP32)
+    with A.Handle(gb.view, spec) as h:
+        full = h.kappa(A.make_run(**kw), want_counts=True)["counts"]
+        r0 = h.kappa(A.make_run(rank=0, nranks=2, **kw), want_counts=True)["counts"]
+        r1 = h.kappa(A.make_run(rank=1, nranks=2, **kw), want_counts=True)["counts"]
+        again = h.kappa(A.make_run(**kw), want_counts=True)["counts"]
+    np.testing.assert_array_equal(r0 + r1, full)
+    np.testing.assert_array_equal(again, full)
