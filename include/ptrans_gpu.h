@@ -176,9 +176,12 @@ typedef struct ptg_options {
   int32_t ref_quirks;       /* 1: a lost phonon also counts as transmitted      */
                             /*    (src/RTMCphon.f90:1701 then :1833)            */
   int32_t bvh_leaf;         /* BVH leaf size (0 = tuned)                        */
-  int64_t max_flights;      /* per-trajectory cap, lost when reached (0 = 2^31-1) */
+  int64_t max_flights;      /* per-trajectory cap, lost when reached (0 = 1e7)  */
   double lost_limit;        /* PTG_ERR_LOST if lost/total exceeds it (0 = off)  */
   int64_t chunk;            /* samples per work-queue chunk (0 = tuned)         */
+  int32_t tune_flags;       /* persistent kernel variants (autotuner):          */
+                            /*   bit 0: no safe-distance p-p fast path          */
+  int32_t fast_steps;       /* fast p-p flights per iteration (0 = tuned)       */
 } ptg_options;
 
 /*
@@ -230,6 +233,11 @@ typedef struct ptg_stats {
   int32_t grid, block;      /* transport launch shape                           */
   uint64_t h2d_bytes;       /* host-to-device bytes copied by the call          */
   uint64_t d2h_bytes;       /* device-to-host bytes copied by the call          */
+  uint64_t max_traj_flights;/* longest trajectory (free flights), FP32 kernel   */
+  double drain_ms;          /* FP32 kernel: start until the work queue ran dry  */
+  double tail_ms;           /* FP32 kernel: queue dry until the last warp ended */
+  uint64_t full_flights;    /* FP32 kernel: flights taken with the full test     */
+  uint64_t safe_balls;      /* FP32 kernel: safe balls computed                 */
 } ptg_stats;
 
 typedef struct ptg_handle ptg_handle;

@@ -299,13 +299,16 @@ int run_transport(ptg_handle* h, const Transport& T) {
   CU(cudaSetDevice(h->device));
   CU(h->counts.ensure(sizeof(unsigned long long) * ntask));
   CU(h->lost.ensure(sizeof(unsigned long long) * ntask));
-  CU(h->stats.ensure(sizeof(unsigned long long) * 4));
+  CU(h->stats.ensure(sizeof(unsigned long long) * 10));
   CU(h->queue.ensure(sizeof(int) * 4));
   CU(cudaMemsetAsync(h->counts.p, 0, sizeof(unsigned long long) * ntask, h->stream));
   CU(cudaMemsetAsync(h->lost.p, 0, sizeof(unsigned long long) * ntask, h->stream));
-  CU(cudaMemsetAsync(h->stats.p, 0, sizeof(unsigned long long) * 4, h->stream));
+  CU(cudaMemsetAsync(h->stats.p, 0, sizeof(unsigned long long) * 10, h->stream));
+  /* stats[5], stats[6] collect minima of the global timer */
+  CU(cudaMemsetAsync(h->stats.as<unsigned long long>() + 5, 0xFF, sizeof(unsigned long long) * 2,
+                     h->stream));
   CU(cudaMemsetAsync(h->queue.p, 0, sizeof(int) * 4, h->stream));
-  const int64_t maxf = h->opt.max_flights > 0 ? h->opt.max_flights : 2147483647LL;
+  const int64_t maxf = h->opt.max_flights > 0 ? h->opt.max_flights : 10000000LL;
   memset(&h->last, 0, sizeof(h->last));
   if (T.precision == PTG_PREC_FP64) {
     std::vector<ptg::Task64> t64(ntask);
@@ -391,6 +394,9 @@ int run_transport(ptg_handle* h, const Transport& T) {
     r.ref_quirks = h->opt.ref_quirks;
     int rt = h->opt.regen_threshold;
     r.regen_threshold = rt < 1 ? 1 : (rt > 32 ? 32 : rt);
+    r.fast_steps = (h->opt.tune_flags & 1) ? 0 : (h->opt.fast_steps > 0 ? h->opt.fast_steps : 16);
+    const double lmin = std::min(h->geom.box[0], std::min(h->geom.box[1], h->geom.box[2]));
+    r.fast_lambda_max = (float)(0.1 * lmin);
     r.counts = h->counts.as<unsigned long long>();
     r.lost = h->lost.as<unsigned long long>();
     r.stats = h->stats.as<unsigned long long>();
@@ -413,7 +419,7 @@ int run_transport(ptg_handle* h, const Transport& T) {
 }
 
 int finish_stats(ptg_handle* h) {
-  unsigned long long st[4];
+  unsigned long long st[10];
   int qerr[4];
   CU(cudaMemcpyAsync(st, h->stats.p, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
   CU(cudaMemcpyAsync(qerr, h->queue.p, sizeof(qerr), cudaMemcpyDeviceToHost, h->stream));
@@ -426,6 +432,14 @@ int finish_stats(ptg_handle* h) {
   h->last.capped = st[2];
   h->last.samples = st[3];
   h->last.kernel_ms = ms;
+  h->last.max_traj_flights = st[4];
+  h->last.full_flights = st[8];
+  h->last.safe_balls = st[9];
+  if (st[5] != ~0ull && st[7] >= st[5]) {
+    const unsigned long long drain = st[6] != ~0ull ? st[6] : st[7];
+    h->last.drain_ms = (double)(drain - st[5]) * 1e-6;
+    h->last.tail_ms = (double)(st[7] - drain) * 1e-6;
+  }
   if (qerr[1] != 0) { h->last_error = "shared-memory staging wait timed out"; return PTG_ERR_TIMEOUT; }
   return PTG_OK;
 }
@@ -824,7 +838,7 @@ int ptg_replay_task(ptg_handle* h, const ptg_run* run, int64_t task, int32_t* en
     r.k0 = (uint32_t)run->seed;
     r.k1 = (uint32_t)(run->seed >> 32);
     r.c1 = ((uint32_t)run->stream) << 8;
-    r.max_flights = h->opt.max_flights > 0 ? h->opt.max_flights : 2147483647LL;
+    r.max_flights = h->opt.max_flights > 0 ? h->opt.max_flights : 10000000LL;
     r.ref_quirks = h->opt.ref_quirks;
     r.counts = dc.as<unsigned long long>();
     r.lost = dl.as<unsigned long long>();

@@ -107,9 +107,14 @@ struct RunF32 {
   uint32_t max_flights;
   int32_t ref_quirks;
   int32_t regen_threshold;
+  int32_t fast_steps;         /* max safe-distance p-p flights per iteration (0: off) */
+  float fast_lambda_max;      /* tasks with a smaller MFP use the fast path           */
   unsigned long long* counts;
   unsigned long long* lost;
-  unsigned long long* stats;  /* flights, lost, capped, samples */
+  /* flights, lost, capped, samples, max trajectory flights,
+     t_start (min), t_drain (min), t_end (max) in globaltimer ns,
+     flights taken with the intersection test, safe balls built */
+  unsigned long long* stats;
   int* queue;                 /* [0] next chunk, [1] error flags */
 };
 

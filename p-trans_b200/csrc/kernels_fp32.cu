@@ -20,9 +20,21 @@
  *     stable quadratic roots, the far root from the inside, and exclude the
  *     surface just left from the outside, which replaces the reference's
  *     absolute 1e-7 nm nudge (src/RTMCphon.f90:1779);
+ *   - safe-ball fast path: after an intrinsic (p-p) event a lane with a short
+ *     MFP computes a lower bound d of the distance from that point to every
+ *     surface of its grain and of the box; while the end point of the next
+ *     free path stays inside the ball of radius d around that point the whole
+ *     segment does (the ball is convex), so the flight must end in another p-p
+ *     event and is taken without an intersection test.  The flight is still
+ *     counted and still draws its own Philox block, so the trajectory is the
+ *     one the full test gives.  A diffusive walk leaves the ball only after
+ *     about (d/MFP)^2 flights, which shortens the serial chain of the longest
+ *     trajectories that bound the kernel's run time;
  *   - one Philox4x32-10 block per free flight supplies the four uniforms of
- *     any event; tallies are integer, aggregated per warp by task
- *     (match_any) before one atomic.
+ *     any event; on the fast path the blocks of four flights are computed
+ *     together so that four independent chains fill the issue slots of a
+ *     warp that is alone on its scheduler (the tail of a run); tallies are
+ *     integer, aggregated per warp by task (match_any) before one atomic.
  */
 #include <cuda_runtime.h>
 #include <math.h>
@@ -37,6 +49,8 @@ namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int kBlock = 256;
+constexpr float kTwoPi = 6.28318530717958648f;
+constexpr float kPi = 3.14159265358979323846f;
 
 struct Geo {
   const float4* base;   /* blob in shared or global memory */
@@ -57,6 +71,20 @@ struct Geo {
   }
   __device__ __forceinline__ float4 start(int i) const { return base[lay.start + i]; }
 };
+
+/* Square root from the hardware approximation (relative error ~2^-22). */
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float y;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+/* sin / cos of 2*pi*u, u in (0,1): hardware approximations on [-pi, pi). */
+__device__ __forceinline__ void sincos2pi(float u, float* s, float* c) {
+  const float a = fmaf(u, kTwoPi, -kPi);
+  *s = -__sinf(a);
+  *c = -__cosf(a);
+}
 
 __device__ __forceinline__ bool inside_edges(const Geo& G, int e0, int ne, float x, float y,
                                              float z, float eps) {
@@ -128,10 +156,44 @@ __device__ __forceinline__ void scan_grain(const Geo& G, int grain, float px, fl
   }
 }
 
+/* Lower bound of the distance from p to every box face and to every
+   candidate surface of the grain (planes bound polygons from below, the
+   infinite cylinder bounds the clipped one). */
+__device__ __forceinline__ float safety(const Geo& G, int grain, float px, float py, float pz,
+                                        float X, float Y, float Z, float eps) {
+  float d = fminf(fminf(fminf(px, X - px), fminf(py, Y - py)), fminf(pz, Z - pz));
+  if (grain > 0) {
+    const int kb = G.cand_begin(grain), ke = G.cand_begin(grain + 1);
+    for (int k = kb; k < ke; ++k) {
+      const int s = G.cand(k);
+      const float4 A = G.hotA(s);
+      const int type = G.hotB(s).x & 0xff;
+      float e;
+      if (type == REC_POLY) {
+        e = fabsf(A.w - fmaf(A.x, px, fmaf(A.y, py, A.z * pz)));
+      } else if (type == REC_SPHERE) {
+        const float wx = px - A.x, wy = py - A.y, wz = pz - A.z;
+        e = fabsf(sqrtf(fmaf(wx, wx, fmaf(wy, wy, wz * wz))) - A.w);
+      } else {
+        const float wx = px - A.x, wy = py - A.y;
+        e = fabsf(sqrtf(fmaf(wx, wx, wy * wy)) - A.z);
+      }
+      d = fminf(d, e);
+    }
+  }
+  return d - 4.0f * eps;
+}
+
 __device__ __forceinline__ unsigned lanemask_lt() {
   unsigned m;
   asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
   return m;
+}
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
 }
 
 __device__ __forceinline__ void warp_add_by_task(bool pred, int task, unsigned long long* arr) {
@@ -179,11 +241,12 @@ __device__ bool stage_blob(const float4* gblob, float4* sblob, int units, int* e
   return ok != 0;
 }
 
-__global__ void __launch_bounds__(kBlock, 4) k_persistent(GeoF32 gp, RunF32 r) {
+__global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   extern __shared__ float4 sblob[];
   Geo G;
   G.lay = gp.lay;
   G.base = gp.blob;
+  if (threadIdx.x == 0) atomicMin(r.stats + 5, globaltimer());
   if (gp.stage_smem) {
     if (stage_blob(gp.blob, sblob, gp.lay.total, r.queue + 1)) G.base = sblob;
   }
@@ -199,9 +262,12 @@ __global__ void __launch_bounds__(kBlock, 4) k_persistent(GeoF32 gp, RunF32 r) {
   /* lane state */
   bool alive = false;
   float px = 0, py = 0, pz = 0, dx = 1, dy = 0, dz = 0, fp = 0, lam = 0, omr = 0;
+  /* safe ball: no surface closer than sqrt(br2) to (bx, by, bz) */
+  float bx = 0, by = 0, bz = 0, br2 = 0;
   int grain = 0, last_geom = -1, task = 0;
   uint32_t slo = 0, shi = 0, flight = 0;
-  unsigned long long my_flights = 0, my_samples = 0, my_capped = 0, my_lost = 0;
+  unsigned long long my_flights = 0, my_samples = 0, my_capped = 0, my_lost = 0, my_max = 0;
+  unsigned my_full = 0, my_balls = 0;
 
   while (true) {
     /* ---- refill idle lanes from the warp's chunk ---------------------- */
@@ -213,7 +279,11 @@ __global__ void __launch_bounds__(kBlock, 4) k_persistent(GeoF32 gp, RunF32 r) {
           int c = 0;
           if (lane == 0) c = atomicAdd(r.queue, 1);
           c = __shfl_sync(FULL, c, 0);
-          if (c >= r.nchunk) { queue_done = true; break; }
+          if (c >= r.nchunk) {
+            queue_done = true;
+            if (lane == 0) atomicMin(r.stats + 6, globaltimer());
+            break;
+          }
           const int4 q = r.chunk[c];
           ch_task = q.x; ch_next = q.y; ch_left = q.z;
         }
@@ -235,7 +305,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_persistent(GeoF32 gp, RunF32 r) {
           py = u23f(R0.x) * Y * gp.scope[0];
           pz = u23f(R0.y) * Z * gp.scope[1];
           float sp, cp;
-          sincospif(2.0f * u23f(R0.z), &sp, &cp);
+          sincos2pi(u23f(R0.z), &sp, &cp);
           dx = T.y;
           dy = T.z * cp;
           dz = T.z * sp;
@@ -262,6 +332,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_persistent(GeoF32 gp, RunF32 r) {
             }
           }
           last_geom = -1;
+          br2 = 0.0f;
           flight = 0;
           alive = true;
           my_samples += 1;
@@ -276,144 +347,196 @@ __global__ void __launch_bounds__(kBlock, 4) k_persistent(GeoF32 gp, RunF32 r) {
       continue;
     }
 
-    /* ---- one free flight ------------------------------------------------ */
     int end_side = -1;  /* -1 still running, 0 lost, 1 x-, 2 x+ */
     if (alive) {
-      if (!(px >= -eps && px <= X + eps && py >= -eps && py <= Y + eps && pz >= -eps &&
-            pz <= Z + eps)) {
-        end_side = 0;
-      } else if (flight >= r.max_flights) {
-        end_side = 0;
-        my_capped += 1;
-      } else {
-        ++flight;
-        const uint4 R = philox10(flight, r.c1, slo, shi, key);
-        /* slab exit of the box grain */
-        float tb = 3.0e38f;
-        int sb = -1;
-        if (dx > 0.0f) { tb = __fdividef(X - px, dx); sb = 1; }
-        else if (dx < 0.0f) { tb = __fdividef(-px, dx); sb = 0; }
-        if (dy != 0.0f) {
-          const float t = __fdividef((dy > 0.0f ? Y : 0.0f) - py, dy);
-          if (t < tb) { tb = t; sb = dy > 0.0f ? 3 : 2; }
-        }
-        if (dz != 0.0f) {
-          const float t = __fdividef((dz > 0.0f ? Z : 0.0f) - pz, dz);
-          if (t < tb) { tb = t; sb = dz > 0.0f ? 5 : 4; }
-        }
-        tb = fmaxf(tb, 0.0f);
-        if (grain > 0) scan_grain(G, grain, px, py, pz, dx, dy, dz, last_geom, eps, Z, tb, sb);
-
-        const float u0 = u23f(R.x), u1 = u23f(R.y), u2 = u23f(R.z), u3 = u23f(R.w);
-        if (fp < tb) {
-          /* intrinsic scattering: isotropic direction, new free path */
-          px = fmaf(fp, dx, px);
-          py = fmaf(fp, dy, py);
-          pz = fmaf(fp, dz, pz);
-          const float ct = fmaf(u0, 2.0f, -1.0f);
-          const float st = sqrtf(fmaxf(0.0f, fmaf(-ct, ct, 1.0f)));
+      /* ---- safe-ball p-p flights: the segment to the next p-p point stays
+         inside the safe ball (convex), so no surface is crossed.  Four
+         flights at a time: their Philox blocks, new directions and free
+         paths do not depend on the phonon state and are computed together;
+         only the position / ball test chain is serial. ---- */
+      int k = 0;
+      bool fast_more = br2 > 0.0f;
+      while (fast_more && k < r.fast_steps && flight + 4u <= r.max_flights) {
+        uint4 B[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) B[j] = philox10(flight + 1u + j, r.c1, slo, shi, key);
+        float nx[4], ny[4], nz[4], nf[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const float ct = fmaf(u23f(B[j].x), 2.0f, -1.0f);
+          const float st = sqrt_approx(fmaxf(0.0f, fmaf(-ct, ct, 1.0f)));
           float sp, cp;
-          sincospif(2.0f * u1, &sp, &cp);
-          dx = ct;
-          dy = st * cp;
-          dz = st * sp;
-          fp = -lam * __logf(u2);
-          last_geom = -1;
-        } else {
-          px = fmaf(tb, dx, px);
-          py = fmaf(tb, dy, py);
-          pz = fmaf(tb, dz, pz);
-          fp -= tb;
-          if (sb == 0) {
-            end_side = 1;
-          } else if (sb == 1) {
-            end_side = 2;
-          } else if (sb < 6 && ((gp.periodic_mask >> sb) & 1)) {
-            const int ax = sb >> 1;
-            const float L = ax == 1 ? Y : Z;
-            const float sg = (sb & 1) ? -L : L;
-            if (ax == 1) py += sg; else pz += sg;
-            last_geom = -1;
-          } else {
-            /* surface event: determinSpecular, reflectSpecular /
-               reflectDiffusive, determinTransmit (src/RTMCphon.f90:2225-2413) */
-            const float4 C0 = G.cold(sb, 0), C1 = G.cold(sb, 1), C2 = G.cold(sb, 2);
-            const int meta = __float_as_int(C2.w);
-            const int kind = meta & 0xff;
-            float thr = 0.0f;
-            if (kind == 1) {
-              thr = C1.w;
-            } else if (kind == 2 || kind == 3) {
-              if (gp.nmaterial == 1) {
-                thr = __frcp_rn(fmaf(C1.w, omr, 1.0f));
-              } else {
-                const uint4 R2 = philox10(flight, r.c1 | 1u, slo, shi, key);
-                const float t11 = __frcp_rn(C1.w + 1.0f);
-                thr = fmaf(u23f(R2.x), 1.0f - t11, t11);
-              }
-            }
-            /* surface normal at the hit point and surface frame */
-            float nx, ny, nz, ax1, ay1, az1, ax2, ay2, az2;
-            const int4 B = G.hotB(sb);
-            const int type = B.x & 0xff;
-            if (type == REC_POLY) {
-              nx = C2.x; ny = C2.y; nz = C2.z;
-              ax1 = C0.x; ay1 = C0.y; az1 = C0.z;
-              ax2 = C1.x; ay2 = C1.y; az2 = C1.z;
+          sincos2pi(u23f(B[j].y), &sp, &cp);
+          nx[j] = ct;
+          ny[j] = st * cp;
+          nz[j] = st * sp;
+          nf[j] = -lam * __logf(u23f(B[j].z));
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          if (fast_more) {
+            const float qx = fmaf(fp, dx, px), qy = fmaf(fp, dy, py), qz = fmaf(fp, dz, pz);
+            const float ex = qx - bx, ey = qy - by, ez = qz - bz;
+            if (fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < br2) {
+              ++flight;
+              px = qx; py = qy; pz = qz;
+              dx = nx[j]; dy = ny[j]; dz = nz[j];
+              fp = nf[j];
+              ++k;
             } else {
-              const float4 A = G.hotA(sb);
-              float rx = px - A.x, ry = py - A.y, rz = (type == REC_SPHERE) ? pz - A.z : 0.0f;
-              const float inv = rsqrtf(fmaf(rx, rx, fmaf(ry, ry, rz * rz)));
-              nx = rx * inv; ny = ry * inv; nz = rz * inv;
-              const float q2 = fmaf(nx, nx, ny * ny);
-              if (q2 > 1.0e-12f) {
-                const float q = rsqrtf(q2);
-                ax2 = -ny * q; ay2 = nx * q; az2 = 0.0f;
-              } else {
-                ax2 = 0.0f; ay2 = 1.0f; az2 = 0.0f;
-              }
-              /* t1 = t2 x n */
-              ax1 = ay2 * nz - az2 * ny;
-              ay1 = az2 * nx - ax2 * nz;
-              az1 = ax2 * ny - ay2 * nx;
-              if (q2 <= 1.0e-12f) { ax1 = 1.0f; ay1 = 0.0f; az1 = 0.0f; }
+              fast_more = false;
             }
-            /* tmpNormal oriented along the incoming direction */
-            const float dn0 = fmaf(nx, dx, fmaf(ny, dy, nz * dz));
-            const float on = dn0 < 0.0f ? -1.0f : 1.0f;
-            bool transmitted = false;
-            if (u0 <= C0.w) {
-              if (u1 <= thr) {
-                transmitted = true;
-              } else {
-                const float k2 = 2.0f * dn0;
-                dx = fmaf(-k2, nx, dx);
-                dy = fmaf(-k2, ny, dy);
-                dz = fmaf(-k2, nz, dz);
-                const float inv = rsqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
-                dx *= inv; dy *= inv; dz *= inv;
-              }
-            } else {
-              const float sint = sqrtf(u1);
-              const float cost = sqrtf(fmaxf(0.0f, 1.0f - u1));
-              float sp, cp;
-              sincospif(2.0f * u2, &sp, &cp);
-              const float a = sint * cp, b = sint * sp;
-              float vx = fmaf(ax1, a, fmaf(ax2, b, nx * cost));
-              float vy = fmaf(ay1, a, fmaf(ay2, b, ny * cost));
-              float vz = fmaf(az1, a, fmaf(az2, b, nz * cost));
-              /* Lambertian into the incidence side, then optionally through */
-              const float s = on * fmaf(vx, nx, fmaf(vy, ny, vz * nz));
-              float sg = s > 0.0f ? -1.0f : 1.0f;
-              if (u3 <= thr) { sg = -sg; transmitted = true; }
-              dx = sg * vx; dy = sg * vy; dz = sg * vz;
-            }
-            if (transmitted) grain = meta >> 8;
-            last_geom = B.w;
           }
-          if (end_side < 0 && fp < 1.0e-10f) {
-            const uint4 R2 = philox10(flight, r.c1 | 1u, slo, shi, key);
-            fp = -lam * __logf(u23f(R2.y));
+        }
+      }
+      /* a lane that used up its fast steps waits for the next iteration;
+         any other lane takes one flight with the full test now */
+      if (!(fast_more && k >= r.fast_steps)) {
+        /* ---- one free flight with the intersection test -------------- */
+        if (!(px >= -eps && px <= X + eps && py >= -eps && py <= Y + eps && pz >= -eps &&
+              pz <= Z + eps)) {
+          end_side = 0;
+        } else if (flight >= r.max_flights) {
+          end_side = 0;
+          my_capped += 1;
+        } else {
+          ++flight;
+          ++my_full;
+          const uint4 R = philox10(flight, r.c1, slo, shi, key);
+          /* slab exit of the box grain */
+          float tb = 3.0e38f;
+          int sb = -1;
+          if (dx > 0.0f) { tb = __fdividef(X - px, dx); sb = 1; }
+          else if (dx < 0.0f) { tb = __fdividef(-px, dx); sb = 0; }
+          if (dy != 0.0f) {
+            const float t = __fdividef((dy > 0.0f ? Y : 0.0f) - py, dy);
+            if (t < tb) { tb = t; sb = dy > 0.0f ? 3 : 2; }
+          }
+          if (dz != 0.0f) {
+            const float t = __fdividef((dz > 0.0f ? Z : 0.0f) - pz, dz);
+            if (t < tb) { tb = t; sb = dz > 0.0f ? 5 : 4; }
+          }
+          tb = fmaxf(tb, 0.0f);
+          if (grain > 0) scan_grain(G, grain, px, py, pz, dx, dy, dz, last_geom, eps, Z, tb, sb);
+
+          const float u0 = u23f(R.x), u1 = u23f(R.y), u2 = u23f(R.z), u3 = u23f(R.w);
+          if (fp < tb) {
+            /* intrinsic scattering: isotropic direction, new free path */
+            px = fmaf(fp, dx, px);
+            py = fmaf(fp, dy, py);
+            pz = fmaf(fp, dz, pz);
+            const float ct = fmaf(u0, 2.0f, -1.0f);
+            const float st = sqrt_approx(fmaxf(0.0f, fmaf(-ct, ct, 1.0f)));
+            float sp, cp;
+            sincos2pi(u1, &sp, &cp);
+            dx = ct;
+            dy = st * cp;
+            dz = st * sp;
+            fp = -lam * __logf(u2);
+            last_geom = -1;
+            br2 = 0.0f;
+            if (r.fast_steps > 0 && lam < r.fast_lambda_max) {
+              const float d = safety(G, grain, px, py, pz, X, Y, Z, eps);
+              ++my_balls;
+              if (d > 0.0f) { bx = px; by = py; bz = pz; br2 = d * d; }
+            }
+          } else {
+            br2 = 0.0f;
+            px = fmaf(tb, dx, px);
+            py = fmaf(tb, dy, py);
+            pz = fmaf(tb, dz, pz);
+            fp -= tb;
+            if (sb == 0) {
+              end_side = 1;
+            } else if (sb == 1) {
+              end_side = 2;
+            } else if (sb < 6 && ((gp.periodic_mask >> sb) & 1)) {
+              const int ax = sb >> 1;
+              const float L = ax == 1 ? Y : Z;
+              const float sg = (sb & 1) ? -L : L;
+              if (ax == 1) py += sg; else pz += sg;
+              last_geom = -1;
+            } else {
+              /* surface event: determinSpecular, reflectSpecular /
+                 reflectDiffusive, determinTransmit (src/RTMCphon.f90:2225-2413) */
+              const float4 C0 = G.cold(sb, 0), C1 = G.cold(sb, 1), C2 = G.cold(sb, 2);
+              const int meta = __float_as_int(C2.w);
+              const int kind = meta & 0xff;
+              float thr = 0.0f;
+              if (kind == 1) {
+                thr = C1.w;
+              } else if (kind == 2 || kind == 3) {
+                if (gp.nmaterial == 1) {
+                  thr = __frcp_rn(fmaf(C1.w, omr, 1.0f));
+                } else {
+                  const uint4 R2 = philox10(flight, r.c1 | 1u, slo, shi, key);
+                  const float t11 = __frcp_rn(C1.w + 1.0f);
+                  thr = fmaf(u23f(R2.x), 1.0f - t11, t11);
+                }
+              }
+              /* surface normal at the hit point and surface frame */
+              float nx, ny, nz, ax1, ay1, az1, ax2, ay2, az2;
+              const int4 B = G.hotB(sb);
+              const int type = B.x & 0xff;
+              if (type == REC_POLY) {
+                nx = C2.x; ny = C2.y; nz = C2.z;
+                ax1 = C0.x; ay1 = C0.y; az1 = C0.z;
+                ax2 = C1.x; ay2 = C1.y; az2 = C1.z;
+              } else {
+                const float4 A = G.hotA(sb);
+                float rx = px - A.x, ry = py - A.y, rz = (type == REC_SPHERE) ? pz - A.z : 0.0f;
+                const float inv = rsqrtf(fmaf(rx, rx, fmaf(ry, ry, rz * rz)));
+                nx = rx * inv; ny = ry * inv; nz = rz * inv;
+                const float q2 = fmaf(nx, nx, ny * ny);
+                if (q2 > 1.0e-12f) {
+                  const float q = rsqrtf(q2);
+                  ax2 = -ny * q; ay2 = nx * q; az2 = 0.0f;
+                  /* t1 = t2 x n */
+                  ax1 = ay2 * nz - az2 * ny;
+                  ay1 = az2 * nx - ax2 * nz;
+                  az1 = ax2 * ny - ay2 * nx;
+                } else {
+                  ax2 = 0.0f; ay2 = 1.0f; az2 = 0.0f;
+                  ax1 = 1.0f; ay1 = 0.0f; az1 = 0.0f;
+                }
+              }
+              /* tmpNormal oriented along the incoming direction */
+              const float dn0 = fmaf(nx, dx, fmaf(ny, dy, nz * dz));
+              const float on = dn0 < 0.0f ? -1.0f : 1.0f;
+              bool transmitted = false;
+              if (u0 <= C0.w) {
+                if (u1 <= thr) {
+                  transmitted = true;
+                } else {
+                  const float k2 = 2.0f * dn0;
+                  dx = fmaf(-k2, nx, dx);
+                  dy = fmaf(-k2, ny, dy);
+                  dz = fmaf(-k2, nz, dz);
+                  const float inv = rsqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+                  dx *= inv; dy *= inv; dz *= inv;
+                }
+              } else {
+                const float sint = sqrt_approx(u1);
+                const float cost = sqrt_approx(fmaxf(0.0f, 1.0f - u1));
+                float sp, cp;
+                sincos2pi(u2, &sp, &cp);
+                const float a = sint * cp, b = sint * sp;
+                const float vx = fmaf(ax1, a, fmaf(ax2, b, nx * cost));
+                const float vy = fmaf(ay1, a, fmaf(ay2, b, ny * cost));
+                const float vz = fmaf(az1, a, fmaf(az2, b, nz * cost));
+                /* Lambertian into the incidence side, then optionally through */
+                const float s = on * fmaf(vx, nx, fmaf(vy, ny, vz * nz));
+                float sg = s > 0.0f ? -1.0f : 1.0f;
+                if (u3 <= thr) { sg = -sg; transmitted = true; }
+                dx = sg * vx; dy = sg * vy; dz = sg * vz;
+              }
+              if (transmitted) grain = meta >> 8;
+              last_geom = B.w;
+            }
+            if (end_side < 0 && fp < 1.0e-10f) {
+              const uint4 R2 = philox10(flight, r.c1 | 1u, slo, shi, key);
+              fp = -lam * __logf(u23f(R2.y));
+            }
           }
         }
       }
@@ -427,22 +550,31 @@ __global__ void __launch_bounds__(kBlock, 4) k_persistent(GeoF32 gp, RunF32 r) {
     if (fin) {
       my_flights += flight;
       my_lost += lostp ? 1 : 0;
+      my_max = max(my_max, (unsigned long long)flight);
       alive = false;
     }
   }
-  /* block-wide totals */
-  unsigned long long v0 = my_flights, v1 = my_lost, v2 = my_capped, v3 = my_samples;
+  /* warp totals */
+  unsigned long long v0 = my_flights, v1 = my_lost, v2 = my_capped, v3 = my_samples, v4 = my_max;
+  unsigned long long v5 = my_full, v6 = my_balls;
   for (int o = 16; o > 0; o >>= 1) {
+    v5 += __shfl_xor_sync(FULL, v5, o);
+    v6 += __shfl_xor_sync(FULL, v6, o);
     v0 += __shfl_xor_sync(FULL, v0, o);
     v1 += __shfl_xor_sync(FULL, v1, o);
     v2 += __shfl_xor_sync(FULL, v2, o);
     v3 += __shfl_xor_sync(FULL, v3, o);
+    v4 = max(v4, __shfl_xor_sync(FULL, v4, o));
   }
   if (lane == 0) {
     if (v0) atomicAdd(r.stats + 0, v0);
     if (v1) atomicAdd(r.stats + 1, v1);
     if (v2) atomicAdd(r.stats + 2, v2);
     if (v3) atomicAdd(r.stats + 3, v3);
+    atomicMax(r.stats + 4, v4);
+    atomicMax(r.stats + 7, globaltimer());
+    if (v5) atomicAdd(r.stats + 8, v5);
+    if (v6) atomicAdd(r.stats + 9, v6);
   }
 }
 

@@ -43,9 +43,11 @@ __device__ __forceinline__ double u52d(uint32_t a, uint32_t b) {
   return ((double)k + 0.5) * (1.0 / 4503599627370496.0);
 }
 
-/* (k + 0.5) * 2^-23 from the top 23 bits of a: open interval (0,1). */
+/* (k + 0.5) * 2^-23 from the top 23 bits k of a: open interval (0,1).
+   Built from the bit pattern 1 + k 2^-23 minus (1 - 2^-24), which is exact
+   and avoids the integer-to-float conversion pipe. */
 __device__ __forceinline__ float u23f(uint32_t a) {
-  return ((float)(a >> 9) + 0.5f) * (1.0f / 8388608.0f);
+  return __uint_as_float((a >> 9) | 0x3f800000u) - 0.99999994039535522f;
 }
 
 }  // namespace ptg
