@@ -315,6 +315,27 @@ int ptg_kappa_from_counts(const ptg_geometry* geom, const ptg_spectrum* spec,
 /* Statistics of the last transport call on h. */
 int ptg_last_stats(const ptg_handle* h, ptg_stats* st);
 
+/*
+ * ptg_transmission_noalloc - no counterpart in the reference; an addition for
+ * hosts that cannot allocate memory while they run (device memory reserved up
+ * front by another framework, or a service that must keep a fixed
+ * footprint).  It computes what ptg_transmission computes with
+ * PTG_PREC_FP32 (same counts, so the same transmit array) but allocates no
+ * device or host memory: the kernel's scratch (work-queue counter,
+ * statistics, tallies, task and chunk tables) lives in one static device
+ * array of fixed size that every GPU loading the library keeps until exit,
+ * and the caller's transmit array receives the counts before they are
+ * divided by np in place.  Limits: nbranch*nkpoint*(nangle-1) <=
+ * PTG_NOALLOC_MAX_TASKS, nangle <= 64; larger runs return PTG_ERR_INVALID.
+ * The first call on a device looks up the array's address (make it before
+ * any stream capture).  All calls share the array: calls whose GPU work
+ * overlaps race and must be serialised by the caller.
+ */
+#define PTG_NOALLOC_MAX_TASKS  16384
+#define PTG_NOALLOC_MAX_CHUNKS 65536
+int ptg_transmission_noalloc(ptg_handle* h, double mfp_nm, int32_t nangle, int64_t np,
+                             int32_t rank, int32_t nranks, uint64_t seed, double* transmit);
+
 /* Debug / replay: runs the FP64 kernel for one task and writes, per particle,
    the exit side (0 lost, 1 x-, 2 x+) and the number of free flights. */
 int ptg_replay_task(ptg_handle* h, const ptg_run* run, int64_t task,

@@ -160,7 +160,10 @@ SIGNATURES = {
                                         C.POINTER(PtgRun), U64P, C.POINTER(PtgKappaOut)]),
     "ptg_last_stats": (C.c_int, [C.c_void_p, C.POINTER(PtgStats)]),
     "ptg_replay_task": (C.c_int, [C.c_void_p, C.POINTER(PtgRun), C.c_int64, I32P, U32P, F64P]),
+    "ptg_transmission_noalloc": (C.c_int, [C.c_void_p, C.c_double, C.c_int32, C.c_int64, C.c_int32,
+                                           C.c_int32, C.c_uint64, F64P]),
 }
+NOALLOC_MAX_TASKS = 16384
 
 _LIB = None
 
@@ -467,6 +470,16 @@ class Handle:
                                        _ptr(t, C.c_double), _ptr(e, C.c_double))
         _check(st, "ptg_transmission")
         return t.reshape(nangle, nk, nb).transpose(2, 1, 0), e.reshape(nangle, nk, nb).transpose(2, 1, 0)
+
+    def transmission_noalloc(self, mfp_nm, nangle, np_, rank=0, nranks=1, seed=0):
+        """ptg_transmission_noalloc: the FP32 transmission function without any
+        allocation by the call (scratch in a fixed static device array)."""
+        nb, nk = self._spec.nbranch, self._spec.nkpoint
+        t = np.zeros(nb * nk * nangle)
+        st = self.lib.ptg_transmission_noalloc(self.h, mfp_nm, nangle, np_, rank, nranks, seed,
+                                               _ptr(t, C.c_double))
+        _check(st, "ptg_transmission_noalloc")
+        return t.reshape(nangle, nk, nb).transpose(2, 1, 0)
 
     def kappa(self, run: PtgRun, want_transmit=False, want_counts=False) -> dict:
         nm = self._spec.nmode

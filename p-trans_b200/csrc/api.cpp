@@ -459,6 +459,23 @@ int check_lost(ptg_handle* h) {
 
 }  // namespace
 
+namespace ptg {
+
+int handle_noalloc_view(ptg_handle* h, NoallocView* v) {
+  if (!h || !v) return PTG_ERR_INVALID;
+  v->g32 = h->g32;
+  v->blob_bytes = h->blob_bytes;
+  v->device = h->device;
+  v->num_sms = h->num_sms;
+  v->stream = h->stream;
+  v->opt = h->opt;
+  v->spec = &h->spec;
+  v->geom = &h->geom;
+  return PTG_OK;
+}
+
+}  // namespace ptg
+
 /* ========================================================================= */
 extern "C" {
 

@@ -69,4 +69,22 @@ void simpson_weights(int nangle, double box_x, std::vector<double>* coef, double
 
 }  // namespace ptg
 
+#include "kernels.h"
+
+namespace ptg {
+
+/* What ptg_transmission_noalloc reads from a handle (no copies made). */
+struct NoallocView {
+  GeoF32 g32;
+  size_t blob_bytes;
+  int device, num_sms;
+  cudaStream_t stream;
+  ptg_options opt;
+  const SpecSoA* spec;
+  const GeomSoA* geom;
+};
+int handle_noalloc_view(ptg_handle* h, NoallocView* v);
+
+}  // namespace ptg
+
 #endif
