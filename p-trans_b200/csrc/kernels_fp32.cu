@@ -52,24 +52,34 @@ constexpr int kBlock = 256;
 constexpr float kTwoPi = 6.28318530717958648f;
 constexpr float kPi = 3.14159265358979323846f;
 
+extern __shared__ float4 sblob[];
+
+/* Geometry blob accessor: SMEM = true reads the copy staged in shared
+   memory (shared-memory loads), false reads global memory through the
+   read-only path. */
+template <bool SMEM>
 struct Geo {
-  const float4* base;   /* blob in shared or global memory */
+  const float4* base;   /* global blob (SMEM = false) */
   BlobLayout lay;
-  __device__ __forceinline__ float4 hotA(int s) const { return base[lay.hot + 2 * s]; }
+  __device__ __forceinline__ float4 ld(int i) const {
+    if (SMEM) return sblob[i];
+    return __ldg(base + i);
+  }
+  __device__ __forceinline__ int ldi(int unit, int k) const {
+    if (SMEM) return reinterpret_cast<const int*>(sblob + unit)[k];
+    return __ldg(reinterpret_cast<const int*>(base + unit) + k);
+  }
+  __device__ __forceinline__ float4 hotA(int s) const { return ld(lay.hot + 2 * s); }
   __device__ __forceinline__ int4 hotB(int s) const {
-    const float4 v = base[lay.hot + 2 * s + 1];
+    const float4 v = ld(lay.hot + 2 * s + 1);
     return make_int4(__float_as_int(v.x), __float_as_int(v.y), __float_as_int(v.z),
                      __float_as_int(v.w));
   }
-  __device__ __forceinline__ float4 cold(int s, int i) const { return base[lay.cold + 3 * s + i]; }
-  __device__ __forceinline__ float4 edge(int e) const { return base[lay.edge + e]; }
-  __device__ __forceinline__ int cand_begin(int g) const {
-    return reinterpret_cast<const int*>(base + lay.cand_begin)[g];
-  }
-  __device__ __forceinline__ int cand(int k) const {
-    return reinterpret_cast<const int*>(base + lay.cand)[k];
-  }
-  __device__ __forceinline__ float4 start(int i) const { return base[lay.start + i]; }
+  __device__ __forceinline__ float4 cold(int s, int i) const { return ld(lay.cold + 3 * s + i); }
+  __device__ __forceinline__ float4 edge(int e) const { return ld(lay.edge + e); }
+  __device__ __forceinline__ int cand_begin(int g) const { return ldi(lay.cand_begin, g); }
+  __device__ __forceinline__ int cand(int k) const { return ldi(lay.cand, k); }
+  __device__ __forceinline__ float4 start(int i) const { return ld(lay.start + i); }
 };
 
 /* Square root from the hardware approximation (relative error ~2^-22). */
@@ -86,7 +96,8 @@ __device__ __forceinline__ void sincos2pi(float u, float* s, float* c) {
   *c = -__cosf(a);
 }
 
-__device__ __forceinline__ bool inside_edges(const Geo& G, int e0, int ne, float x, float y,
+template <class G_t>
+__device__ __forceinline__ bool inside_edges(const G_t& G, int e0, int ne, float x, float y,
                                              float z, float eps) {
   for (int e = 0; e < ne; ++e) {
     const float4 m = G.edge(e0 + e);
@@ -96,7 +107,8 @@ __device__ __forceinline__ bool inside_edges(const Geo& G, int e0, int ne, float
 }
 
 /* Nearest surface among the candidates of a grain (not the box). */
-__device__ __forceinline__ void scan_grain(const Geo& G, int grain, float px, float py, float pz,
+template <class G_t>
+__device__ __forceinline__ void scan_grain(const G_t& G, int grain, float px, float py, float pz,
                                            float dx, float dy, float dz, int last_geom, float eps,
                                            float zmax, float& tb, int& sb) {
   const int kb = G.cand_begin(grain), ke = G.cand_begin(grain + 1);
@@ -159,7 +171,8 @@ __device__ __forceinline__ void scan_grain(const Geo& G, int grain, float px, fl
 /* Lower bound of the distance from p to every box face and to every
    candidate surface of the grain (planes bound polygons from below, the
    infinite cylinder bounds the clipped one). */
-__device__ __forceinline__ float safety(const Geo& G, int grain, float px, float py, float pz,
+template <class G_t>
+__device__ __forceinline__ float safety(const G_t& G, int grain, float px, float py, float pz,
                                         float X, float Y, float Z, float eps) {
   float d = fminf(fminf(fminf(px, X - px), fminf(py, Y - py)), fminf(pz, Z - pz));
   if (grain > 0) {
@@ -241,14 +254,15 @@ __device__ bool stage_blob(const float4* gblob, float4* sblob, int units, int* e
   return ok != 0;
 }
 
+template <bool SMEM>
 __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
-  extern __shared__ float4 sblob[];
-  Geo G;
+  Geo<SMEM> G;
   G.lay = gp.lay;
   G.base = gp.blob;
   if (threadIdx.x == 0) atomicMin(r.stats + 5, globaltimer());
-  if (gp.stage_smem) {
-    if (stage_blob(gp.blob, sblob, gp.lay.total, r.queue + 1)) G.base = sblob;
+  if (SMEM) {
+    /* on a timeout the block records the error and leaves: the host reports it */
+    if (!stage_blob(gp.blob, sblob, gp.lay.total, r.queue + 1)) return;
   }
   const int lane = threadIdx.x & 31;
   const float X = gp.box[0], Y = gp.box[1], Z = gp.box[2];
@@ -372,22 +386,21 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           nz[j] = st * sp;
           nf[j] = -lam * __logf(u23f(B[j].z));
         }
+        /* position relative to the ball centre along the four steps */
+        float wx = px - bx, wy = py - by, wz = pz - bz;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-          if (fast_more) {
-            const float qx = fmaf(fp, dx, px), qy = fmaf(fp, dy, py), qz = fmaf(fp, dz, pz);
-            const float ex = qx - bx, ey = qy - by, ez = qz - bz;
-            if (fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < br2) {
-              ++flight;
-              px = qx; py = qy; pz = qz;
-              dx = nx[j]; dy = ny[j]; dz = nz[j];
-              fp = nf[j];
-              ++k;
-            } else {
-              fast_more = false;
-            }
-          }
+          /* predicated: no branch per step */
+          const float qx = fmaf(fp, dx, wx), qy = fmaf(fp, dy, wy), qz = fmaf(fp, dz, wz);
+          const bool acc = fast_more && (fmaf(qx, qx, fmaf(qy, qy, qz * qz)) < br2);
+          flight += acc ? 1u : 0u;
+          k += acc ? 1 : 0;
+          wx = acc ? qx : wx; wy = acc ? qy : wy; wz = acc ? qz : wz;
+          dx = acc ? nx[j] : dx; dy = acc ? ny[j] : dy; dz = acc ? nz[j] : dz;
+          fp = acc ? nf[j] : fp;
+          fast_more = acc;
         }
+        px = bx + wx; py = by + wy; pz = bz + wz;
       }
       /* a lane that used up its fast steps waits for the next iteration;
          any other lane takes one flight with the full test now */
@@ -581,18 +594,23 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
 }  // namespace
 
 cudaError_t persistent_occupancy(int block, size_t smem, int* bps) {
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_persistent, block, smem);
+  if (smem > 0) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_persistent<true>, block, smem);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_persistent<false>, block, 0);
 }
 
 cudaError_t launch_persistent_fp32(const GeoF32& g, const RunF32& r, int grid, int block,
                                    size_t smem, cudaStream_t st) {
   if (block != kBlock) return cudaErrorInvalidConfiguration;
-  if (smem > 48 * 1024) {
-    cudaError_t e =
-        cudaFuncSetAttribute(k_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
+  if (g.stage_smem && smem > 0) {
+    if (smem > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(k_persistent<true>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+    }
+    k_persistent<true><<<grid, block, smem, st>>>(g, r);
+  } else {
+    k_persistent<false><<<grid, block, 0, st>>>(g, r);
   }
-  k_persistent<<<grid, block, smem, st>>>(g, r);
   return cudaGetLastError();
 }
 

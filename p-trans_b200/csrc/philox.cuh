@@ -21,16 +21,15 @@ __device__ __forceinline__ uint4 philox10(uint32_t c0, uint32_t c1, uint32_t c2,
   uint32_t k0 = k.k0, k1 = k.k1;
 #pragma unroll
   for (int r = 0; r < 10; ++r) {
-    const uint32_t lo0 = 0xD2511F53u * c0;
-    const uint32_t hi0 = __umulhi(0xD2511F53u, c0);
-    const uint32_t lo1 = 0xCD9E8D57u * c2;
-    const uint32_t hi1 = __umulhi(0xCD9E8D57u, c2);
-    const uint32_t n0 = hi1 ^ c1 ^ k0;
-    const uint32_t n2 = hi0 ^ c3 ^ k1;
+    /* one 32x32 -> 64-bit product per multiplier gives both halves */
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+    const uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+    const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0;
+    const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
     c0 = n0;
-    c1 = lo1;
+    c1 = (uint32_t)p1;
     c2 = n2;
-    c3 = lo0;
+    c3 = (uint32_t)p0;
     k0 += 0x9E3779B9u;
     k1 += 0xBB67AE85u;
   }
@@ -43,11 +42,11 @@ __device__ __forceinline__ double u52d(uint32_t a, uint32_t b) {
   return ((double)k + 0.5) * (1.0 / 4503599627370496.0);
 }
 
-/* (k + 0.5) * 2^-23 from the top 23 bits k of a: open interval (0,1).
+/* (k + 0.5) * 2^-23 from the low 23 bits k of a: open interval (0,1).
    Built from the bit pattern 1 + k 2^-23 minus (1 - 2^-24), which is exact
    and avoids the integer-to-float conversion pipe. */
 __device__ __forceinline__ float u23f(uint32_t a) {
-  return __uint_as_float((a >> 9) | 0x3f800000u) - 0.99999994039535522f;
+  return __uint_as_float((a & 0x007fffffu) | 0x3f800000u) - 0.99999994039535522f;
 }
 
 }  // namespace ptg
