@@ -206,7 +206,9 @@ typedef struct ptg_run {
   double temperature;       /* param%temperature [K] (tau rescale, heat capacity) */
   int32_t nbins;            /* per-frequency-bin outputs (0 = none)             */
   double bin_omega_min, bin_omega_max;   /* rad/s                               */
-  double scatter_scale;     /* multiplies intrinsic scattering rates (0 = 1)    */
+  double scatter_scale;     /* s: intrinsic rates times s, i.e. every mode's    */
+                            /* bulk MFP divided by s (0 = 1); grid MFPs are    */
+                            /* sampling points and do not change               */
 } ptg_run;
 
 /* Results of ptg_kappa.  Pointers are caller-owned outputs (NULL = skip). */
@@ -311,6 +313,33 @@ int ptg_kappa(ptg_handle* h, const ptg_run* run, ptg_kappa_out* out);
 int ptg_kappa_from_counts(const ptg_geometry* geom, const ptg_spectrum* spec,
                           const ptg_run* run, const uint64_t* counts,
                           ptg_kappa_out* out);
+
+/*
+ * Adjoint (path-reweighting) derivatives of kappa.  A forward pass of the
+ * persistent FP32 kernel records which samples leave through x+; a second
+ * pass re-generates exactly those trajectories from their Philox counters
+ * (no path is stored) and accumulates, with the weight dkappa/dT_task / np,
+ *   d log P / d p_k = sum over events on surface record k of 1/p_k for a
+ *                     specular choice and -1/(1-p_k) for a diffuse one,
+ *   d log P / d s   = (intrinsic events) - (path length) / lambda
+ * for the scale s of the intrinsic rates (PER_MODE; MATTHIESSEN and GRID add
+ * the analytic term of the bulk-MFP dependence of their kappa rule).
+ * Derivatives are per surface record of the built geometry; records with
+ * p = 0 or 1 get NaN (the estimator is biased at the end points).  Standard
+ * errors come from 8 interleaved sample batches.  At most 2^25 transmitted
+ * samples per call (PTG_ERR_UNSUPPORTED beyond).
+ */
+typedef struct ptg_adjoint_out {
+  double kappa, kappa_stderr;
+  double* dk_dp;            /* [nsurf] dkappa / d specularity of each record     */
+  double* dk_dp_stderr;     /* [nsurf]                                           */
+  double dk_dscale, dk_dscale_stderr;
+  uint64_t flights;         /* forward + replay free flights                     */
+  uint64_t replayed;        /* transmitted samples re-generated                  */
+  uint64_t mismatched;      /* replays that did not transmit again (expect 0)    */
+  double kernel_ms;         /* forward + replay transport time                   */
+} ptg_adjoint_out;
+int ptg_adjoint(ptg_handle* h, const ptg_run* run, ptg_adjoint_out* out);
 
 /* Statistics of the last transport call on h. */
 int ptg_last_stats(const ptg_handle* h, ptg_stats* st);

@@ -822,7 +822,7 @@ Task task_of(const orc_handle* h, const ptg_run* r, int64_t task) {
   if (r->kind_mfp == PTG_MFP_MATTHIESSEN) {
     t.lambda = BALLISTIC;
   } else if (r->kind_mfp == PTG_MFP_GRID) {
-    t.lambda = r->mfp_grid_nm[s] / scale;
+    t.lambda = r->mfp_grid_nm[s];
   } else {
     double tau_s = h->tau[m] * 1.0e-12 * (h->rtemp / r->temperature);
     t.lambda = tau_s * h->vel[m] * 1.0e9 / scale;
@@ -972,9 +972,10 @@ int orc_kappa_from_counts(orc_handle* h, const ptg_run* run, const uint64_t* cou
   std::vector<double> om(h->omega), wt(h->weight), ta(h->tau), ve(h->vel), mf(nm);
   std::vector<int64_t> perm(nm);
   for (int64_t m = 0; m < nm; ++m) perm[m] = m;
+  const double scale = (run->scatter_scale > 0.0) ? run->scatter_scale : 1.0;
   for (int64_t m = 0; m < nm; ++m) {
     ta[m] = ta[m] * 1.0e-12 * (h->rtemp / T);
-    mf[m] = ta[m] * ve[m];
+    mf[m] = ta[m] * ve[m] / scale;
   }
   double wsum = 0.0;
   for (int64_t m = 0; m < nm; ++m) wsum += wt[m];

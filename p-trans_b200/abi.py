@@ -119,6 +119,14 @@ class PtgStats(C.Structure):
     ]
 
 
+class PtgAdjointOut(C.Structure):
+    _fields_ = [
+        ("kappa", C.c_double), ("kappa_stderr", C.c_double), ("dk_dp", F64P), ("dk_dp_stderr", F64P),
+        ("dk_dscale", C.c_double), ("dk_dscale_stderr", C.c_double), ("flights", C.c_uint64),
+        ("replayed", C.c_uint64), ("mismatched", C.c_uint64), ("kernel_ms", C.c_double),
+    ]
+
+
 class PtgError(RuntimeError):
     def __init__(self, status: int, what: str = ""):
         self.status = status
@@ -160,6 +168,7 @@ SIGNATURES = {
                                         C.POINTER(PtgRun), U64P, C.POINTER(PtgKappaOut)]),
     "ptg_last_stats": (C.c_int, [C.c_void_p, C.POINTER(PtgStats)]),
     "ptg_replay_task": (C.c_int, [C.c_void_p, C.POINTER(PtgRun), C.c_int64, I32P, U32P, F64P]),
+    "ptg_adjoint": (C.c_int, [C.c_void_p, C.POINTER(PtgRun), C.POINTER(PtgAdjointOut)]),
     "ptg_transmission_noalloc": (C.c_int, [C.c_void_p, C.c_double, C.c_int32, C.c_int64, C.c_int32,
                                            C.c_int32, C.c_uint64, F64P]),
 }
@@ -498,6 +507,20 @@ class Handle:
         return {"kappa": out.kappa, "kappa_stderr": out.kappa_stderr, "bin_T": bt[: run.nbins],
                 "bin_T_stderr": be[: run.nbins], "emfp_nm": em, "transmit": tr, "counts": cn,
                 "flights": out.flights, "lost": out.lost, "samples": out.samples,
+                "kernel_ms": out.kernel_ms}
+
+    def adjoint(self, run: PtgRun) -> dict:
+        """ptg_adjoint: kappa and its path-reweighting derivatives with respect
+        to every surface record's specularity and the intrinsic-rate scale."""
+        ns = self._geom.nsurf
+        out = PtgAdjointOut()
+        d = np.zeros(ns)
+        e = np.zeros(ns)
+        out.dk_dp, out.dk_dp_stderr = _ptr(d, C.c_double), _ptr(e, C.c_double)
+        _check(self.lib.ptg_adjoint(self.h, C.byref(run), C.byref(out)), "ptg_adjoint")
+        return {"kappa": out.kappa, "kappa_stderr": out.kappa_stderr, "dk_dp": d, "dk_dp_stderr": e,
+                "dk_dscale": out.dk_dscale, "dk_dscale_stderr": out.dk_dscale_stderr,
+                "flights": out.flights, "replayed": out.replayed, "mismatched": out.mismatched,
                 "kernel_ms": out.kernel_ms}
 
     def stats(self) -> dict:

@@ -77,11 +77,14 @@ struct ptg_handle {
   /* reduction */
   DevBuf red_coef, red_K, red_W, red_mfp, red_bin, red_grid, red_tc, red_kv, red_bw, red_bv,
       red_emfp, red_trans, red_result;
+  /* adjoint: list of transmitted samples, per-sample weights, accumulators */
+  DevBuf adj_list, adj_w, adj_acc;
+  unsigned long long list_n = 0, mismatch = 0;
   ~ptg_handle() {
     for (DevBuf* b : owned) { b->release(); delete b; }
     DevBuf* all[] = {&blob, &task, &chunk, &counts, &lost, &stats, &queue, &red_coef, &red_K,
                      &red_W, &red_mfp, &red_bin, &red_grid, &red_tc, &red_kv, &red_bw, &red_bv,
-                     &red_emfp, &red_trans, &red_result};
+                     &red_emfp, &red_trans, &red_result, &adj_list, &adj_w, &adj_acc};
     for (DevBuf* b : all) b->release();
     for (cudaEvent_t e : ev) if (e) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);
@@ -292,6 +295,14 @@ struct Transport {
   int32_t stream = 0;
   int32_t precision = PTG_PREC_FP32;
   const std::vector<ptg::TaskHost>* tasks = nullptr;
+  /* persistent kernel mode and the adjoint buffers */
+  int mode = ptg::MODE_FORWARD;
+  unsigned long long* tlist = nullptr;
+  unsigned long long tlist_cap = 0;
+  const unsigned long long* alist = nullptr;
+  long long alist_n = 0;
+  const float* wsample = nullptr;
+  double* adj = nullptr;
 };
 
 int run_transport(ptg_handle* h, const Transport& T) {
@@ -299,11 +310,11 @@ int run_transport(ptg_handle* h, const Transport& T) {
   CU(cudaSetDevice(h->device));
   CU(h->counts.ensure(sizeof(unsigned long long) * ntask));
   CU(h->lost.ensure(sizeof(unsigned long long) * ntask));
-  CU(h->stats.ensure(sizeof(unsigned long long) * 10));
+  CU(h->stats.ensure(sizeof(unsigned long long) * 16));
   CU(h->queue.ensure(sizeof(int) * 4));
   CU(cudaMemsetAsync(h->counts.p, 0, sizeof(unsigned long long) * ntask, h->stream));
   CU(cudaMemsetAsync(h->lost.p, 0, sizeof(unsigned long long) * ntask, h->stream));
-  CU(cudaMemsetAsync(h->stats.p, 0, sizeof(unsigned long long) * 10, h->stream));
+  CU(cudaMemsetAsync(h->stats.p, 0, sizeof(unsigned long long) * 16, h->stream));
   /* stats[5], stats[6] collect minima of the global timer */
   CU(cudaMemsetAsync(h->stats.as<unsigned long long>() + 5, 0xFF, sizeof(unsigned long long) * 2,
                      h->stream));
@@ -401,15 +412,23 @@ int run_transport(ptg_handle* h, const Transport& T) {
     r.lost = h->lost.as<unsigned long long>();
     r.stats = h->stats.as<unsigned long long>();
     r.queue = h->queue.as<int>();
+    r.tlist = T.tlist;
+    r.tlist_cap = T.tlist_cap;
+    r.alist = T.alist;
+    r.alist_n = T.alist_n;
+    r.wsample = T.wsample;
+    r.adj = T.adj;
+    r.nsurf = h->geom.nsurf();
     const int block = 256;
     const size_t smem = h->g32.stage_smem ? h->blob_bytes : 0;
     int bps = 0;
-    CU(ptg::persistent_occupancy(block, smem, &bps));
+    CU(ptg::persistent_occupancy(block, smem, &bps, T.mode));
     if (h->opt.blocks_per_sm > 0 && h->opt.blocks_per_sm < bps) bps = h->opt.blocks_per_sm;
     if (bps < 1) bps = 1;
     const int grid = h->num_sms * bps;
     CU(cudaEventRecord(h->ev[0], h->stream));
-    if (r.nchunk > 0) CU(ptg::launch_persistent_fp32(h->g32, r, grid, block, smem, h->stream));
+    const bool work = (T.mode == ptg::MODE_ADJOINT) ? T.alist_n > 0 : r.nchunk > 0;
+    if (work) CU(ptg::launch_persistent_fp32(h->g32, r, grid, block, smem, h->stream, T.mode));
     CU(cudaEventRecord(h->ev[1], h->stream));
     h->last.grid = grid;
     h->last.block = block;
@@ -419,7 +438,7 @@ int run_transport(ptg_handle* h, const Transport& T) {
 }
 
 int finish_stats(ptg_handle* h) {
-  unsigned long long st[10];
+  unsigned long long st[16];
   int qerr[4];
   CU(cudaMemcpyAsync(st, h->stats.p, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
   CU(cudaMemcpyAsync(qerr, h->queue.p, sizeof(qerr), cudaMemcpyDeviceToHost, h->stream));
@@ -435,6 +454,8 @@ int finish_stats(ptg_handle* h) {
   h->last.max_traj_flights = st[4];
   h->last.full_flights = st[8];
   h->last.safe_balls = st[9];
+  h->list_n = st[10];
+  h->mismatch = st[11];
   if (st[5] != ~0ull && st[7] >= st[5]) {
     const unsigned long long drain = st[6] != ~0ull ? st[6] : st[7];
     h->last.drain_ms = (double)(drain - st[5]) * 1e-6;
@@ -460,6 +481,133 @@ int check_lost(ptg_handle* h) {
 }  // namespace
 
 namespace ptg {
+
+/* effectiveMFP + the kappa sum of fileoutput from transmitted counts (host
+   FP64), with the binomial standard errors and per-bin transmission; wtask
+   (optional) receives d kappa / d T_task for every task and dk_ds_an the
+   analytic part of d kappa / d s (the bulk-MFP dependence of the
+   Matthiessen and grid-interpolation rules). */
+int assemble_host(const ptg::SpecSoA& S, const ptg_run* run, double box_x, const uint64_t* counts,
+                  ptg_kappa_out* out, std::vector<double>* wtask, double* dk_ds_an) {
+  const int ns = run->kind_mfp == PTG_MFP_GRID ? run->nmfp : 1;
+  const int na = run->nangle;
+  const int64_t nm = S.nmode();
+  ptg::ModeConst mc;
+  ptg::mode_constants(S, run, &mc);
+  std::vector<double> coef;
+  double dS = 0.0;
+  ptg::simpson_weights(na, box_x, &coef, &dS);
+  const double tnorm = 0.75 * box_x;
+  const double np = (double)run->np;
+  double kappa = 0.0, kvar = 0.0, dks = 0.0;
+  const double scale = (run->scatter_scale > 0.0) ? run->scatter_scale : 1.0;
+  if (wtask) wtask->assign((size_t)nm * ns * (na - 1), 0.0);
+  std::vector<double> sw(run->nbins, 0.0), swt(run->nbins, 0.0), sv(run->nbins, 0.0);
+  std::vector<double> Sv(ns), Vv(ns), dE(ns);
+  for (int64_t m = 0; m < nm; ++m) {
+    for (int s = 0; s < ns; ++s) {
+      double acc = 0.0, var = 0.0;
+      for (int ia = 0; ia < na - 1; ++ia) {
+        const int64_t task = m + nm * (s + (int64_t)ns * ia);
+        const double tr = (double)counts[task] / np;
+        acc += coef[ia] * tr;
+        var += coef[ia] * coef[ia] * (tr * (1.0 - tr) / np);
+        if (out->transmit) out->transmit[task] = tr;
+      }
+      if (out->transmit) out->transmit[m + nm * (s + (int64_t)ns * (na - 1))] = 0.0;
+      Sv[s] = acc * dS;
+      Vv[s] = var * dS * dS;
+      dE[s] = 0.0;
+    }
+    const double mf = mc.mfp_m[m];
+    double E;
+    if (run->kind_mfp == PTG_MFP_MATTHIESSEN) {
+      if (mf == 0.0) { E = Sv[0] * 1.0e-9; dE[0] = 1.0e-9; }
+      else {
+        const double sm = Sv[0] * 1.0e-9;
+        E = 1.0 / (1.0 / mf + 1.0 / sm);
+        dE[0] = (sm > 0.0) ? 1.0e-9 * (E * E) / (sm * sm) : 1.0e-9;
+      }
+    } else if (run->kind_mfp == PTG_MFP_PER_MODE) {
+      E = Sv[0] * 1.0e-9;
+      dE[0] = 1.0e-9;
+    } else {
+      const double* g = run->mfp_grid_nm;
+      if (mf < g[0] * 1.0e-9) {
+        E = Sv[0] * 1.0e-9 * mf / (g[0] * 1.0e-9);
+        dE[0] = 1.0e-9 * mf / (g[0] * 1.0e-9);
+      } else if (mf > g[ns - 1] * 1.0e-9) {
+        E = Sv[ns - 1] * 1.0e-9;
+        dE[ns - 1] = 1.0e-9;
+      } else {
+        E = Sv[ns - 1] * 1.0e-9;
+        dE[ns - 1] = 1.0e-9;
+        for (int s = 0; s < ns - 1; ++s) {
+          if (g[s] * 1.0e-9 <= mf && mf < g[s + 1] * 1.0e-9) {
+            const double ip = (mf - g[s] * 1.0e-9) / ((g[s + 1] - g[s]) * 1.0e-9);
+            E = Sv[s] * 1.0e-9 * (1.0 - ip) + Sv[s + 1] * 1.0e-9 * ip;
+            dE[ns - 1] = 0.0;
+            dE[s] = 1.0e-9 * (1.0 - ip);
+            dE[s + 1] = 1.0e-9 * ip;
+            break;
+          }
+        }
+      }
+    }
+    kappa += mc.K[m] * E;
+    for (int s = 0; s < ns; ++s) {
+      const double gk = mc.K[m] * dE[s];
+      kvar += gk * gk * Vv[s];
+      if (wtask)
+        for (int ia = 0; ia < na - 1; ++ia)
+          (*wtask)[m + nm * (s + (int64_t)ns * ia)] = gk * dS * coef[ia];
+    }
+    /* d E / d s through the bulk MFP mf = MFP0 / s */
+    if (run->kind_mfp == PTG_MFP_MATTHIESSEN && mf > 0.0) {
+      dks += mc.K[m] * (-(E * E) / (mf * scale));
+    } else if (run->kind_mfp == PTG_MFP_GRID) {
+      const double* g = run->mfp_grid_nm;
+      double dEdm = 0.0;
+      if (mf < g[0] * 1.0e-9) {
+        dEdm = Sv[0] / g[0];
+      } else {
+        for (int s = 0; s < ns - 1; ++s)
+          if (g[s] * 1.0e-9 <= mf && mf < g[s + 1] * 1.0e-9) {
+            dEdm = (Sv[s + 1] - Sv[s]) / (g[s + 1] - g[s]);
+            break;
+          }
+      }
+      dks += mc.K[m] * dEdm * (-mf / scale);
+    }
+    if (out->emfp_nm) out->emfp_nm[m] = E * 1.0e9;
+    if (run->nbins > 0 && mc.bin[m] >= 0) {
+      double tm, vm = 0.0;
+      if (run->kind_mfp == PTG_MFP_MATTHIESSEN) {
+        tm = Sv[0] / tnorm;
+        vm = Vv[0] / (tnorm * tnorm);
+      } else {
+        tm = E * 1.0e9 / tnorm;
+        for (int s = 0; s < ns; ++s) {
+          const double gk = dE[s] * 1.0e9 / tnorm;
+          vm += gk * gk * Vv[s];
+        }
+      }
+      const int b = mc.bin[m];
+      sw[b] += mc.W[m];
+      swt[b] += mc.W[m] * tm;
+      sv[b] += mc.W[m] * mc.W[m] * vm;
+    }
+  }
+  out->kappa = kappa;
+  out->kappa_stderr = sqrt(kvar);
+  if (dk_ds_an) *dk_ds_an = dks;
+  for (int b = 0; b < run->nbins; ++b) {
+    if (out->bin_T) out->bin_T[b] = sw[b] > 0 ? swt[b] / sw[b] : 0.0;
+    if (out->bin_T_stderr) out->bin_T_stderr[b] = sw[b] > 0 ? sqrt(sv[b]) / sw[b] : 0.0;
+  }
+  return PTG_OK;
+}
+
 
 int handle_noalloc_view(ptg_handle* h, NoallocView* v) {
   if (!h || !v) return PTG_ERR_INVALID;
@@ -718,99 +866,110 @@ int ptg_kappa_from_counts(const ptg_geometry* geom, const ptg_spectrum* spec, co
   std::string why;
   if (ptg::copy_spectrum(spec, &S, &why) != PTG_OK) return PTG_ERR_INVALID;
   if (!ptg::run_valid(S, run, &why)) return PTG_ERR_INVALID;
+  return ptg::assemble_host(S, run, geom->box[0], counts, out, nullptr, nullptr);
+}
+
+int ptg_adjoint(ptg_handle* h, const ptg_run* run, ptg_adjoint_out* out) {
+  if (!h || !run || !out) return PTG_ERR_INVALID;
+  std::string why;
+  if (!ptg::run_valid(h->spec, run, &why)) { h->last_error = why; return PTG_ERR_INVALID; }
   const int ns = run->kind_mfp == PTG_MFP_GRID ? run->nmfp : 1;
-  const int na = run->nangle;
-  const int64_t nm = S.nmode();
-  ptg::ModeConst mc;
-  ptg::mode_constants(S, run, &mc);
-  std::vector<double> coef;
-  double dS = 0.0;
-  ptg::simpson_weights(na, geom->box[0], &coef, &dS);
-  const double tnorm = 0.75 * geom->box[0];
-  const double np = (double)run->np;
-  double kappa = 0.0, kvar = 0.0;
-  std::vector<double> sw(run->nbins, 0.0), swt(run->nbins, 0.0), sv(run->nbins, 0.0);
-  std::vector<double> Sv(ns), Vv(ns), dE(ns);
-  for (int64_t m = 0; m < nm; ++m) {
-    for (int s = 0; s < ns; ++s) {
-      double acc = 0.0, var = 0.0;
-      for (int ia = 0; ia < na - 1; ++ia) {
-        const int64_t task = m + nm * (s + (int64_t)ns * ia);
-        const double tr = (double)counts[task] / np;
-        acc += coef[ia] * tr;
-        var += coef[ia] * coef[ia] * (tr * (1.0 - tr) / np);
-        if (out->transmit) out->transmit[task] = tr;
-      }
-      if (out->transmit) out->transmit[m + nm * (s + (int64_t)ns * (na - 1))] = 0.0;
-      Sv[s] = acc * dS;
-      Vv[s] = var * dS * dS;
-      dE[s] = 0.0;
+  if (ns > 64) return PTG_ERR_UNSUPPORTED;
+  std::vector<ptg::TaskHost> tasks;
+  ptg::run_tasks(h->spec, run, &tasks);
+  const int64_t ntask = (int64_t)tasks.size();
+  const int nsurf = h->geom.nsurf();
+  const unsigned long long cap = 1ull << 25;
+  CU(cudaSetDevice(h->device));
+  /* 1. forward pass that lists the samples leaving through x+ */
+  Transport T;
+  T.ntask = ntask;
+  T.np = run->np;
+  T.np_local = np_local_of(run->np, run->rank, run->nranks);
+  if (T.np_local > 2147483647LL) return PTG_ERR_INVALID;
+  T.rank = run->rank;
+  T.nranks = run->nranks;
+  T.seed = run->seed;
+  T.stream = run->stream;
+  T.precision = PTG_PREC_FP32;
+  T.tasks = &tasks;
+  T.mode = ptg::MODE_LIST;
+  const unsigned long long total = (unsigned long long)ntask * (unsigned long long)T.np_local;
+  T.tlist_cap = total < cap ? total : cap;
+  CU(h->adj_list.ensure(sizeof(unsigned long long) * (T.tlist_cap ? T.tlist_cap : 1)));
+  T.tlist = h->adj_list.as<unsigned long long>();
+  int st = run_transport(h, T);
+  if (st != PTG_OK) return st;
+  std::vector<uint64_t> counts(ntask);
+  CU(cudaMemcpyAsync(counts.data(), h->counts.p, sizeof(uint64_t) * ntask, cudaMemcpyDeviceToHost,
+                     h->stream));
+  st = finish_stats(h);
+  if (st != PTG_OK) return st;
+  const double fwd_ms = h->last.kernel_ms;
+  const uint64_t fwd_flights = h->last.flights;
+  const unsigned long long nlist = h->list_n;
+  if (nlist > T.tlist_cap) { h->last_error = "more than 2^25 transmitted samples"; return PTG_ERR_UNSUPPORTED; }
+  /* 2. kappa and d kappa / d T_task on the host */
+  ptg_kappa_out ko;
+  memset(&ko, 0, sizeof(ko));
+  std::vector<double> wtask;
+  double dks_an = 0.0;
+  st = ptg::assemble_host(h->spec, run, h->geom.box[0], counts.data(), &ko, &wtask, &dks_an);
+  if (st != PTG_OK) return st;
+  std::vector<float> wsample(ntask);
+  for (int64_t t = 0; t < ntask; ++t) wsample[t] = (float)(wtask[t] / (double)run->np);
+  CU(h->adj_w.ensure(sizeof(float) * ntask));
+  CU(cudaMemcpyAsync(h->adj_w.p, wsample.data(), sizeof(float) * ntask, cudaMemcpyHostToDevice,
+                     h->stream));
+  const size_t nacc = (size_t)ptg::kAdjBatches * (nsurf + 1);
+  CU(h->adj_acc.ensure(sizeof(double) * nacc));
+  CU(cudaMemsetAsync(h->adj_acc.p, 0, sizeof(double) * nacc, h->stream));
+  /* 3. replay of the listed samples with the score accumulation */
+  T.mode = ptg::MODE_ADJOINT;
+  T.tlist = nullptr;
+  T.tlist_cap = 0;
+  T.alist = h->adj_list.as<const unsigned long long>();
+  T.alist_n = (long long)nlist;
+  T.wsample = h->adj_w.as<const float>();
+  T.adj = h->adj_acc.as<double>();
+  st = run_transport(h, T);
+  if (st != PTG_OK) return st;
+  std::vector<double> acc(nacc);
+  CU(cudaMemcpyAsync(acc.data(), h->adj_acc.p, sizeof(double) * nacc, cudaMemcpyDeviceToHost,
+                     h->stream));
+  st = finish_stats(h);
+  if (st != PTG_OK) return st;
+  /* 4. batch sums and standard errors */
+  const int B = ptg::kAdjBatches;
+  auto reduce = [&](int col, double* mean_total, double* se) {
+    double sum = 0.0, sq = 0.0;
+    for (int b = 0; b < B; ++b) sum += acc[(size_t)b * (nsurf + 1) + col];
+    const double mb = sum / B;
+    for (int b = 0; b < B; ++b) {
+      const double d = acc[(size_t)b * (nsurf + 1) + col] - mb;
+      sq += d * d;
     }
-    const double mf = mc.mfp_m[m];
-    double E;
-    if (run->kind_mfp == PTG_MFP_MATTHIESSEN) {
-      if (mf == 0.0) { E = Sv[0] * 1.0e-9; dE[0] = 1.0e-9; }
-      else {
-        const double sm = Sv[0] * 1.0e-9;
-        E = 1.0 / (1.0 / mf + 1.0 / sm);
-        dE[0] = (sm > 0.0) ? 1.0e-9 * (E * E) / (sm * sm) : 1.0e-9;
-      }
-    } else if (run->kind_mfp == PTG_MFP_PER_MODE) {
-      E = Sv[0] * 1.0e-9;
-      dE[0] = 1.0e-9;
-    } else {
-      const double* g = run->mfp_grid_nm;
-      if (mf < g[0] * 1.0e-9) {
-        E = Sv[0] * 1.0e-9 * mf / (g[0] * 1.0e-9);
-        dE[0] = 1.0e-9 * mf / (g[0] * 1.0e-9);
-      } else if (mf > g[ns - 1] * 1.0e-9) {
-        E = Sv[ns - 1] * 1.0e-9;
-        dE[ns - 1] = 1.0e-9;
-      } else {
-        E = Sv[ns - 1] * 1.0e-9;
-        dE[ns - 1] = 1.0e-9;
-        for (int s = 0; s < ns - 1; ++s) {
-          if (g[s] * 1.0e-9 <= mf && mf < g[s + 1] * 1.0e-9) {
-            const double ip = (mf - g[s] * 1.0e-9) / ((g[s + 1] - g[s]) * 1.0e-9);
-            E = Sv[s] * 1.0e-9 * (1.0 - ip) + Sv[s + 1] * 1.0e-9 * ip;
-            dE[ns - 1] = 0.0;
-            dE[s] = 1.0e-9 * (1.0 - ip);
-            dE[s + 1] = 1.0e-9 * ip;
-            break;
-          }
-        }
-      }
-    }
-    kappa += mc.K[m] * E;
-    for (int s = 0; s < ns; ++s) {
-      const double gk = mc.K[m] * dE[s];
-      kvar += gk * gk * Vv[s];
-    }
-    if (out->emfp_nm) out->emfp_nm[m] = E * 1.0e9;
-    if (run->nbins > 0 && mc.bin[m] >= 0) {
-      double tm, vm = 0.0;
-      if (run->kind_mfp == PTG_MFP_MATTHIESSEN) {
-        tm = Sv[0] / tnorm;
-        vm = Vv[0] / (tnorm * tnorm);
-      } else {
-        tm = E * 1.0e9 / tnorm;
-        for (int s = 0; s < ns; ++s) {
-          const double gk = dE[s] * 1.0e9 / tnorm;
-          vm += gk * gk * Vv[s];
-        }
-      }
-      const int b = mc.bin[m];
-      sw[b] += mc.W[m];
-      swt[b] += mc.W[m] * tm;
-      sv[b] += mc.W[m] * mc.W[m] * vm;
-    }
+    *mean_total = sum;
+    *se = sqrt((double)B * sq / (B - 1));
+  };
+  for (int k = 0; k < nsurf; ++k) {
+    double v, e;
+    reduce(k, &v, &e);
+    const double p = h->geom.specularity[k];
+    const bool interior = p > 0.0 && p < 1.0;
+    if (out->dk_dp) out->dk_dp[k] = interior ? v : NAN;
+    if (out->dk_dp_stderr) out->dk_dp_stderr[k] = interior ? e : NAN;
   }
-  out->kappa = kappa;
-  out->kappa_stderr = sqrt(kvar);
-  for (int b = 0; b < run->nbins; ++b) {
-    if (out->bin_T) out->bin_T[b] = sw[b] > 0 ? swt[b] / sw[b] : 0.0;
-    if (out->bin_T_stderr) out->bin_T_stderr[b] = sw[b] > 0 ? sqrt(sv[b]) / sw[b] : 0.0;
-  }
+  double vs, es;
+  reduce(nsurf, &vs, &es);
+  out->dk_dscale = (run->kind_mfp == PTG_MFP_PER_MODE ? vs : 0.0) + dks_an;
+  out->dk_dscale_stderr = run->kind_mfp == PTG_MFP_PER_MODE ? es : 0.0;
+  out->kappa = ko.kappa;
+  out->kappa_stderr = ko.kappa_stderr;
+  out->flights = fwd_flights + h->last.flights;
+  out->replayed = nlist;
+  out->mismatched = h->mismatch;
+  out->kernel_ms = fwd_ms + h->last.kernel_ms;
   return PTG_OK;
 }
 

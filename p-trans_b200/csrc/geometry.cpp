@@ -543,7 +543,7 @@ void run_tasks(const SpecSoA& s, const ptg_run* r, std::vector<TaskHost>* tasks)
     if (r->kind_mfp == PTG_MFP_MATTHIESSEN) {
       th.lambda = 1.0e10;
     } else if (r->kind_mfp == PTG_MFP_GRID) {
-      th.lambda = r->mfp_grid_nm[sg] / scale;
+      th.lambda = r->mfp_grid_nm[sg];   /* grid points are sampling points */
     } else {
       const double tau_s = s.tau[m] * 1.0e-12 * (s.rtemp / r->temperature);
       th.lambda = tau_s * s.vel[m] * 1.0e9 / scale;
@@ -579,7 +579,8 @@ void mode_constants(const SpecSoA& s, const ptg_run* r, ModeConst* mc) {
     if (x <= 1.0e-10) cap = KB;
     else { double q = (x / 2) / sinh(x / 2); cap = KB * (q * q); }
     const double tau = s.tau[m] * 1.0e-12 * (s.rtemp / T);
-    mc->mfp_m[m] = tau * s.vel[m];
+    const double scale = (r->scatter_scale > 0.0) ? r->scatter_scale : 1.0;
+    mc->mfp_m[m] = tau * s.vel[m] / scale;
     mc->K[m] = cap * s.weight[m] * s.vel[m] / 3 / s.vol / nqfbz;
     mc->W[m] = cap * s.weight[m] * s.vel[m];
     if (r->nbins > 0) {

@@ -116,12 +116,27 @@ struct RunF32 {
      flights taken with the intersection test, safe balls built */
   unsigned long long* stats;
   int* queue;                 /* [0] next chunk, [1] error flags */
+  /* adjoint support */
+  unsigned long long* tlist;  /* mode 1: sample ids of transmitted phonons         */
+  unsigned long long tlist_cap;
+  const unsigned long long* alist;  /* mode 2: sample ids to replay               */
+  long long alist_n;
+  const float* wsample;       /* mode 2: d kappa / d T_task / np, per task         */
+  double* adj;                /* mode 2: [kAdjBatches][nsurf + 1] accumulators     */
+  int nsurf;
 };
 
+/* Replays are split in this many interleaved batches (sample % kAdjBatches)
+   whose spread gives the standard error of the adjoint estimates. */
+constexpr int kAdjBatches = 8;
+/* kernel modes: forward, forward + list of transmitted samples, adjoint replay */
+enum { MODE_FORWARD = 0, MODE_LIST = 1, MODE_ADJOINT = 2 };
+
 cudaError_t launch_persistent_fp32(const GeoF32& g, const RunF32& r, int grid, int block,
-                                   size_t smem, cudaStream_t st);
+                                   size_t smem, cudaStream_t st, int mode = MODE_FORWARD);
 /* Residency of the persistent kernel for a block size and shared memory. */
-cudaError_t persistent_occupancy(int block, size_t smem, int* blocks_per_sm);
+cudaError_t persistent_occupancy(int block, size_t smem, int* blocks_per_sm,
+                                 int mode = MODE_FORWARD);
 
 /* ---------------- FP64 kappa reduction ---------------------------------- */
 

@@ -254,7 +254,11 @@ __device__ bool stage_blob(const float4* gblob, float4* sblob, int units, int* e
   return ok != 0;
 }
 
-template <bool SMEM>
+/* Shared-memory accumulators of the adjoint replay: [kAdjBatches][nsurf+1]
+   doubles when they fit, else the replay adds to global memory directly. */
+constexpr int kAdjSmemDoubles = 2048;
+
+template <bool SMEM, int MODE>
 __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   Geo<SMEM> G;
   G.lay = gp.lay;
@@ -268,6 +272,18 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   const float X = gp.box[0], Y = gp.box[1], Z = gp.box[2];
   const float eps = gp.eps;
   const Key2 key = {r.k0, r.k1};
+  /* adjoint replay: per-block accumulators */
+  __shared__ double adj_sh[MODE == MODE_ADJOINT ? kAdjSmemDoubles : 1];
+  const int adj_stride = r.nsurf + 1;
+  const bool adj_in_smem = (MODE == MODE_ADJOINT) && kAdjBatches * adj_stride <= kAdjSmemDoubles;
+  if (MODE == MODE_ADJOINT && adj_in_smem) {
+    for (int i = threadIdx.x; i < kAdjBatches * adj_stride; i += blockDim.x) adj_sh[i] = 0.0;
+    __syncthreads();
+  }
+  float adj_w = 0.0f, adj_len = 0.0f;   /* weight of the sample, path length */
+  unsigned adj_npp = 0;                 /* intrinsic events of the sample   */
+  int adj_b = 0;                        /* batch of the sample               */
+  unsigned long long my_mismatch = 0;
 
   /* warp-uniform chunk cursor */
   int ch_task = -1, ch_next = 0, ch_left = 0;
@@ -293,20 +309,41 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           int c = 0;
           if (lane == 0) c = atomicAdd(r.queue, 1);
           c = __shfl_sync(FULL, c, 0);
-          if (c >= r.nchunk) {
-            queue_done = true;
-            if (lane == 0) atomicMin(r.stats + 6, globaltimer());
-            break;
+          if (MODE == MODE_ADJOINT) {
+            /* the replay list in chunks of 32 sample ids */
+            if ((long long)c * 32 >= r.alist_n) {
+              queue_done = true;
+              if (lane == 0) atomicMin(r.stats + 6, globaltimer());
+              break;
+            }
+            ch_next = c * 32;
+            ch_left = (int)min((long long)32, r.alist_n - (long long)c * 32);
+          } else {
+            if (c >= r.nchunk) {
+              queue_done = true;
+              if (lane == 0) atomicMin(r.stats + 6, globaltimer());
+              break;
+            }
+            const int4 q = r.chunk[c];
+            ch_task = q.x; ch_next = q.y; ch_left = q.z;
           }
-          const int4 q = r.chunk[c];
-          ch_task = q.x; ch_next = q.y; ch_left = q.z;
         }
         const int take = min(__popc(idle), ch_left);
         const int rank = __popc(idle & lanemask_lt());
         if (((idle >> lane) & 1u) && rank < take) {
-          const int64_t p = (int64_t)r.rank + (int64_t)(ch_next + rank) * r.nranks;
-          const uint64_t sample = (uint64_t)ch_task * (uint64_t)r.np + (uint64_t)p;
-          task = ch_task;
+          uint64_t sample;
+          if (MODE == MODE_ADJOINT) {
+            sample = r.alist[ch_next + rank];
+            task = (int)(sample / (uint64_t)r.np);
+            adj_w = r.wsample[task];
+            adj_b = (int)(sample % kAdjBatches);
+            adj_len = 0.0f;
+            adj_npp = 0;
+          } else {
+            const int64_t p = (int64_t)r.rank + (int64_t)(ch_next + rank) * r.nranks;
+            sample = (uint64_t)ch_task * (uint64_t)r.np + (uint64_t)p;
+            task = ch_task;
+          }
           slo = (uint32_t)sample;
           shi = (uint32_t)(sample >> 32);
           const float4 T = r.task[task];
@@ -393,6 +430,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           /* predicated: no branch per step */
           const float qx = fmaf(fp, dx, wx), qy = fmaf(fp, dy, wy), qz = fmaf(fp, dz, wz);
           const bool acc = fast_more && (fmaf(qx, qx, fmaf(qy, qy, qz * qz)) < br2);
+          if (MODE == MODE_ADJOINT) {
+            adj_len += acc ? fp : 0.0f;
+            adj_npp += acc ? 1u : 0u;
+          }
           flight += acc ? 1u : 0u;
           k += acc ? 1 : 0;
           wx = acc ? qx : wx; wy = acc ? qy : wy; wz = acc ? qz : wz;
@@ -435,6 +476,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           const float u0 = u23f(R.x), u1 = u23f(R.y), u2 = u23f(R.z), u3 = u23f(R.w);
           if (fp < tb) {
             /* intrinsic scattering: isotropic direction, new free path */
+            if (MODE == MODE_ADJOINT) {
+              adj_len += fp;
+              adj_npp += 1u;
+            }
             px = fmaf(fp, dx, px);
             py = fmaf(fp, dy, py);
             pz = fmaf(fp, dz, pz);
@@ -455,6 +500,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             }
           } else {
             br2 = 0.0f;
+            if (MODE == MODE_ADJOINT) adj_len += tb;
             px = fmaf(tb, dx, px);
             py = fmaf(tb, dy, py);
             pz = fmaf(tb, dz, pz);
@@ -517,6 +563,17 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
               const float dn0 = fmaf(nx, dx, fmaf(ny, dy, nz * dz));
               const float on = dn0 < 0.0f ? -1.0f : 1.0f;
               bool transmitted = false;
+              if (MODE == MODE_ADJOINT) {
+                /* d log P / d p of the specular (1/p) or diffuse (-1/(1-p)) choice */
+                const float pk = C0.w;
+                if (pk > 0.0f && pk < 1.0f) {
+                  const double sc = (u0 <= pk) ? 1.0 / (double)pk : -1.0 / (1.0 - (double)pk);
+                  const double v = (double)adj_w * sc;
+                  const int idx = adj_b * adj_stride + sb;
+                  if (adj_in_smem) atomicAdd(&adj_sh[idx], v);
+                  else atomicAdd(&r.adj[idx], v);
+                }
+              }
               if (u0 <= C0.w) {
                 if (u1 <= thr) {
                   transmitted = true;
@@ -558,8 +615,35 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
     const bool fin = alive && end_side >= 0;
     const bool trans = fin && (end_side == 2 || (end_side == 0 && r.ref_quirks));
     const bool lostp = fin && end_side == 0;
-    warp_add_by_task(trans, task, r.counts);
-    warp_add_by_task(lostp, task, r.lost);
+    if (MODE != MODE_ADJOINT) {
+      warp_add_by_task(trans, task, r.counts);
+      warp_add_by_task(lostp, task, r.lost);
+    }
+    if (MODE == MODE_LIST) {
+      /* compact the ids of transmitted phonons (exit through x+) */
+      const bool put = fin && end_side == 2;
+      const unsigned m = __ballot_sync(FULL, put);
+      if (m) {
+        unsigned long long base = 0;
+        if (lane == __ffs(m) - 1) base = atomicAdd(r.stats + 10, (unsigned long long)__popc(m));
+        base = __shfl_sync(FULL, base, __ffs(m) - 1);
+        const unsigned long long at = base + __popc(m & lanemask_lt());
+        if (put && at < r.tlist_cap) r.tlist[at] = ((unsigned long long)shi << 32) | slo;
+      }
+    }
+    if (MODE == MODE_ADJOINT && fin) {
+      if (end_side == 2) {
+        /* d log P / d s of the exponential free paths at rate s / lambda */
+        const double v = (double)adj_w * ((double)adj_npp - (double)adj_len / (double)lam);
+        const int idx = adj_b * adj_stride + r.nsurf;
+        if (!isinf(lam)) {
+          if (adj_in_smem) atomicAdd(&adj_sh[idx], v);
+          else atomicAdd(&r.adj[idx], v);
+        }
+      } else {
+        my_mismatch += 1;
+      }
+    }
     if (fin) {
       my_flights += flight;
       my_lost += lostp ? 1 : 0;
@@ -579,6 +663,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
     v3 += __shfl_xor_sync(FULL, v3, o);
     v4 = max(v4, __shfl_xor_sync(FULL, v4, o));
   }
+  if (MODE == MODE_ADJOINT) {
+    for (int o = 16; o > 0; o >>= 1) my_mismatch += __shfl_xor_sync(FULL, my_mismatch, o);
+    if (lane == 0 && my_mismatch) atomicAdd(r.stats + 11, my_mismatch);
+  }
   if (lane == 0) {
     if (v0) atomicAdd(r.stats + 0, v0);
     if (v1) atomicAdd(r.stats + 1, v1);
@@ -589,29 +677,50 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
     if (v5) atomicAdd(r.stats + 8, v5);
     if (v6) atomicAdd(r.stats + 9, v6);
   }
+  if (MODE == MODE_ADJOINT && adj_in_smem) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < kAdjBatches * adj_stride; i += blockDim.x)
+      if (adj_sh[i] != 0.0) atomicAdd(&r.adj[i], adj_sh[i]);
+  }
 }
 
 }  // namespace
 
-cudaError_t persistent_occupancy(int block, size_t smem, int* bps) {
-  if (smem > 0) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_persistent<true>, block, smem);
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_persistent<false>, block, 0);
+template <int MODE>
+cudaError_t occupancy_mode(int block, size_t smem, int* bps) {
+  if (smem > 0)
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_persistent<true, MODE>, block, smem);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_persistent<false, MODE>, block, 0);
 }
 
-cudaError_t launch_persistent_fp32(const GeoF32& g, const RunF32& r, int grid, int block,
-                                   size_t smem, cudaStream_t st) {
-  if (block != kBlock) return cudaErrorInvalidConfiguration;
+template <int MODE>
+cudaError_t launch_mode(const GeoF32& g, const RunF32& r, int grid, int block, size_t smem,
+                        cudaStream_t st) {
   if (g.stage_smem && smem > 0) {
     if (smem > 48 * 1024) {
-      cudaError_t e = cudaFuncSetAttribute(k_persistent<true>,
+      cudaError_t e = cudaFuncSetAttribute(k_persistent<true, MODE>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (e != cudaSuccess) return e;
     }
-    k_persistent<true><<<grid, block, smem, st>>>(g, r);
+    k_persistent<true, MODE><<<grid, block, smem, st>>>(g, r);
   } else {
-    k_persistent<false><<<grid, block, 0, st>>>(g, r);
+    k_persistent<false, MODE><<<grid, block, 0, st>>>(g, r);
   }
   return cudaGetLastError();
+}
+
+cudaError_t persistent_occupancy(int block, size_t smem, int* bps, int mode) {
+  if (mode == MODE_LIST) return occupancy_mode<MODE_LIST>(block, smem, bps);
+  if (mode == MODE_ADJOINT) return occupancy_mode<MODE_ADJOINT>(block, smem, bps);
+  return occupancy_mode<MODE_FORWARD>(block, smem, bps);
+}
+
+cudaError_t launch_persistent_fp32(const GeoF32& g, const RunF32& r, int grid, int block,
+                                   size_t smem, cudaStream_t st, int mode) {
+  if (block != kBlock) return cudaErrorInvalidConfiguration;
+  if (mode == MODE_LIST) return launch_mode<MODE_LIST>(g, r, grid, block, smem, st);
+  if (mode == MODE_ADJOINT) return launch_mode<MODE_ADJOINT>(g, r, grid, block, smem, st);
+  return launch_mode<MODE_FORWARD>(g, r, grid, block, smem, st);
 }
 
 }  // namespace ptg

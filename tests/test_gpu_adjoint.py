@@ -1,0 +1,126 @@
+"""Adjoint (score-function) derivatives of kappa against central finite
+differences with common random numbers (CRN): the same seeds, so the two
+kappa evaluations share every trajectory until a specular decision u <= p
+flips.  Finite differences are taken with the GPU FP32 kernel and with the
+CPU FP64 oracle (the reference algorithm); agreement is required within
+3.5 combined standard errors, the errors coming from independent seeds."""
+import math
+
+import numpy as np
+import pytest
+
+from ptrans_b200 import abi as A
+from ptrans_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _film(p_hole=0.5):
+    return synth.film_with_holes(lx=300.0, ly=300.0, lz=145.0, nholes=3, radius=50.0, seed=4,
+                                 p_hole=p_hole, t_hole=0.0, p_z=0.3)
+
+
+def _with_spec(geom_np, records, delta):
+    d = {k: (np.array(v) if isinstance(v, np.ndarray) else v) for k, v in geom_np.items()}
+    d["specularity"] = geom_np["specularity"].copy()
+    d["specularity"][records] += delta
+    return d
+
+
+def _mean_se(x):
+    x = np.asarray(x, float)
+    return x.mean(), x.std(ddof=1) / math.sqrt(len(x))
+
+
+def test_adjoint_specularity_matches_finite_differences(orc):
+    model = _film()
+    spec = synth.spectrum(24, seed=3, mfp_lo=20e-9, mfp_hi=2e-6)
+    gb = A.GeomBuf(model)
+    g = gb.numpy()
+    holes = np.where(g["shape"] == A.SHAPE_CYLINDER)[0]
+    delta = 0.05
+    seeds = [11, 12, 13, 14, 15, 16]
+    np_ = 3000
+    adj, fd = [], []
+    gp = A.numpy_to_geometry(_with_spec(g, holes, +delta))
+    gm = A.numpy_to_geometry(_with_spec(g, holes, -delta))
+    with A.Handle(gb.view, spec) as h0, A.Handle(gp, spec) as hp, A.Handle(gm, spec) as hm:
+        for sd in seeds:
+            run = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=9, np_=np_, seed=sd)
+            a = h0.adjoint(run)
+            assert a["mismatched"] == 0
+            assert a["replayed"] > 0
+            adj.append(np.nansum(a["dk_dp"][holes]))
+            fd.append((hp.kappa(run)["kappa"] - hm.kappa(run)["kappa"]) / (2 * delta))
+    ma, sa = _mean_se(adj)
+    mf, sf = _mean_se(fd)
+    assert abs(ma - mf) < 3.5 * math.hypot(sa, sf), (ma, sa, mf, sf)
+    assert abs(ma) > 3 * sa  # a resolved, non-zero derivative
+
+    # the reference-side finite difference: CPU FP64 oracle with CRN
+    from oracle import oracle as O
+    op = O.Oracle(geometry=A.numpy_to_geometry(_with_spec(g, holes, +delta)), spectrum=spec)
+    om = O.Oracle(geometry=A.numpy_to_geometry(_with_spec(g, holes, -delta)), spectrum=spec)
+    ofd = []
+    for sd in seeds[:4]:
+        run = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=9, np_=1500, seed=sd)
+        cp, _, _ = op.counts(run)
+        cm, _, _ = om.counts(run)
+        ofd.append((op.kappa(run, cp)["kappa"] - om.kappa(run, cm)["kappa"]) / (2 * delta))
+    mo, so = _mean_se(ofd)
+    assert abs(ma - mo) < 3.5 * math.hypot(sa, so), (ma, sa, mo, so)
+
+
+def test_adjoint_scale_matches_finite_differences():
+    model = _film()
+    spec = synth.spectrum(24, seed=5, mfp_lo=10e-9, mfp_hi=1e-6)
+    gb = A.GeomBuf(model)
+    delta = 0.05
+    adj, fd = [], []
+    with A.Handle(gb.view, spec) as h:
+        for sd in [21, 22, 23, 24, 25, 26]:
+            kw = dict(kind_mfp=A.MFP_PER_MODE, nangle=9, np_=3000, seed=sd)
+            a = h.adjoint(A.make_run(**kw))
+            assert a["mismatched"] == 0
+            adj.append(a["dk_dscale"])
+            kp = h.kappa(A.make_run(scatter_scale=1 + delta, **kw))["kappa"]
+            km = h.kappa(A.make_run(scatter_scale=1 - delta, **kw))["kappa"]
+            fd.append((kp - km) / (2 * delta))
+    ma, sa = _mean_se(adj)
+    mf, sf = _mean_se(fd)
+    assert ma < 0  # stronger intrinsic scattering lowers kappa
+    assert abs(ma - mf) < 3.5 * math.hypot(sa, sf), (ma, sa, mf, sf)
+
+
+def test_matthiessen_scale_derivative_is_analytic():
+    """With the Matthiessen rule the transport is ballistic and the scale only
+    enters EMFP = 1/(s/MFP + 1/SEMFP): with common random numbers the finite
+    difference equals the analytic term."""
+    model = _film()
+    spec = synth.spectrum(16, seed=6)
+    gb = A.GeomBuf(model)
+    d = 1e-4
+    with A.Handle(gb.view, spec) as h:
+        kw = dict(kind_mfp=A.MFP_MATTHIESSEN, nangle=9, np_=500, seed=3)
+        a = h.adjoint(A.make_run(**kw))
+        kp = h.kappa(A.make_run(scatter_scale=1 + d, **kw))["kappa"]
+        km = h.kappa(A.make_run(scatter_scale=1 - d, **kw))["kappa"]
+    assert a["dk_dscale"] == pytest.approx((kp - km) / (2 * d), rel=1e-4)
+
+
+def test_adjoint_replays_exactly_the_transmitted_samples():
+    model = _film()
+    spec = synth.spectrum(12, seed=7)
+    gb = A.GeomBuf(model)
+    run = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=7, np_=700, seed=9)
+    with A.Handle(gb.view, spec) as h:
+        a = h.adjoint(run)
+        k = h.kappa(run, want_counts=True)
+    assert a["replayed"] == int(k["counts"].sum())
+    assert a["mismatched"] == 0
+    assert a["kappa"] == pytest.approx(k["kappa"], rel=1e-12)
+    # records never hit (brick interiors of void holes, x faces) have zero derivative
+    g = gb.numpy()
+    bricks = np.where((g["shape"] == A.SHAPE_CYLINDER) & (g["grain_inside"] != g["igrain_fill"]))[0]
+    assert np.all(a["dk_dp"][bricks] == 0.0)
+    assert np.isnan(a["dk_dp"][0]) or a["dk_dp"][0] == 0.0
