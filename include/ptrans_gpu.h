@@ -341,6 +341,37 @@ typedef struct ptg_adjoint_out {
 } ptg_adjoint_out;
 int ptg_adjoint(ptg_handle* h, const ptg_run* run, ptg_adjoint_out* out);
 
+/*
+ * Batched screening: many structures (each a built geometry with its own
+ * particle count, seed and stream) share one spectrum and run settings and
+ * run in ONE persistent kernel launch, replayed as a CUDA graph by
+ * ptg_batch_run.  Each geometry gets exactly the counts of its own ptg_kappa
+ * run with the same np, seed and stream (the FP32 kernel), i.e. the
+ * reference's RayTrace repeated per structure (src/RTMCphon.f90:3334-3433).
+ * The run's np, seed and stream are ignored (per item instead); the tables
+ * are built once, so a batch object is re-run without any host work.
+ */
+typedef struct ptg_batch ptg_batch;
+typedef struct ptg_batch_item {
+  const ptg_geometry* geom;
+  int64_t np;               /* particles per (mode, angle) task              */
+  uint64_t seed;
+  int32_t stream;
+} ptg_batch_item;
+typedef struct ptg_batch_out {
+  double* kappa;            /* [nitems]                                      */
+  double* kappa_stderr;     /* [nitems]                                      */
+  double* bin_T;            /* [nitems*nbins]                                */
+  double* bin_T_stderr;     /* [nitems*nbins]                                */
+  uint64_t* counts;         /* [nitems*ntask] or NULL                        */
+  uint64_t flights, lost, samples;
+  double graph_ms;          /* device time of the graph launch               */
+} ptg_batch_out;
+int ptg_batch_create(const ptg_batch_item* items, int32_t nitems, const ptg_spectrum* spec,
+                     const ptg_run* run, const ptg_options* opt, ptg_batch** out);
+int ptg_batch_run(ptg_batch* b, ptg_batch_out* out);
+void ptg_batch_destroy(ptg_batch* b);
+
 /* Statistics of the last transport call on h. */
 int ptg_last_stats(const ptg_handle* h, ptg_stats* st);
 

@@ -127,6 +127,17 @@ class PtgAdjointOut(C.Structure):
     ]
 
 
+class PtgBatchItem(C.Structure):
+    _fields_ = [("geom", C.POINTER(PtgGeometry)), ("np", C.c_int64), ("seed", C.c_uint64),
+                ("stream", C.c_int32)]
+
+
+class PtgBatchOut(C.Structure):
+    _fields_ = [("kappa", F64P), ("kappa_stderr", F64P), ("bin_T", F64P), ("bin_T_stderr", F64P),
+                ("counts", U64P), ("flights", C.c_uint64), ("lost", C.c_uint64),
+                ("samples", C.c_uint64), ("graph_ms", C.c_double)]
+
+
 class PtgError(RuntimeError):
     def __init__(self, status: int, what: str = ""):
         self.status = status
@@ -169,6 +180,10 @@ SIGNATURES = {
     "ptg_last_stats": (C.c_int, [C.c_void_p, C.POINTER(PtgStats)]),
     "ptg_replay_task": (C.c_int, [C.c_void_p, C.POINTER(PtgRun), C.c_int64, I32P, U32P, F64P]),
     "ptg_adjoint": (C.c_int, [C.c_void_p, C.POINTER(PtgRun), C.POINTER(PtgAdjointOut)]),
+    "ptg_batch_create": (C.c_int, [C.POINTER(PtgBatchItem), C.c_int32, C.POINTER(PtgSpectrum),
+                                   C.POINTER(PtgRun), C.POINTER(PtgOptions), C.POINTER(C.c_void_p)]),
+    "ptg_batch_run": (C.c_int, [C.c_void_p, C.POINTER(PtgBatchOut)]),
+    "ptg_batch_destroy": (None, [C.c_void_p]),
     "ptg_transmission_noalloc": (C.c_int, [C.c_void_p, C.c_double, C.c_int32, C.c_int64, C.c_int32,
                                            C.c_int32, C.c_uint64, F64P]),
 }
@@ -537,6 +552,66 @@ class Handle:
                                       _ptr(fl, C.c_uint32), _ptr(fp, C.c_double))
         _check(st, "ptg_replay_task")
         return es, fl, fp.reshape(npl, 3)
+
+
+class Batch:
+    """ptg_batch_*: many geometries in one persistent launch replayed as a CUDA graph."""
+
+    def __init__(self, geometries, nps, seeds, streams, spectrum: Spectrum, run: PtgRun, device=0, **opts):
+        self.lib = load_library()
+        n = len(geometries)
+        self._geoms = list(geometries)
+        items = (PtgBatchItem * n)()
+        for i, g in enumerate(self._geoms):
+            items[i].geom = C.pointer(g)
+            items[i].np, items[i].seed, items[i].stream = int(nps[i]), int(seeds[i]), int(streams[i])
+        self._items = items
+        self.n = n
+        self.nbins = run.nbins
+        self.ntask = ntask_of(spectrum.nmode, run)
+        self._cs = spectrum.to_c()
+        self._run = run
+        o = PtgOptions()
+        o.device = device
+        for k, v in opts.items():
+            setattr(o, k, v)
+        h = C.c_void_p()
+        _check(self.lib.ptg_batch_create(items, n, C.byref(self._cs), C.byref(run), C.byref(o), C.byref(h)),
+               "ptg_batch_create")
+        self.h = h
+
+    def run(self, want_counts=False) -> dict:
+        out = PtgBatchOut()
+        k = np.zeros(self.n)
+        ke = np.zeros(self.n)
+        bt = np.zeros(max(1, self.n * self.nbins))
+        be = np.zeros_like(bt)
+        cn = np.zeros(self.n * self.ntask, np.uint64) if want_counts else None
+        out.kappa, out.kappa_stderr = _ptr(k, C.c_double), _ptr(ke, C.c_double)
+        out.bin_T, out.bin_T_stderr = _ptr(bt, C.c_double), _ptr(be, C.c_double)
+        out.counts = _ptr(cn, C.c_uint64)
+        _check(self.lib.ptg_batch_run(self.h, C.byref(out)), "ptg_batch_run")
+        return {"kappa": k, "kappa_stderr": ke, "bin_T": bt[: self.n * self.nbins].reshape(self.n, self.nbins),
+                "bin_T_stderr": be[: self.n * self.nbins].reshape(self.n, self.nbins),
+                "counts": None if cn is None else cn.reshape(self.n, self.ntask),
+                "flights": out.flights, "lost": out.lost, "samples": out.samples, "graph_ms": out.graph_ms}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ptg_batch_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def kappa_from_counts(geometry: PtgGeometry, spectrum: Spectrum, run: PtgRun, counts: np.ndarray) -> dict:

@@ -118,8 +118,13 @@ inline float4 i4(int a, int b, int c, int d) {
   return v;
 }
 
-int build_blob(ptg_handle* h) {
-  const ptg::GeomSoA& G = h->geom;
+}  // namespace
+
+namespace ptg {
+
+/* The FP32 geometry blob of a built geometry (host copy) and its layout. */
+int blob_from_geometry(const GeomSoA& G, std::vector<float4>* out, BlobLayout* lay_out,
+                       std::string* why) {
   const int ns = G.nsurf(), ngt = G.ngrain_total();
   std::vector<float4> hot(2 * (size_t)ns), cold(3 * (size_t)ns), edges;
   std::vector<int> geom_id(ns);
@@ -165,7 +170,7 @@ int build_blob(ptg_handle* h) {
           wn[2] += a[0] * b[1] - a[1] * b[0];
         }
         double ln = sqrt(wn[0] * wn[0] + wn[1] * wn[1] + wn[2] * wn[2]);
-        if (!(ln > 0.0)) { h->last_error = "degenerate polygon"; return PTG_ERR_INVALID; }
+        if (!(ln > 0.0)) { *why = "degenerate polygon"; return PTG_ERR_INVALID; }
         for (int d = 0; d < 3; ++d) wn[d] /= ln;
         const int e0 = (int)edges.size();
         for (int i = 0; i < nv; ++i) {
@@ -231,6 +236,22 @@ int build_blob(ptg_handle* h) {
   memcpy(&blob[L.cand_begin], cb.data(), cb.size() * 4);
   if (!cand.empty()) memcpy(&blob[L.cand], cand.data(), cand.size() * 4);
   std::copy(start.begin(), start.end(), blob.begin() + L.start);
+  *out = std::move(blob);
+  *lay_out = L;
+  return PTG_OK;
+}
+
+}  // namespace ptg
+
+namespace {
+
+int build_blob(ptg_handle* h) {
+  const ptg::GeomSoA& G = h->geom;
+  std::vector<float4> blob;
+  ptg::BlobLayout L;
+  std::string why;
+  int st = ptg::blob_from_geometry(G, &blob, &L, &why);
+  if (st != PTG_OK) { h->last_error = why; return st; }
   h->blob_bytes = blob.size() * 16;
   CU(h->blob.ensure(h->blob_bytes));
   CU(cudaMemcpy(h->blob.p, blob.data(), h->blob_bytes, cudaMemcpyHostToDevice));

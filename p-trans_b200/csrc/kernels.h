@@ -96,6 +96,20 @@ struct GeoF32 {
   int stage_smem;      /* 1: copy the blob to shared memory (bulk copy)  */
 };
 
+/* One geometry of a batched launch (device table, read through the cache). */
+struct GeoEntry {
+  const float4* blob;
+  BlobLayout lay;
+  float box[3];
+  float scope[2];
+  float eps;
+  float fast_lambda_max;
+  int periodic_mask, kind_grain, igrain_fill, nmaterial;
+  long long np;                /* particles per task of this geometry        */
+  unsigned k0, k1, c1;         /* Philox key and stream word                 */
+  int task_base;               /* first global task of this geometry         */
+};
+
 /* Per task (FP32): lambda (inf = ballistic, <= 0 skipped), cos, sin, omega/max_omega */
 struct RunF32 {
   const float4* task;
@@ -124,6 +138,9 @@ struct RunF32 {
   const float* wsample;       /* mode 2: d kappa / d T_task / np, per task         */
   double* adj;                /* mode 2: [kAdjBatches][nsurf + 1] accumulators     */
   int nsurf;
+  /* batched launch: geometry table and the geometry of every global task */
+  const GeoEntry* geos;
+  const int* task_geo;
 };
 
 /* Replays are split in this many interleaved batches (sample % kAdjBatches)
@@ -134,6 +151,9 @@ enum { MODE_FORWARD = 0, MODE_LIST = 1, MODE_ADJOINT = 2 };
 
 cudaError_t launch_persistent_fp32(const GeoF32& g, const RunF32& r, int grid, int block,
                                    size_t smem, cudaStream_t st, int mode = MODE_FORWARD);
+/* Batched launch over several geometries (forward mode, geometry in global memory). */
+cudaError_t launch_persistent_batch(const RunF32& r, int grid, int block, cudaStream_t st);
+cudaError_t persistent_batch_occupancy(int block, int* blocks_per_sm);
 /* Residency of the persistent kernel for a block size and shared memory. */
 cudaError_t persistent_occupancy(int block, size_t smem, int* blocks_per_sm,
                                  int mode = MODE_FORWARD);
@@ -164,6 +184,19 @@ struct ReduceIn {
 };
 
 cudaError_t launch_kappa_reduce(const ReduceIn& in, cudaStream_t st);
+
+/* Batched reduction: the same spectrum for ngeo geometries whose counts are
+   stored one after another (ntask_per_geo each); per geometry np and box x.
+   result: [ngeo][2 + 3*nbins]. */
+struct ReduceBatchIn {
+  ReduceIn base;               /* counts, coef, K, W, mfp_m, bin, grid, nbins... */
+  int ngeo;
+  long long ntask_per_geo;
+  const double* np_geo;        /* [ngeo] */
+  const double* dS_geo;        /* [ngeo] */
+  const double* tnorm_geo;     /* [ngeo] */
+};
+cudaError_t launch_kappa_reduce_batch(const ReduceBatchIn& in, cudaStream_t st);
 
 }  // namespace ptg
 

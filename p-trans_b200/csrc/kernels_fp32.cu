@@ -39,6 +39,9 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
+#include <string.h>
+
+#include <type_traits>
 
 #include "kernels.h"
 #include "philox.cuh"
@@ -95,6 +98,29 @@ __device__ __forceinline__ void sincos2pi(float u, float* s, float* c) {
   *s = -__sinf(a);
   *c = -__cosf(a);
 }
+
+/* Geometry accessor of a batched launch: each lane reads the blob of its own
+   geometry from global memory. */
+struct GeoBatch {
+  const float4* base;
+  BlobLayout lay;
+  __device__ __forceinline__ float4 ld(int i) const { return __ldg(base + i); }
+  __device__ __forceinline__ float4 hotA(int s) const { return ld(lay.hot + 2 * s); }
+  __device__ __forceinline__ int4 hotB(int s) const {
+    const float4 v = ld(lay.hot + 2 * s + 1);
+    return make_int4(__float_as_int(v.x), __float_as_int(v.y), __float_as_int(v.z),
+                     __float_as_int(v.w));
+  }
+  __device__ __forceinline__ float4 cold(int s, int i) const { return ld(lay.cold + 3 * s + i); }
+  __device__ __forceinline__ float4 edge(int e) const { return ld(lay.edge + e); }
+  __device__ __forceinline__ int cand_begin(int g) const {
+    return __ldg(reinterpret_cast<const int*>(base + lay.cand_begin) + g);
+  }
+  __device__ __forceinline__ int cand(int k) const {
+    return __ldg(reinterpret_cast<const int*>(base + lay.cand) + k);
+  }
+  __device__ __forceinline__ float4 start(int i) const { return ld(lay.start + i); }
+};
 
 template <class G_t>
 __device__ __forceinline__ bool inside_edges(const G_t& G, int e0, int ne, float x, float y,
@@ -258,9 +284,9 @@ __device__ bool stage_blob(const float4* gblob, float4* sblob, int units, int* e
    doubles when they fit, else the replay adds to global memory directly. */
 constexpr int kAdjSmemDoubles = 2048;
 
-template <bool SMEM, int MODE>
+template <bool SMEM, int MODE, bool BATCH>
 __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
-  Geo<SMEM> G;
+  typename std::conditional<BATCH, GeoBatch, Geo<SMEM>>::type G;
   G.lay = gp.lay;
   G.base = gp.blob;
   if (threadIdx.x == 0) atomicMin(r.stats + 5, globaltimer());
@@ -269,9 +295,13 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
     if (!stage_blob(gp.blob, sblob, gp.lay.total, r.queue + 1)) return;
   }
   const int lane = threadIdx.x & 31;
-  const float X = gp.box[0], Y = gp.box[1], Z = gp.box[2];
-  const float eps = gp.eps;
-  const Key2 key = {r.k0, r.k1};
+  /* geometry and run scalars: kernel-wide, or per lane in a batched launch */
+  float X = gp.box[0], Y = gp.box[1], Z = gp.box[2];
+  float eps = gp.eps;
+  Key2 key = {r.k0, r.k1};
+  uint32_t c1 = r.c1;
+  int pmask = gp.periodic_mask, nmat = gp.nmaterial;
+  float flmax = r.fast_lambda_max;
   /* adjoint replay: per-block accumulators */
   __shared__ double adj_sh[MODE == MODE_ADJOINT ? kAdjSmemDoubles : 1];
   const int adj_stride = r.nsurf + 1;
@@ -339,6 +369,20 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             adj_b = (int)(sample % kAdjBatches);
             adj_len = 0.0f;
             adj_npp = 0;
+          } else if (BATCH) {
+            const int64_t p = (int64_t)r.rank + (int64_t)(ch_next + rank) * r.nranks;
+            task = ch_task;
+            const GeoEntry* e = r.geos + __ldg(r.task_geo + task);
+            G.base = e->blob;
+            G.lay = e->lay;
+            X = e->box[0]; Y = e->box[1]; Z = e->box[2];
+            eps = e->eps;
+            key.k0 = e->k0; key.k1 = e->k1;
+            c1 = e->c1;
+            pmask = e->periodic_mask;
+            nmat = e->nmaterial;
+            flmax = e->fast_lambda_max;
+            sample = (uint64_t)(task - e->task_base) * (uint64_t)e->np + (uint64_t)p;
           } else {
             const int64_t p = (int64_t)r.rank + (int64_t)(ch_next + rank) * r.nranks;
             sample = (uint64_t)ch_task * (uint64_t)r.np + (uint64_t)p;
@@ -351,10 +395,17 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           omr = T.w;
           /* emission: createRandomPosition / createRandomDirectionPhi,
              src/RTMCphon.f90:1845-1871; flight 0 draws y, z, phi, free path */
-          const uint4 R0 = philox10(0u, r.c1, slo, shi, key);
+          const uint4 R0 = philox10(0u, c1, slo, shi, key);
+          float sc0 = gp.scope[0], sc1 = gp.scope[1];
+          int kgrain = gp.kind_grain, gfill = gp.igrain_fill;
+          if (BATCH) {
+            const GeoEntry* e = r.geos + __ldg(r.task_geo + task);
+            sc0 = e->scope[0]; sc1 = e->scope[1];
+            kgrain = e->kind_grain; gfill = e->igrain_fill;
+          }
           px = 0.0f;
-          py = u23f(R0.x) * Y * gp.scope[0];
-          pz = u23f(R0.y) * Z * gp.scope[1];
+          py = u23f(R0.x) * Y * sc0;
+          pz = u23f(R0.y) * Z * sc1;
           float sp, cp;
           sincos2pi(u23f(R0.z), &sp, &cp);
           dx = T.y;
@@ -365,17 +416,17 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
              src/RTMCphon.f90:2100-2118) or the last incident polygon
              containing the point, else the fill grain (bricks, :2131-2163) */
           grain = 0;
-          if (gp.kind_grain == 1) {
+          if (kgrain == 1) {
             float dmin = 3.0e38f;
-            for (int i = 0; i < gp.lay.nstart; ++i) {
+            for (int i = 0; i < G.lay.nstart; ++i) {
               const float4 s = G.start(i);
               const float a = px - s.x, b = py - s.y, c = pz - s.z;
               const float d2 = fmaf(a, a, fmaf(b, b, c * c));
               if (d2 < dmin) { dmin = d2; grain = __float_as_int(s.w); }
             }
           } else {
-            grain = gp.igrain_fill;
-            for (int i = 0; i < gp.lay.nstart; ++i) {
+            grain = gfill;
+            for (int i = 0; i < G.lay.nstart; ++i) {
               const float4 s = G.start(i);
               const int sid = __float_as_int(s.x);
               const int4 B = G.hotB(sid);
@@ -410,7 +461,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
       while (fast_more && k < r.fast_steps && flight + 4u <= r.max_flights) {
         uint4 B[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) B[j] = philox10(flight + 1u + j, r.c1, slo, shi, key);
+        for (int j = 0; j < 4; ++j) B[j] = philox10(flight + 1u + j, c1, slo, shi, key);
         float nx[4], ny[4], nz[4], nf[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
@@ -456,7 +507,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
         } else {
           ++flight;
           ++my_full;
-          const uint4 R = philox10(flight, r.c1, slo, shi, key);
+          const uint4 R = philox10(flight, c1, slo, shi, key);
           /* slab exit of the box grain */
           float tb = 3.0e38f;
           int sb = -1;
@@ -493,7 +544,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             fp = -lam * __logf(u2);
             last_geom = -1;
             br2 = 0.0f;
-            if (r.fast_steps > 0 && lam < r.fast_lambda_max) {
+            if (r.fast_steps > 0 && lam < flmax) {
               const float d = safety(G, grain, px, py, pz, X, Y, Z, eps);
               ++my_balls;
               if (d > 0.0f) { bx = px; by = py; bz = pz; br2 = d * d; }
@@ -509,7 +560,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
               end_side = 1;
             } else if (sb == 1) {
               end_side = 2;
-            } else if (sb < 6 && ((gp.periodic_mask >> sb) & 1)) {
+            } else if (sb < 6 && ((pmask >> sb) & 1)) {
               const int ax = sb >> 1;
               const float L = ax == 1 ? Y : Z;
               const float sg = (sb & 1) ? -L : L;
@@ -525,10 +576,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
               if (kind == 1) {
                 thr = C1.w;
               } else if (kind == 2 || kind == 3) {
-                if (gp.nmaterial == 1) {
+                if (nmat == 1) {
                   thr = __frcp_rn(fmaf(C1.w, omr, 1.0f));
                 } else {
-                  const uint4 R2 = philox10(flight, r.c1 | 1u, slo, shi, key);
+                  const uint4 R2 = philox10(flight, c1 | 1u, slo, shi, key);
                   const float t11 = __frcp_rn(C1.w + 1.0f);
                   thr = fmaf(u23f(R2.x), 1.0f - t11, t11);
                 }
@@ -604,7 +655,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
               last_geom = B.w;
             }
             if (end_side < 0 && fp < 1.0e-10f) {
-              const uint4 R2 = philox10(flight, r.c1 | 1u, slo, shi, key);
+              const uint4 R2 = philox10(flight, c1 | 1u, slo, shi, key);
               fp = -lam * __logf(u23f(R2.y));
             }
           }
@@ -689,8 +740,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
 template <int MODE>
 cudaError_t occupancy_mode(int block, size_t smem, int* bps) {
   if (smem > 0)
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_persistent<true, MODE>, block, smem);
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_persistent<false, MODE>, block, 0);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_persistent<true, MODE, false>,
+                                                         block, smem);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_persistent<false, MODE, false>,
+                                                       block, 0);
 }
 
 template <int MODE>
@@ -698,14 +751,27 @@ cudaError_t launch_mode(const GeoF32& g, const RunF32& r, int grid, int block, s
                         cudaStream_t st) {
   if (g.stage_smem && smem > 0) {
     if (smem > 48 * 1024) {
-      cudaError_t e = cudaFuncSetAttribute(k_persistent<true, MODE>,
+      cudaError_t e = cudaFuncSetAttribute(k_persistent<true, MODE, false>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (e != cudaSuccess) return e;
     }
-    k_persistent<true, MODE><<<grid, block, smem, st>>>(g, r);
+    k_persistent<true, MODE, false><<<grid, block, smem, st>>>(g, r);
   } else {
-    k_persistent<false, MODE><<<grid, block, 0, st>>>(g, r);
+    k_persistent<false, MODE, false><<<grid, block, 0, st>>>(g, r);
   }
+  return cudaGetLastError();
+}
+
+cudaError_t persistent_batch_occupancy(int block, int* bps) {
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      bps, k_persistent<false, MODE_FORWARD, true>, block, 0);
+}
+
+cudaError_t launch_persistent_batch(const RunF32& r, int grid, int block, cudaStream_t st) {
+  if (block != kBlock) return cudaErrorInvalidConfiguration;
+  GeoF32 g;
+  memset(&g, 0, sizeof(g));
+  k_persistent<false, MODE_FORWARD, true><<<grid, block, 0, st>>>(g, r);
   return cudaGetLastError();
 }
 

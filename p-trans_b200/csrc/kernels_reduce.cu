@@ -19,9 +19,9 @@ namespace ptg {
 
 namespace {
 
-__global__ void k_mode_terms(ReduceIn in) {
-  const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= in.nmode) return;
+/* Per-mode terms of one geometry; the batched kernel calls it with the
+   geometry's counts, np, Simpson step and output rows. */
+__device__ void mode_terms(const ReduceIn& in, int64_t m) {
   const int na = in.nangle, ns = in.ns;
   double S[64], V[64], dE[64];
   /* ns <= 64 is checked on the host */
@@ -103,10 +103,34 @@ __global__ void k_mode_terms(ReduceIn in) {
   in.bv[m] = W * W * vm;
 }
 
+__global__ void k_mode_terms(ReduceIn in) {
+  const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= in.nmode) return;
+  mode_terms(in, m);
+}
+
+__global__ void k_mode_terms_batch(ReduceBatchIn b) {
+  const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int g = blockIdx.y;
+  if (m >= b.base.nmode) return;
+  ReduceIn in = b.base;
+  const int64_t nm = in.nmode;
+  in.counts = b.base.counts + (int64_t)g * b.ntask_per_geo;
+  in.np = b.np_geo[g];
+  in.dS = b.dS_geo[g];
+  in.tnorm = b.tnorm_geo[g];
+  in.tc = b.base.tc + g * nm;
+  in.kv = b.base.kv + g * nm;
+  in.bw = b.base.bw + g * nm;
+  in.bv = b.base.bv + g * nm;
+  in.emfp_nm = b.base.emfp_nm + g * nm;
+  in.transmit = nullptr;
+  mode_terms(in, m);
+}
+
 /* block 0: kappa and its variance; block 1+b: bin b. Fixed-order sums. */
-__global__ void __launch_bounds__(1024) k_sums(ReduceIn in) {
+__device__ void sums(const ReduceIn& in, int b) {
   __shared__ double sh[3][1024];
-  const int b = (int)blockIdx.x - 1;
   double a0 = 0.0, a1 = 0.0, a2 = 0.0;
   for (int64_t m = threadIdx.x; m < in.nmode; m += blockDim.x) {
     if (b < 0) {
@@ -142,6 +166,20 @@ __global__ void __launch_bounds__(1024) k_sums(ReduceIn in) {
   }
 }
 
+__global__ void __launch_bounds__(1024) k_sums(ReduceIn in) { sums(in, (int)blockIdx.x - 1); }
+
+__global__ void __launch_bounds__(1024) k_sums_batch(ReduceBatchIn bi) {
+  ReduceIn in = bi.base;
+  const int g = blockIdx.y;
+  const int64_t nm = in.nmode;
+  in.tc = bi.base.tc + g * nm;
+  in.kv = bi.base.kv + g * nm;
+  in.bw = bi.base.bw + g * nm;
+  in.bv = bi.base.bv + g * nm;
+  in.result = bi.base.result + (int64_t)g * (2 + 3 * in.nbins);
+  sums(in, (int)blockIdx.x - 1);
+}
+
 }  // namespace
 
 cudaError_t launch_kappa_reduce(const ReduceIn& in, cudaStream_t st) {
@@ -153,6 +191,19 @@ cudaError_t launch_kappa_reduce(const ReduceIn& in, cudaStream_t st) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   k_sums<<<1 + in.nbins, 1024, 0, st>>>(in);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_kappa_reduce_batch(const ReduceBatchIn& b, cudaStream_t st) {
+  if (b.base.nmode <= 0 || b.ngeo <= 0) return cudaSuccess;
+  if (b.base.ns > 64 || b.ngeo > 65535) return cudaErrorInvalidValue;
+  const int block = 128;
+  dim3 g1((unsigned)((b.base.nmode + block - 1) / block), (unsigned)b.ngeo);
+  k_mode_terms_batch<<<g1, block, 0, st>>>(b);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  dim3 g2((unsigned)(1 + b.base.nbins), (unsigned)b.ngeo);
+  k_sums_batch<<<g2, 1024, 0, st>>>(b);
   return cudaGetLastError();
 }
 

@@ -85,6 +85,13 @@ struct NoallocView {
 };
 int handle_noalloc_view(ptg_handle* h, NoallocView* v);
 
+/* FP32 geometry blob (host copy) of a built geometry. */
+int blob_from_geometry(const GeomSoA& G, std::vector<float4>* out, BlobLayout* lay,
+                       std::string* why);
+/* Host FP64 kappa assembly (see api.cpp). */
+int assemble_host(const SpecSoA& S, const ptg_run* run, double box_x, const uint64_t* counts,
+                  ptg_kappa_out* out, std::vector<double>* wtask, double* dk_ds_an);
+
 }  // namespace ptg
 
 #endif

@@ -246,3 +246,25 @@ def write_mcp(model: Model, path: str, np_: int = 100, nangle: int = 11,
             spos += 1
     with open(path, "w") as f:
         f.write("\n".join(w) + "\n")
+
+
+def film_batch(n: int = 256, seed: int = 0, n_modes: int = 2000, nangle: int = 11,
+               samples_lo: float = 1e5, samples_hi: float = 1e7):
+    """Screening set: n periodic films, one through-thickness hole per cell.
+
+    hole radius ~ U(10, 60) nm, period ~ U(100, 400) nm (cell x = y = period,
+    radius kept below period/2 - 5 nm), thickness ~ U(50, 300) nm, samples per
+    film log-uniform in [samples_lo, samples_hi] (rounded to particles per
+    (mode, angle) task).  Returns (models, particles per task)."""
+    rng = np.random.default_rng(seed)
+    models, nps = [], []
+    for _ in range(n):
+        period = rng.uniform(100.0, 400.0)
+        radius = min(rng.uniform(10.0, 60.0), period / 2 - 5.0)
+        thick = rng.uniform(50.0, 300.0)
+        m = film_with_holes(lx=period, ly=period, lz=thick, nholes=1, radius=radius,
+                            centres=np.array([[period / 2, period / 2]]), periodic_y=True)
+        samples = math.exp(rng.uniform(math.log(samples_lo), math.log(samples_hi)))
+        nps.append(max(1, int(round(samples / (n_modes * (nangle - 1))))))
+        models.append(m)
+    return models, nps
