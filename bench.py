@@ -197,6 +197,56 @@ def run_reference(args):
     return 0
 
 
+def run_c5(args):
+    """256 periodic films with one hole each, uneven sample counts (1e5-1e7),
+    2000 modes, 64 bins: one batched persistent launch replayed as a CUDA graph
+    against sequential plain FP64 launches (timed on a subset of films)."""
+    import torch
+    torch.cuda.set_device(0)
+    pkg = load_pkg()
+    A, synth = pkg.abi, pkg.synth
+    models, nps = synth.film_batch(256, seed=0)
+    spec = synth.spectrum(2000, seed=0)
+    bufs = [A.GeomBuf(m) for m in models]
+    run = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=11, np_=1, temperature=300.0, nbins=64,
+                     bin_omega=(0.0, 15.0 * 2 * math.pi * 1e12))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda:0")
+    with A.Batch([b.view for b in bufs], nps, list(range(256)), [0] * 256, spec, run) as bt:
+        for _ in range(args.warmup):
+            bt.run()
+        ms = fl = 0.0
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            r = bt.run()
+            ms += r["graph_ms"]
+            fl += r["flights"]
+    batch_rate = fl / (ms * 1e-3)
+    # sequential plain FP64 runs of a subset of the films
+    idx = list(range(0, 256, max(1, 256 // args.fp64_subset)))[: args.fp64_subset]
+    f64_ms = f64_fl = 0.0
+    for i in idx:
+        with A.Handle(bufs[i].view, spec) as h:
+            r64 = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=11, np_=nps[i], seed=i, precision=A.PREC_FP64,
+                             temperature=300.0, nbins=64, bin_omega=(0.0, 15.0 * 2 * math.pi * 1e12))
+            h.kappa(r64)
+            st = h.stats()
+            f64_ms += st["kernel_ms"] + st["reduce_ms"]
+            f64_fl += st["flights"]
+    f64_rate = f64_fl / (f64_ms * 1e-3)
+    print(json.dumps({
+        "metric": "phonon free-flights/s, 256-film batched screening (one CUDA-graph launch)",
+        "value": batch_rate, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "256 periodic films, hole r~U(10,60) nm, period~U(100,400) nm, "
+                               "thickness~U(50,300) nm, samples per film log-uniform 1e5-1e7, 2000 modes, 64 bins",
+                   "samples_total": int(sum(nps) * 20000), "fp64_subset": len(idx)},
+        "plain_fp64_sequential": {"value": f64_rate, "unit": UNIT, "films": len(idx),
+                                  "speedup_batch_over_fp64": batch_rate / f64_rate},
+        "flights_per_step": fl / args.steps}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -206,9 +256,15 @@ def main():
     ap.add_argument("--np", type=int, default=500, help="particles per (mode, angle) per GPU")
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="thinfilm", choices=["thinfilm", "c5"],
+                    help="thinfilm: the metric's configuration; c5: 256-film batched screening")
+    ap.add_argument("--fp64-subset", type=int, default=16,
+                    help="c5: films timed one by one with the plain FP64 kernel")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "c5":
+        return run_c5(args)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
