@@ -181,7 +181,10 @@ typedef struct ptg_options {
   int64_t chunk;            /* samples per work-queue chunk (0 = tuned)         */
   int32_t tune_flags;       /* persistent kernel variants (autotuner):          */
                             /*   bit 0: no safe-distance p-p fast path          */
+                            /*   bit 1: no warp-cooperative tail                */
   int32_t fast_steps;       /* fast p-p flights per iteration (0 = tuned)       */
+  int32_t coop_lanes;       /* a warp with at most this many live phonons       */
+                            /* advances them with all 32 lanes (0 = tuned)      */
 } ptg_options;
 
 /*
@@ -240,6 +243,8 @@ typedef struct ptg_stats {
   double tail_ms;           /* FP32 kernel: queue dry until the last warp ended */
   uint64_t full_flights;    /* FP32 kernel: flights taken with the full test     */
   uint64_t safe_balls;      /* FP32 kernel: safe balls computed                 */
+  uint64_t coop_rounds;     /* FP32 kernel: warp-cooperative rounds             */
+  uint64_t coop_flights;    /* FP32 kernel: p-p flights taken in those rounds   */
 } ptg_stats;
 
 typedef struct ptg_handle ptg_handle;

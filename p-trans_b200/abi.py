@@ -85,7 +85,7 @@ class PtgOptions(C.Structure):
         ("device", C.c_int32), ("block_size", C.c_int32), ("blocks_per_sm", C.c_int32),
         ("regen_threshold", C.c_int32), ("ref_quirks", C.c_int32), ("bvh_leaf", C.c_int32),
         ("max_flights", C.c_int64), ("lost_limit", C.c_double), ("chunk", C.c_int64),
-        ("tune_flags", C.c_int32), ("fast_steps", C.c_int32),
+        ("tune_flags", C.c_int32), ("fast_steps", C.c_int32), ("coop_lanes", C.c_int32),
     ]
 
 
@@ -116,6 +116,7 @@ class PtgStats(C.Structure):
         ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64),
         ("max_traj_flights", C.c_uint64), ("drain_ms", C.c_double), ("tail_ms", C.c_double),
         ("full_flights", C.c_uint64), ("safe_balls", C.c_uint64),
+        ("coop_rounds", C.c_uint64), ("coop_flights", C.c_uint64),
     ]
 
 

@@ -429,6 +429,8 @@ int run_transport(ptg_handle* h, const Transport& T) {
     r.fast_steps = (h->opt.tune_flags & 1) ? 0 : (h->opt.fast_steps > 0 ? h->opt.fast_steps : 16);
     const double lmin = std::min(h->geom.box[0], std::min(h->geom.box[1], h->geom.box[2]));
     r.fast_lambda_max = (float)(0.1 * lmin);
+    /* tune_flags bit 1 turns the cooperative tail off; 0 selects 8 lanes */
+    r.coop_lanes = (h->opt.tune_flags & 2) ? 0 : (h->opt.coop_lanes > 0 ? std::min(h->opt.coop_lanes, 32) : 8);
     r.counts = h->counts.as<unsigned long long>();
     r.lost = h->lost.as<unsigned long long>();
     r.stats = h->stats.as<unsigned long long>();
@@ -475,6 +477,8 @@ int finish_stats(ptg_handle* h) {
   h->last.max_traj_flights = st[4];
   h->last.full_flights = st[8];
   h->last.safe_balls = st[9];
+  h->last.coop_rounds = st[12];
+  h->last.coop_flights = st[13];
   h->list_n = st[10];
   h->mismatch = st[11];
   if (st[5] != ~0ull && st[7] >= st[5]) {

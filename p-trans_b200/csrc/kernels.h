@@ -123,6 +123,8 @@ struct RunF32 {
   int32_t regen_threshold;
   int32_t fast_steps;         /* max safe-distance p-p flights per iteration (0: off) */
   float fast_lambda_max;      /* tasks with a smaller MFP use the fast path           */
+  int32_t coop_lanes;         /* warps with at most this many live lanes advance them
+                                 cooperatively, 32 flights a round (0: off)       */
   unsigned long long* counts;
   unsigned long long* lost;
   /* flights, lost, capped, samples, max trajectory flights,

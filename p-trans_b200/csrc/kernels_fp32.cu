@@ -34,7 +34,12 @@
  *     any event; on the fast path the blocks of four flights are computed
  *     together so that four independent chains fill the issue slots of a
  *     warp that is alone on its scheduler (the tail of a run); tallies are
- *     integer, aggregated per warp by task (match_any) before one atomic.
+ *     integer, aggregated per warp by task (match_any) before one atomic;
+ *   - warp-cooperative tail: a warp left with few live phonons advances each
+ *     of them 32 flights per round, one flight per lane, with the flights'
+ *     start points summed in flight order; every path (fast, full,
+ *     cooperative) moves the position with the same fma, so a trajectory is
+ *     the same whichever path takes its flights.
  */
 #include <cuda_runtime.h>
 #include <math.h>
@@ -194,6 +199,26 @@ __device__ __forceinline__ void scan_grain(const G_t& G, int grain, float px, fl
   }
 }
 
+/* Exit of the box grain along d from p: distance tb and face sb (0 x-,
+   1 x+, 2 y-, 3 y+, 4 z-, 5 z+), clamped at 0. */
+__device__ __forceinline__ void slab_exit(float px, float py, float pz, float dx, float dy,
+                                          float dz, float X, float Y, float Z, float& tb,
+                                          int& sb) {
+  tb = 3.0e38f;
+  sb = -1;
+  if (dx > 0.0f) { tb = __fdividef(X - px, dx); sb = 1; }
+  else if (dx < 0.0f) { tb = __fdividef(-px, dx); sb = 0; }
+  if (dy != 0.0f) {
+    const float t = __fdividef((dy > 0.0f ? Y : 0.0f) - py, dy);
+    if (t < tb) { tb = t; sb = dy > 0.0f ? 3 : 2; }
+  }
+  if (dz != 0.0f) {
+    const float t = __fdividef((dz > 0.0f ? Z : 0.0f) - pz, dz);
+    if (t < tb) { tb = t; sb = dz > 0.0f ? 5 : 4; }
+  }
+  tb = fmaxf(tb, 0.0f);
+}
+
 /* Lower bound of the distance from p to every box face and to every
    candidate surface of the grain (planes bound polygons from below, the
    infinite cylinder bounds the clipped one). */
@@ -284,6 +309,10 @@ __device__ bool stage_blob(const float4* gblob, float4* sblob, int units, int* e
    doubles when they fit, else the replay adds to global memory directly. */
 constexpr int kAdjSmemDoubles = 2048;
 
+/* rounds of 32 flights one cooperative visit may take before the phonon's
+   lane returns to the refill / tally step */
+constexpr int kCoopRounds = 8;
+
 template <bool SMEM, int MODE, bool BATCH>
 __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   typename std::conditional<BATCH, GeoBatch, Geo<SMEM>>::type G;
@@ -328,6 +357,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   uint32_t slo = 0, shi = 0, flight = 0;
   unsigned long long my_flights = 0, my_samples = 0, my_capped = 0, my_lost = 0, my_max = 0;
   unsigned my_full = 0, my_balls = 0;
+  unsigned long long my_coop_rounds = 0, my_coop_flights = 0;
 
   while (true) {
     /* ---- refill idle lanes from the warp's chunk ---------------------- */
@@ -450,6 +480,142 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
     }
 
     int end_side = -1;  /* -1 still running, 0 lost, 1 x-, 2 x+ */
+
+    /* ---- warp-cooperative flights for the last few live lanes ----------
+       Once a warp holds at most coop_lanes live phonons (the tail of a run,
+       when only the longest diffusive trajectories are left), its 32 lanes
+       advance one phonon at a time, 32 flights per round: lane j draws the
+       Philox block of flight f+1+j, the start point of every flight is the
+       serial sum of the earlier flights (in their order, with the rounding
+       of the one-lane path), and each lane runs the full intersection test
+       of its own flight.  The first flight that hits a surface, leaves the
+       box or reaches the cap ends the round; the flights before it are p-p
+       events.  The hit flight's Philox block and nearest surface are handed
+       to the phonon's lane, which processes the event below. */
+    bool coop = false;       /* this lane was advanced cooperatively          */
+    bool pre = false;        /* ... up to a surface hit: preR / pre_tb / pre_sb */
+    bool skip_full = false;  /* ... up to the round limit: no event this pass  */
+    uint4 preR = make_uint4(0u, 0u, 0u, 0u);
+    float pre_tb = 0.0f;
+    int pre_sb = -1;
+    if (!BATCH && r.coop_lanes > 0) {
+      const unsigned todo0 = __ballot_sync(FULL, alive && lam < flmax);
+      if (todo0 && __popc(__ballot_sync(FULL, alive)) <= r.coop_lanes) {
+        unsigned todo = todo0;
+        while (todo) {
+          const int L = __ffs(todo) - 1;
+          todo &= todo - 1;
+          float cpx = __shfl_sync(FULL, px, L), cpy = __shfl_sync(FULL, py, L);
+          float cpz = __shfl_sync(FULL, pz, L);
+          float cdx = __shfl_sync(FULL, dx, L), cdy = __shfl_sync(FULL, dy, L);
+          float cdz = __shfl_sync(FULL, dz, L), cfp = __shfl_sync(FULL, fp, L);
+          const float clam = __shfl_sync(FULL, lam, L);
+          uint32_t cfl = __shfl_sync(FULL, flight, L);
+          const uint32_t cslo = __shfl_sync(FULL, slo, L), cshi = __shfl_sync(FULL, shi, L);
+          const int cgrain = __shfl_sync(FULL, grain, L);
+          int clast = __shfl_sync(FULL, last_geom, L);
+          float clen = 0.0f;
+          unsigned cnpp = 0, ctaken = 0, crounds = 0;
+          int stop = 0;  /* 0 round limit, 1 surface hit, 2 lost or capped */
+          uint4 sR = make_uint4(0u, 0u, 0u, 0u);
+          float stb = 0.0f;
+          int ssb = -1;
+          for (int round = 0; round < kCoopRounds; ++round) {
+            ++crounds;
+            const uint4 R = philox10(cfl + 1u + (uint32_t)lane, c1, cslo, cshi, key);
+            /* direction and free path after a p-p event ending flight `lane` */
+            const float ct = fmaf(u23f(R.x), 2.0f, -1.0f);
+            const float st = sqrt_approx(fmaxf(0.0f, fmaf(-ct, ct, 1.0f)));
+            float sp, cp;
+            sincos2pi(u23f(R.y), &sp, &cp);
+            const float nx = ct, ny = st * cp, nz = st * sp;
+            const float nf = -clam * __logf(u23f(R.z));
+            /* flight `lane` starts with the state the previous flight drew */
+            float sdx = __shfl_up_sync(FULL, nx, 1), sdy = __shfl_up_sync(FULL, ny, 1);
+            float sdz = __shfl_up_sync(FULL, nz, 1), sfp = __shfl_up_sync(FULL, nf, 1);
+            if (lane == 0) { sdx = cdx; sdy = cdy; sdz = cdz; sfp = cfp; }
+            float qx = cpx, qy = cpy, qz = cpz;
+#pragma unroll
+            for (int i = 0; i < 31; ++i) {
+              const float a = __shfl_sync(FULL, sfp, i);
+              const float ex = __shfl_sync(FULL, sdx, i);
+              const float ey = __shfl_sync(FULL, sdy, i);
+              const float ez = __shfl_sync(FULL, sdz, i);
+              if (i < lane) {
+                qx = fmaf(a, ex, qx);
+                qy = fmaf(a, ey, qy);
+                qz = fmaf(a, ez, qz);
+              }
+            }
+            const bool inbox = qx >= -eps && qx <= X + eps && qy >= -eps && qy <= Y + eps &&
+                               qz >= -eps && qz <= Z + eps;
+            const bool capd = (unsigned long long)cfl + (unsigned)lane >= r.max_flights;
+            float tb;
+            int sb;
+            slab_exit(qx, qy, qz, sdx, sdy, sdz, X, Y, Z, tb, sb);
+            if (cgrain > 0)
+              scan_grain(G, cgrain, qx, qy, qz, sdx, sdy, sdz, lane == 0 ? clast : -1, eps, Z,
+                         tb, sb);
+            const bool brk = !inbox || capd;
+            const unsigned sm = __ballot_sync(FULL, brk || !(sfp < tb));
+            const int j = sm ? __ffs(sm) - 1 : 32;
+            if (MODE == MODE_ADJOINT) {
+              float l = lane < j ? sfp : 0.0f;
+              for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(FULL, l, o);
+              clen += l;
+              cnpp += (unsigned)j;
+            }
+            ctaken += (unsigned)j;
+            if (j < 32) {
+              cpx = __shfl_sync(FULL, qx, j); cpy = __shfl_sync(FULL, qy, j);
+              cpz = __shfl_sync(FULL, qz, j);
+              cdx = __shfl_sync(FULL, sdx, j); cdy = __shfl_sync(FULL, sdy, j);
+              cdz = __shfl_sync(FULL, sdz, j); cfp = __shfl_sync(FULL, sfp, j);
+              cfl += (uint32_t)j;
+              if (j > 0) clast = -1;
+              stop = __shfl_sync(FULL, brk ? 2 : 1, j);
+              if (stop == 1) {
+                sR.x = __shfl_sync(FULL, R.x, j); sR.y = __shfl_sync(FULL, R.y, j);
+                sR.z = __shfl_sync(FULL, R.z, j); sR.w = __shfl_sync(FULL, R.w, j);
+                stb = __shfl_sync(FULL, tb, j);
+                ssb = __shfl_sync(FULL, sb, j);
+              }
+              break;
+            }
+            /* all 32 flights end in p-p events: the state after the last */
+            cpx = __shfl_sync(FULL, fmaf(sfp, sdx, qx), 31);
+            cpy = __shfl_sync(FULL, fmaf(sfp, sdy, qy), 31);
+            cpz = __shfl_sync(FULL, fmaf(sfp, sdz, qz), 31);
+            cdx = __shfl_sync(FULL, nx, 31); cdy = __shfl_sync(FULL, ny, 31);
+            cdz = __shfl_sync(FULL, nz, 31); cfp = __shfl_sync(FULL, nf, 31);
+            cfl += 32u;
+            clast = -1;
+          }
+          if (lane == L) {
+            px = cpx; py = cpy; pz = cpz;
+            dx = cdx; dy = cdy; dz = cdz; fp = cfp;
+            flight = cfl;
+            last_geom = clast;
+            if (MODE == MODE_ADJOINT) {
+              adj_len += clen;
+              adj_npp += cnpp;
+            }
+            coop = true;
+            if (stop == 1) {
+              pre = true;
+              preR = sR;
+              pre_tb = stb;
+              pre_sb = ssb;
+            } else if (stop == 0) {
+              skip_full = true;
+            }
+            my_coop_rounds += crounds;
+            my_coop_flights += ctaken;
+          }
+        }
+      }
+    }
+
     if (alive) {
       /* ---- safe-ball p-p flights: the segment to the next p-p point stays
          inside the safe ball (convex), so no surface is crossed.  Four
@@ -457,7 +623,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
          paths do not depend on the phonon state and are computed together;
          only the position / ball test chain is serial. ---- */
       int k = 0;
-      bool fast_more = br2 > 0.0f;
+      bool fast_more = br2 > 0.0f && !coop;
       while (fast_more && k < r.fast_steps && flight + 4u <= r.max_flights) {
         uint4 B[4];
 #pragma unroll
@@ -474,32 +640,41 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           nz[j] = st * sp;
           nf[j] = -lam * __logf(u23f(B[j].z));
         }
-        /* position relative to the ball centre along the four steps */
-        float wx = px - bx, wy = py - by, wz = pz - bz;
+        /* the position advances with the same rounding as a full flight's
+           p-p event, so the trajectory does not depend on which path took
+           a flight */
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
           /* predicated: no branch per step */
-          const float qx = fmaf(fp, dx, wx), qy = fmaf(fp, dy, wy), qz = fmaf(fp, dz, wz);
-          const bool acc = fast_more && (fmaf(qx, qx, fmaf(qy, qy, qz * qz)) < br2);
+          const float qx = fmaf(fp, dx, px), qy = fmaf(fp, dy, py), qz = fmaf(fp, dz, pz);
+          const float ex = qx - bx, ey = qy - by, ez = qz - bz;
+          const bool acc = fast_more && (fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < br2);
           if (MODE == MODE_ADJOINT) {
             adj_len += acc ? fp : 0.0f;
             adj_npp += acc ? 1u : 0u;
           }
           flight += acc ? 1u : 0u;
           k += acc ? 1 : 0;
-          wx = acc ? qx : wx; wy = acc ? qy : wy; wz = acc ? qz : wz;
+          px = acc ? qx : px; py = acc ? qy : py; pz = acc ? qz : pz;
           dx = acc ? nx[j] : dx; dy = acc ? ny[j] : dy; dz = acc ? nz[j] : dz;
           fp = acc ? nf[j] : fp;
           fast_more = acc;
         }
-        px = bx + wx; py = by + wy; pz = bz + wz;
       }
       /* a lane that used up its fast steps waits for the next iteration;
          any other lane takes one flight with the full test now */
-      if (!(fast_more && k >= r.fast_steps)) {
-        /* ---- one free flight with the intersection test -------------- */
-        if (!(px >= -eps && px <= X + eps && py >= -eps && py <= Y + eps && pz >= -eps &&
-              pz <= Z + eps)) {
+      if (!(fast_more && k >= r.fast_steps) && !skip_full) {
+        /* ---- one free flight with the intersection test (already run by
+           the cooperative round when it handed over a hit) -------------- */
+        bool go = false;
+        uint4 R = preR;
+        float tb = pre_tb;
+        int sb = pre_sb;
+        if (pre) {
+          ++flight;
+          go = true;
+        } else if (!(px >= -eps && px <= X + eps && py >= -eps && py <= Y + eps &&
+                     pz >= -eps && pz <= Z + eps)) {
           end_side = 0;
         } else if (flight >= r.max_flights) {
           end_side = 0;
@@ -507,23 +682,12 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
         } else {
           ++flight;
           ++my_full;
-          const uint4 R = philox10(flight, c1, slo, shi, key);
-          /* slab exit of the box grain */
-          float tb = 3.0e38f;
-          int sb = -1;
-          if (dx > 0.0f) { tb = __fdividef(X - px, dx); sb = 1; }
-          else if (dx < 0.0f) { tb = __fdividef(-px, dx); sb = 0; }
-          if (dy != 0.0f) {
-            const float t = __fdividef((dy > 0.0f ? Y : 0.0f) - py, dy);
-            if (t < tb) { tb = t; sb = dy > 0.0f ? 3 : 2; }
-          }
-          if (dz != 0.0f) {
-            const float t = __fdividef((dz > 0.0f ? Z : 0.0f) - pz, dz);
-            if (t < tb) { tb = t; sb = dz > 0.0f ? 5 : 4; }
-          }
-          tb = fmaxf(tb, 0.0f);
+          R = philox10(flight, c1, slo, shi, key);
+          slab_exit(px, py, pz, dx, dy, dz, X, Y, Z, tb, sb);
           if (grain > 0) scan_grain(G, grain, px, py, pz, dx, dy, dz, last_geom, eps, Z, tb, sb);
-
+          go = true;
+        }
+        if (go) {
           const float u0 = u23f(R.x), u1 = u23f(R.y), u2 = u23f(R.z), u3 = u23f(R.w);
           if (fp < tb) {
             /* intrinsic scattering: isotropic direction, new free path */
@@ -704,10 +868,12 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   }
   /* warp totals */
   unsigned long long v0 = my_flights, v1 = my_lost, v2 = my_capped, v3 = my_samples, v4 = my_max;
-  unsigned long long v5 = my_full, v6 = my_balls;
+  unsigned long long v5 = my_full, v6 = my_balls, v7 = my_coop_rounds, v8 = my_coop_flights;
   for (int o = 16; o > 0; o >>= 1) {
     v5 += __shfl_xor_sync(FULL, v5, o);
     v6 += __shfl_xor_sync(FULL, v6, o);
+    v7 += __shfl_xor_sync(FULL, v7, o);
+    v8 += __shfl_xor_sync(FULL, v8, o);
     v0 += __shfl_xor_sync(FULL, v0, o);
     v1 += __shfl_xor_sync(FULL, v1, o);
     v2 += __shfl_xor_sync(FULL, v2, o);
@@ -727,6 +893,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
     atomicMax(r.stats + 7, globaltimer());
     if (v5) atomicAdd(r.stats + 8, v5);
     if (v6) atomicAdd(r.stats + 9, v6);
+    if (v7) atomicAdd(r.stats + 12, v7);
+    if (v8) atomicAdd(r.stats + 13, v8);
   }
   if (MODE == MODE_ADJOINT && adj_in_smem) {
     __syncthreads();

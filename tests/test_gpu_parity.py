@@ -176,3 +176,34 @@ def test_rank_partition_is_exact_fp32():
         again = h.kappa(A.make_run(**kw), want_counts=True)["counts"]
     np.testing.assert_array_equal(r0 + r1, full)
     np.testing.assert_array_equal(again, full)
+
+
+@pytest.mark.parametrize("name", ["film_periodic", "film_mirror_transmit", "spheres", "brick_tris",
+                                  "nanowire_mixed"])
+@pytest.mark.parametrize("cap", [0, 40])
+def test_cooperative_tail_takes_the_same_trajectories(name, cap):
+    """Warp-cooperative rounds (every warp, coop_lanes = 32) and the one-lane
+    path (tune_flags bit 1) give identical per-task counts, lost counts and
+    flight totals: a flight advances the position with the same rounding on
+    every path, so the trajectory depends only on its Philox counter."""
+    m = geometries()[name]
+    spec = synth.spectrum(12, seed=5, mfp_lo=1e-9, mfp_hi=3e-8)
+    gb = A.GeomBuf(m)
+    run = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=5, np_=257, seed=21, precision=A.PREC_FP32)
+    out = {}
+    for key, opts in (("lane", dict(tune_flags=2)), ("coop", dict(coop_lanes=32)),
+                      ("tail", dict()), ("coop_nofast", dict(coop_lanes=32, tune_flags=1))):
+        with A.Handle(gb.view, spec, max_flights=cap, **opts) as h:
+            k = h.kappa(run, want_counts=True)
+            out[key] = (k["counts"], k["lost"], h.stats())
+    base_counts, base_lost, base_st = out["lane"]
+    assert base_st["coop_rounds"] == 0
+    for key in ("coop", "tail", "coop_nofast"):
+        counts, lost, st = out[key]
+        np.testing.assert_array_equal(counts, base_counts, err_msg=key)
+        assert lost == base_lost, key
+        assert st["flights"] == base_st["flights"], key
+        assert st["max_traj_flights"] == base_st["max_traj_flights"], key
+    assert out["coop"][2]["coop_rounds"] > 0 and out["coop"][2]["coop_flights"] > 0
+    if cap:
+        assert base_lost > 0
