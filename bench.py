@@ -28,7 +28,6 @@ import json
 import math
 import os
 import statistics
-import subprocess
 import sys
 import time
 
@@ -74,54 +73,54 @@ def make_run(pkg, spec, np_total, rank, nranks, precision, seed=12345):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """SM clock and throttle reasons of one GPU, read through NVML every
+    10 ms on a background thread (read-only queries)."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event reason bits
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+               0x4: "sw_power_cap"}
 
     def __init__(self, device):
         self.device = device
-        self.p = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_dev{device}.csv")
+        self.samples = []
+        self.thread = None
+        self.stop_flag = False
 
     def start(self):
+        import threading
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
-            self.f = open(self.path, "w")
-            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                       "-i", str(self.device), "-lms", "200"], stdout=self.f,
-                                      stderr=subprocess.DEVNULL)
-        except (OSError, FileNotFoundError):
-            self.p = None
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(self.device)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+            return
+
+        def loop():
+            while not self.stop_flag:
+                try:
+                    sm = self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM)
+                    rs = self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                    self.samples.append((sm, rs))
+                except Exception:
+                    pass
+                time.sleep(0.01)
+
+        self.thread = threading.Thread(target=loop, daemon=True)
+        self.thread.start()
 
     def stop(self):
-        if self.p is None:
+        if self.thread is None:
             return None
-        self.p.terminate()
-        try:
-            self.p.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.p.kill()
-        self.f.close()
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                mx.append(float(parts[2]))
-            except ValueError:
-                continue
-            for n, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        if not sm:
+        self.stop_flag = True
+        self.thread.join(timeout=5)
+        if not self.samples:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        reasons = sorted({n for _, rs in self.samples for bit, n in self.REASONS.items() if rs & bit})
+        return {"sm_mhz": statistics.median(sm for sm, _ in self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(self.samples), "source": "NVML, 10 ms"}
 
 
 def measured_peaks():
@@ -132,13 +131,14 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def traffic_per_flight():
-    """DRAM bytes per free flight of the persistent kernel from the committed ncu summary."""
+def dram_traffic():
+    """DRAM bytes of one persistent-kernel launch (read + write) from the
+    committed ncu summary, and the workload they were captured on."""
     p = os.path.join(ROOT, "profiles", "persistent_fp32_thinfilm_dram.json")
     if os.path.exists(p):
         d = json.load(open(p))
-        return float(d["dram_bytes_per_flight"])
-    return None
+        return float(d["dram_bytes_read"] + d["dram_bytes_write"]), d["workload"]
+    return None, None
 
 
 def cpu_baseline(pkg, model, spec, target_s=10.0):
@@ -247,6 +247,81 @@ def run_c5(args):
     return 0
 
 
+def run_structure(args):
+    """C4 structures: 5 Voronoi grains in a 1 um cube (internal facets T = 0.5,
+    p = 0, diffuse outer walls), or a simple-cubic lattice of 16^3 cubic voids
+    (49152 triangles in the matrix grain, BVH).  20000-mode spectrum, 64 bins,
+    per-mode MFP runs.  Device time of ptg_kappa (FP32 persistent kernel +
+    reduction) against the plain FP64 kernel on a bounded sample (fewer
+    particles per task) and, for the mesh, the FP32 kernel without the BVH."""
+    import torch
+    torch.cuda.set_device(0)
+    pkg = load_pkg()
+    A, synth = pkg.abi, pkg.synth
+    if args.workload == "voronoi":
+        model = synth.voronoi_box(5, box=(1000.0, 1000.0, 1000.0), seed=0, trans=0.5, spec=0.0, p_wall=0.0)
+        desc = "5 Voronoi grains in a 1000^3 nm box, internal facets T=0.5 p=0, diffuse walls"
+        np_default, np64 = 500, 5
+    else:
+        model = synth.cube_lattice(n=16, l=1000.0, fill=0.5, trans=0.0, spec=0.0, p_wall=0.0)
+        desc = ("16^3 cubic voids (side 31.25 nm, pitch 62.5 nm) in a 1000^3 nm box, "
+                "49152 triangles in the matrix grain, diffuse")
+        np_default, np64 = 10, 1
+    npt = args.np if args.np != 500 else np_default
+    spec = synth.spectrum(20000, seed=0)
+    gb = A.GeomBuf(model)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda:0")
+
+    def timed(opts, np_, prec, steps, warm):
+        with A.Handle(gb.view, spec, **opts) as h:
+            run = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=11, np_=np_, seed=12345, precision=prec,
+                             temperature=300.0, nbins=64, bin_omega=(0.0, 15.0 * 2 * math.pi * 1e12))
+            for _ in range(warm):
+                h.kappa(run)
+            ms = fl = 0.0
+            out = st = None
+            for _ in range(steps):
+                flush.zero_()
+                torch.cuda.synchronize()
+                out = h.kappa(run)
+                st = h.stats()
+                ms += st["kernel_ms"] + st["reduce_ms"]
+                fl += st["flights"]
+            return fl / (ms * 1e-3), ms / steps, fl / steps, out, st
+
+    v, ms, fl, out, st = timed({}, npt, A.PREC_FP32, args.steps, args.warmup)
+    line = {"metric": f"phonon free-flights/s, {args.workload} structure", "value": v, "unit": UNIT,
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": desc, "modes": 20000, "bins": 64, "nangle": 11,
+                       "particles_per_task": npt, "samples": 20000 * 10 * npt},
+            "flights_per_step": fl, "kappa": out["kappa"], "kappa_stderr": out["kappa_stderr"],
+            "tests_per_flight": {"bvh_boxes": st["box_tests"] / max(st["flights"], 1),
+                                 "surfaces": st["surface_tests"] / max(st["flights"], 1),
+                                 "full_flight_fraction": st["full_flights"] / max(st["flights"], 1)},
+            "tail": {"max_trajectory_flights": st["max_traj_flights"], "queue_drain_ms": st["drain_ms"],
+                     "tail_ms": st["tail_ms"]}}
+    if args.workload == "mesh":
+        # the linear-scan comparators test 49152 triangles per flight: a
+        # bounded sample of the first 100 modes with one particle per task
+        full = spec
+        spec = A.Spectrum(omega=full.omega[:100], tau=full.tau[:100], vel=full.vel[:100],
+                          weight=full.weight[:100], nbranch=1, rtemp=full.rtemp, vol=full.vol,
+                          mfp=full.mfp[:100])
+        sample = "first 100 modes, 1 particle per (mode, angle) task"
+        vl, _, _, _, _ = timed({"bvh_leaf": -1}, np64, A.PREC_FP32, 1, 1)
+        vb, _, _, _, _ = timed({}, np64, A.PREC_FP32, 1, 1)
+        line["no_bvh_fp32"] = {"value": vl, "unit": UNIT, "sample": sample,
+                               "bvh_speedup_same_sample": vb / vl}
+    else:
+        sample = f"all modes, {np64} particles per (mode, angle) task"
+    v64, ms64, fl64, _, _ = timed({}, np64, A.PREC_FP64, 1, 0)
+    line["plain_fp64"] = {"value": v64, "unit": UNIT, "sample": sample, "ms": ms64,
+                          "speedup_fp32_over_fp64": v / v64}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -256,8 +331,9 @@ def main():
     ap.add_argument("--np", type=int, default=500, help="particles per (mode, angle) per GPU")
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="thinfilm", choices=["thinfilm", "c5"],
-                    help="thinfilm: the metric's configuration; c5: 256-film batched screening")
+    ap.add_argument("--workload", default="thinfilm", choices=["thinfilm", "c5", "voronoi", "mesh"],
+                    help="thinfilm: the metric's configuration; c5: 256-film batched screening; "
+                         "voronoi / mesh: the C4 structures")
     ap.add_argument("--fp64-subset", type=int, default=16,
                     help="c5: films timed one by one with the plain FP64 kernel")
     args = ap.parse_args()
@@ -265,6 +341,8 @@ def main():
         return run_reference(args)
     if args.workload == "c5":
         return run_c5(args)
+    if args.workload in ("voronoi", "mesh"):
+        return run_structure(args)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -358,7 +436,7 @@ def main():
         per_launch_flights = flights / world / args.steps
         launch_s = kern_ms / args.steps * 1e-3
         achieved = BYTES_PER_FLIGHT * per_launch_flights / launch_s / 1e9
-        tpf = traffic_per_flight()
+        traffic, traffic_case = dram_traffic()
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
@@ -371,7 +449,7 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
                          "bytes_per_flight": BYTES_PER_FLIGHT,
-                         "traffic": (tpf * per_launch_flights) if tpf is not None else None,
+                         "traffic": traffic, "traffic_case": traffic_case,
                          "kernel": "k_persistent", "launch_ms": launch_s * 1e3, "grid": grid, "block": block},
             "fp32_roofline": {"flops_per_flight": FLOPS_PER_FLIGHT_C2,
                               "achieved_tflops": FLOPS_PER_FLIGHT_C2 * per_launch_flights / launch_s / 1e12,

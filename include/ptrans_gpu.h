@@ -175,7 +175,8 @@ typedef struct ptg_options {
   int32_t regen_threshold;  /* idle lanes before a warp refills (0 = 1)         */
   int32_t ref_quirks;       /* 1: a lost phonon also counts as transmitted      */
                             /*    (src/RTMCphon.f90:1701 then :1833)            */
-  int32_t bvh_leaf;         /* BVH leaf size (0 = tuned)                        */
+  int32_t bvh_leaf;         /* BVH leaf size (0 = tuned, < 0 = no BVH): grains  */
+                            /* with more than 32 candidate surfaces get a BVH   */
   int64_t max_flights;      /* per-trajectory cap, lost when reached (0 = 1e7)  */
   double lost_limit;        /* PTG_ERR_LOST if lost/total exceeds it (0 = off)  */
   int64_t chunk;            /* samples per work-queue chunk (0 = tuned)         */
@@ -185,6 +186,8 @@ typedef struct ptg_options {
   int32_t fast_steps;       /* fast p-p flights per iteration (0 = tuned)       */
   int32_t coop_lanes;       /* a warp with at most this many live phonons       */
                             /* advances them with all 32 lanes (0 = tuned)      */
+  int32_t long_flights;     /* a phonon past this many flights is advanced by   */
+                            /* its whole warp even in a busy warp (<= 0: never) */
 } ptg_options;
 
 /*
@@ -245,6 +248,10 @@ typedef struct ptg_stats {
   uint64_t safe_balls;      /* FP32 kernel: safe balls computed                 */
   uint64_t coop_rounds;     /* FP32 kernel: warp-cooperative rounds             */
   uint64_t coop_flights;    /* FP32 kernel: p-p flights taken in those rounds   */
+  uint64_t box_tests;       /* FP32 kernel: BVH node boxes tested (32-bit lane  */
+                            /*   counters: exact below 2^32 tests per thread)   */
+  uint64_t surface_tests;   /* FP32 kernel: grain surfaces tested (box faces    */
+                            /*   are one slab test and not counted)             */
 } ptg_stats;
 
 typedef struct ptg_handle ptg_handle;
@@ -320,6 +327,34 @@ int ptg_kappa_from_counts(const ptg_geometry* geom, const ptg_spectrum* spec,
                           ptg_kappa_out* out);
 
 /*
+ * The reference's result files from the counts of a run: replaces fileoutput
+ * (src/RTMCphon.f90:2601-2881), called after RayTrace's MFP loop with
+ * SEMFP from effectiveMFP (:2418-2451).  Writes thermalproperty.out,
+ * effectiveMFP.out and phononconductivity.out in the directory of geofile
+ * (the .mcp path, as the reference derives it, :2629-2632), with the
+ * reference's record layouts and Fortran edit descriptors; only
+ * thermalproperty.out when geom->nmaterial > 1, as the reference.
+ * Returns PTG_ERR_IO when a file cannot be written.
+ */
+int ptg_write_outputs(const char* geofile, const ptg_geometry* geom, const ptg_spectrum* spec,
+                      const ptg_run* run, const uint64_t* counts);
+/*
+ * Interface parameter of a "TBC" transmission entry: GammaDeterm
+ * (src/RTMCphon.f90:2499-2599, called from the .mcp reader at :856-873).
+ * Newton's method for the gamma whose transmissivity
+ * T = 1/(gamma omega/omega_max + 1) over the modes of `material` gives the
+ * boundary conductance tbc [W m^-2 K^-1] (the .mcp value times 1e6, as
+ * ptg_mcp_load stores it in tt_trans); the result goes into tt_trans in
+ * place of the conductance.  PTG_ERR_INVALID when gamma < 0 ("Gamma cannot
+ * determine").
+ */
+int ptg_gamma_from_tbc(const ptg_spectrum* material, double temperature, double tbc,
+                       double* gamma);
+/* The writer's rendering of one Fortran edit descriptor (kind 0: Iw,
+   1: Fw.d with w = 0 for F0.d, 2: Ew.d) into out (cap bytes, NUL ended). */
+int ptg_fortran_format(int32_t kind, double v, int32_t w, int32_t d, char* out, int32_t cap);
+
+/*
  * Adjoint (path-reweighting) derivatives of kappa.  A forward pass of the
  * persistent FP32 kernel records which samples leave through x+; a second
  * pass re-generates exactly those trajectories from their Philox counters
@@ -379,6 +414,49 @@ void ptg_batch_destroy(ptg_batch* b);
 
 /* Statistics of the last transport call on h. */
 int ptg_last_stats(const ptg_handle* h, ptg_stats* st);
+
+/*
+ * Trajectory trace by replay: replaces the trace.out output of calcTransmit
+ * (src/RTMCphon.f90:1661-1665, 1818-1831, file set-up :3373-3383), which
+ * the reference writes from inside its hot loop.  Here the transport
+ * kernels write nothing per flight; ptg_trace re-generates the FP32
+ * trajectories of the listed samples (global sample ids task * np + p of
+ * the run's numbering) from their Philox counters, one lane per sample with
+ * the full intersection test on every flight (the same trajectory as any
+ * other path of the kernel), and returns per sample the number of
+ * positions npos (emission point + one per free flight), the exit side
+ * (0 lost, 1 x-, 2 x+) and, when pos is not NULL, the positions
+ * (3 floats each, sample i at the running sum of the earlier npos); a
+ * buffer smaller than the sum of npos gives PTG_ERR_INVALID with npos and
+ * end_side filled.  ptg_write_trace picks particle_trace samples every
+ * interval_trace = ntask * np / particle_trace ids (the reference's
+ * interval, one rank) and writes the reference's trace.out: its header,
+ * one record per position (x y z as FP32 values, 9 significant digits),
+ * two blank records after each phonon.
+ */
+int ptg_trace(ptg_handle* h, const ptg_run* run, int64_t n, const uint64_t* samples,
+              int64_t cap_positions, float* pos, int64_t* npos, int32_t* end_side);
+int ptg_write_trace(ptg_handle* h, const ptg_run* run, int32_t particle_trace, const char* path);
+
+/*
+ * Options of a live handle and the autotuner - no counterpart in the
+ * reference, whose OpenMP loop has a fixed static schedule
+ * (src/RTMCphon.f90:1573).
+ *
+ * ptg_set_options replaces the handle's options (same device); a new
+ * bvh_leaf rebuilds the device geometry.  ptg_autotune times ptg_kappa with
+ * `run` in FP32 (best of `reps` calls per trial) while it varies, one at a
+ * time, bvh_leaf (when a grain has a BVH), block_size, blocks_per_sm,
+ * coop_lanes, long_flights, fast_steps, regen_threshold and chunk; it leaves the fastest
+ * options on the handle and in *best, with their kernel time in *best_ms.
+ * Trajectories depend only on their Philox counters, so no option changes a
+ * result.  The call runs about 20 trials of the given run: tune on a run
+ * with fewer particles when the full one is long.
+ */
+int ptg_get_options(const ptg_handle* h, ptg_options* out);
+int ptg_set_options(ptg_handle* h, const ptg_options* opt);
+int ptg_autotune(ptg_handle* h, const ptg_run* run, int32_t reps, ptg_options* best,
+                 double* best_ms);
 
 /*
  * ptg_transmission_noalloc - no counterpart in the reference; an addition for

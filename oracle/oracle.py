@@ -51,6 +51,8 @@ def lib():
                                  C.POINTER(C.c_int64), C.c_int64, U64P, U64P, C.POINTER(OrcResult)]
     L.orc_replay_task.argtypes = [vp, C.POINTER(A.PtgRun), C.c_int64, C.c_int64, I32P, U32P, F64P]
     L.orc_kappa_from_counts.argtypes = [vp, C.POINTER(A.PtgRun), U64P, C.POINTER(A.PtgKappaOut)]
+    L.orc_write_outputs.argtypes = [vp, C.c_char_p, C.POINTER(A.PtgRun), U64P]
+    L.orc_gamma_from_tbc.argtypes = [vp, C.c_double, C.c_double, C.POINTER(C.c_double)]
     L.orc_philox.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
     L.orc_philox.restype = None
     L.orc_log.argtypes = [C.c_double]
@@ -145,6 +147,19 @@ class Oracle:
         if st != 0:
             raise RuntimeError(f"oracle replay failed: status {st}")
         return es, fl, fp.reshape(n, 3)
+
+    def gamma_from_tbc(self, temperature, tbc):
+        """GammaDeterm: (status, gamma)."""
+        g = C.c_double(0.0)
+        st = self.L.orc_gamma_from_tbc(self.h, temperature, tbc, C.byref(g))
+        return st, g.value
+
+    def write_outputs(self, geofile, run, counts):
+        """fileoutput's three files next to geofile."""
+        c = np.ascontiguousarray(counts, dtype=np.uint64)
+        st = self.L.orc_write_outputs(self.h, geofile.encode(), C.byref(run), _p(c, C.c_uint64))
+        if st != 0:
+            raise RuntimeError(f"orc_write_outputs: status {st}")
 
     def kappa(self, run, counts):
         from ptrans_b200 import abi as A

@@ -32,7 +32,10 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#include <algorithm>
 #include <chrono>
+#include <cstdio>
+#include <string>
 #include <vector>
 
 namespace {
@@ -1093,3 +1096,270 @@ double orc_log(double x) { return orc::log_pos(x); }
 void orc_sincos2pi(double u, double* s, double* c) { orc::sincos_2pi(u, s, c); }
 
 }  // extern "C"
+
+/* ------------------------------------------------------------------------ */
+/* fileoutput's files, src/RTMCphon.f90:2601-2881, restated with the
+   reference's exchange sorts and gfortran's rendering of its edit
+   descriptors (Iw right-justified or asterisks; Fw.d; Ew.d as 0.ddE+xx,
+   +xxx past two exponent digits). */
+namespace {
+
+std::string orc_rjust(const std::string& s, int w) {
+  return (w > 0 && (int)s.size() < w) ? std::string(w - s.size(), ' ') + s : s;
+}
+
+std::string orc_I(long long v, int w) {
+  char b[64];
+  snprintf(b, sizeof(b), "%lld", v);
+  std::string s = b;
+  return (int)s.size() > w ? std::string(w, '*') : orc_rjust(s, w);
+}
+
+std::string orc_F(double v, int w, int d) {
+  char b[512];
+  snprintf(b, sizeof(b), "%.*f", d, v);
+  std::string s = b;
+  if (w == 0) return s;
+  if ((int)s.size() > w && s.compare(0, 2, "0.") == 0) s.erase(0, 1);
+  if ((int)s.size() > w && s.compare(0, 3, "-0.") == 0) s.erase(1, 1);
+  return (int)s.size() > w ? std::string(w, '*') : orc_rjust(s, w);
+}
+
+std::string orc_E(double v, int w, int d) {
+  /* d significant digits of |v| as 0.d1..dd * 10^e */
+  std::string digits(d, '0');
+  int e = 0;
+  if (v != 0.0) {
+    char b[128];
+    snprintf(b, sizeof(b), "%.*e", d - 1, fabs(v));
+    std::string t = b;
+    size_t ep = t.find('e');
+    std::string m = t.substr(0, ep);
+    m.erase(std::remove(m.begin(), m.end(), '.'), m.end());
+    digits = m;
+    e = atoi(t.c_str() + ep + 1) + 1;
+  }
+  char x[16];
+  if (e >= -99 && e <= 99) snprintf(x, sizeof(x), "E%+03d", e);
+  else snprintf(x, sizeof(x), "%+04d", e);
+  const std::string sg = (v < 0.0) ? "-" : "";
+  std::string s = sg + "0." + digits + x;
+  if ((int)s.size() > w) s = sg + "." + digits + x;
+  return (int)s.size() > w ? std::string(w, '*') : orc_rjust(s, w);
+}
+
+}  // namespace
+
+extern "C" int orc_write_outputs(orc_handle* h, const char* geofile, const ptg_run* run,
+                                 const uint64_t* counts) {
+  if (!h || !geofile || !run_valid(h, run) || !counts) return PTG_ERR_INVALID;
+  const int nb = h->nb, nk = h->nk, na = run->nangle;
+  const int nmfp = (run->kind_mfp == PTG_MFP_GRID) ? run->nmfp : 1;
+  const int64_t nm = (int64_t)nb * nk;
+  const double T = run->temperature;
+  /* effectiveMFP: SEMFP(ik, ib, s) */
+  std::vector<double> vangle(na), WT(na);
+  for (int ia = 0; ia < na; ++ia) vangle[ia] = 0.0 + (double)ia / (double)(na - 1) * M_PI_2_D;
+  const double dS = (vangle[1] - vangle[0]) / 3.0 * 3.0 * 0.5 * h->box[0];
+  std::vector<double> SEMFP((size_t)nk * nb * nmfp);
+  auto sidx = [&](int ik, int ib, int s) { return (size_t)ik + (size_t)nk * ((size_t)ib + (size_t)nb * s); };
+  for (int s = 0; s < nmfp; ++s)
+    for (int ik = 0; ik < nk; ++ik)
+      for (int ib = 0; ib < nb; ++ib) {
+        for (int ia = 0; ia < na; ++ia) {
+          const double tr = (ia < na - 1)
+              ? (double)counts[ib + (int64_t)nb * ik + nm * (s + (int64_t)nmfp * ia)] / (double)run->np
+              : 0.0;
+          WT[ia] = sin(vangle[ia]) * cos(vangle[ia]) * tr;
+        }
+        double I = 0.0;
+        for (int ia = 2; ia <= na - 1; ia += 2) I = I + (WT[ia - 2] + 4.0 * WT[ia - 1] + WT[ia]);
+        SEMFP[sidx(ik, ib, s)] = I * dS;
+      }
+  std::string g = geofile;
+  size_t c = g.rfind('/');
+  if (c == std::string::npos) c = g.rfind('\\');
+  const std::string pre = (c == std::string::npos) ? "" : g.substr(0, c + 1);
+  std::string f41 = "# Datatype = thermalproperty\n";
+  f41 += "# Incident_Phonon                               =   " + orc_I(run->np, 6) + "\n";
+  if (h->nmaterial > 1) {
+    f41 += "# Effective_MeanFreePath [nm]       = " + orc_E(SEMFP[0], 20, 10) + "\n";
+    FILE* f = fopen((pre + "thermalproperty.out").c_str(), "w");
+    if (!f) return PTG_ERR_IO;
+    fputs(f41.c_str(), f);
+    fclose(f);
+    return PTG_OK;
+  }
+  double ssum = 0.0;
+  for (double v : SEMFP) ssum += v;
+  f41 += "# Averaged Effective_MeanFreePath [nm]          = " +
+         orc_F(ssum / (nb * nk * nmfp), 20, 10) + "\n";
+  /* anphon copies (ii = branch, jj = k-point), tau rescale, MFP */
+  const double scale = (run->scatter_scale > 0.0) ? run->scatter_scale : 1.0;
+  std::vector<double> om(h->omega), wt(h->weight), ta(h->tau), ve(h->vel), mf(nm);
+  auto A = [&](int ii, int jj) { return (size_t)ii + (size_t)nb * jj; };
+  for (int jj = 0; jj < nk; ++jj)
+    for (int ii = 0; ii < nb; ++ii) {
+      ta[A(ii, jj)] = ta[A(ii, jj)] * 1.0e-12 * (h->rtemp / T);
+      mf[A(ii, jj)] = ta[A(ii, jj)] * ve[A(ii, jj)] / scale;
+    }
+  double wsum = 0.0;
+  for (double v : wt) wsum += v;
+  const int nqfbz = (int)(wsum / nb);
+  for (int ii = 0; ii < nb; ++ii)
+    for (int jj = 0; jj < nk - 1; ++jj)
+      for (int kk = jj + 1; kk < nk; ++kk)
+        if (om[A(ii, jj)] > om[A(ii, kk)]) {
+          std::swap(om[A(ii, jj)], om[A(ii, kk)]);
+          std::swap(wt[A(ii, jj)], wt[A(ii, kk)]);
+          std::swap(ta[A(ii, jj)], ta[A(ii, kk)]);
+          std::swap(ve[A(ii, jj)], ve[A(ii, kk)]);
+          std::swap(mf[A(ii, jj)], mf[A(ii, kk)]);
+          for (int s = 0; s < nmfp; ++s) std::swap(SEMFP[sidx(jj, ii, s)], SEMFP[sidx(kk, ii, s)]);
+        }
+  std::vector<double> cap(nm), EMFP(nm), TC(nm);
+  for (int ii = 0; ii < nb; ++ii)
+    for (int jj = 0; jj < nk; ++jj) {
+      const double x = HBAR * om[A(ii, jj)] / (KB * T);
+      cap[A(ii, jj)] = (x <= 1.0e-10) ? KB : KB * (((x / 2) / sinh(x / 2)) * ((x / 2) / sinh(x / 2)));
+    }
+  for (int ii = 0; ii < nb; ++ii)
+    for (int jj = 0; jj < nk; ++jj) {
+      const double m = mf[A(ii, jj)];
+      double E;
+      if (run->kind_mfp == PTG_MFP_MATTHIESSEN) {
+        E = (m == 0.0) ? SEMFP[sidx(jj, ii, 0)] * 1.0e-9
+                       : 1.0 / (1.0 / m + 1.0 / (SEMFP[sidx(jj, ii, 0)] * 1.0e-9));
+      } else if (run->kind_mfp == PTG_MFP_PER_MODE) {
+        E = SEMFP[sidx(jj, ii, 0)] * 1.0e-9;
+      } else {
+        const double* v = run->mfp_grid_nm;
+        E = SEMFP[sidx(jj, ii, nmfp - 1)] * 1.0e-9;
+        if (m < v[0] * 1.0e-9) {
+          E = SEMFP[sidx(jj, ii, 0)] * 1.0e-9 * m / (v[0] * 1.0e-9);
+        } else if (!(m > v[nmfp - 1] * 1.0e-9)) {
+          for (int s = 0; s < nmfp - 1; ++s)
+            if (v[s] * 1.0e-9 <= m && m < v[s + 1] * 1.0e-9) {
+              const double ip = (m - v[s] * 1.0e-9) / ((v[s + 1] - v[s]) * 1.0e-9);
+              E = SEMFP[sidx(jj, ii, s)] * 1.0e-9 * (1.0 - ip) + SEMFP[sidx(jj, ii, s + 1)] * 1.0e-9 * ip;
+              break;
+            }
+        }
+      }
+      EMFP[A(ii, jj)] = E;
+      TC[A(ii, jj)] = cap[A(ii, jj)] * wt[A(ii, jj)] * EMFP[A(ii, jj)] * ve[A(ii, jj)] / 3 / h->vol / nqfbz;
+    }
+  double ktot = 0.0;
+  for (size_t i = 0; i < (size_t)nm; ++i) ktot += TC[i];  /* column-major sum(TC(:,:)) */
+  f41 += "# Thermal_conductivity@" + orc_F(T, 0, 6) + "K [W m-1 K-1]  = " + orc_F(ktot, 20, 10) + "\n";
+  {
+    FILE* f = fopen((pre + "thermalproperty.out").c_str(), "w");
+    if (!f) return PTG_ERR_IO;
+    fputs(f41.c_str(), f);
+    fclose(f);
+  }
+  /* effectiveMFP.out */
+  struct Rec { int ib, ik; double bulk, eff, cond, acc; };
+  std::vector<Rec> vd;
+  for (int ii = 0; ii < nb; ++ii)
+    for (int jj = 0; jj < nk; ++jj)
+      vd.push_back({ii + 1, jj + 1, mf[A(ii, jj)], EMFP[A(ii, jj)], TC[A(ii, jj)], 0.0});
+  const int cf = (int)vd.size();
+  for (int ii = 0; ii < cf; ++ii)
+    for (int jj = ii + 1; jj < cf; ++jj)
+      if (vd[ii].eff > vd[jj].eff) std::swap(vd[ii], vd[jj]);
+  vd[0].acc = vd[0].cond;
+  for (int ii = 1; ii < cf; ++ii) vd[ii].acc = vd[ii].cond + vd[ii - 1].acc;
+  {
+    FILE* f = fopen((pre + "effectiveMFP.out").c_str(), "w");
+    if (!f) return PTG_ERR_IO;
+    fputs("# Datatype = Effective Mean Free Path of phonon.\n", f);
+    fputs("# data are sorted by effective MFP in ascending order.\n", f);
+    fprintf(f, "#   total branches: %s\n", orc_I(nb, 3).c_str());
+    fprintf(f, "#   total Kpoints:  %s\n", orc_I(nk, 3).c_str());
+    fputs("#\n", f);
+    fputs("# branch, kpoint, bulk MFP[nm], effective MFP[nm], ThermalConductivity, and its accumulated[W m-1 K-1].\n", f);
+    for (const Rec& r : vd)
+      fprintf(f, "%s%s%s%s%s%s\n", orc_I(r.ib, 5).c_str(), orc_I(r.ik, 5).c_str(),
+              orc_E(r.bulk * 1.0e9, 15, 6).c_str(), orc_E(r.eff * 1.0e9, 15, 6).c_str(),
+              orc_E(r.cond, 15, 6).c_str(), orc_E(r.acc, 15, 6).c_str());
+    fclose(f);
+  }
+  /* phononconductivity.out */
+  std::vector<double> so;
+  for (int ii = 0; ii < nb; ++ii)
+    for (int jj = 0; jj < nk; ++jj) {
+      bool dup = false;
+      for (double v : so) if (v == om[A(ii, jj)]) { dup = true; break; }
+      if (!dup) so.push_back(om[A(ii, jj)]);
+    }
+  const int nf = (int)so.size();
+  for (int ii = 0; ii < nf - 1; ++ii)
+    for (int jj = ii + 1; jj < nf; ++jj)
+      if (so[ii] > so[jj]) std::swap(so[ii], so[jj]);
+  FILE* f = fopen((pre + "phononconductivity.out").c_str(), "w");
+  if (!f) return PTG_ERR_IO;
+  fputs("# Datatype = phononconductivity\n", f);
+  fprintf(f, "# Nb = %s\n", orc_I(nf - 1, 6).c_str());
+  fprintf(f, "# Nbranch = %s\n", orc_I(nb, 4).c_str());
+  fputs("# omega, fluxphononout(1:Nbranch)\n", f);
+  for (int ii = 0; ii < nf - 1; ++ii) {
+    fputs(orc_E(so[ii], 20, 10).c_str(), f);
+    for (int jj = 0; jj < nb; ++jj) {
+      double k = 0.0;
+      for (int kk = 0; kk < nk; ++kk)
+        if (om[A(jj, kk)] == so[ii]) k = k + TC[A(jj, kk)];
+      fputs(orc_E(k, 20, 10).c_str(), f);
+    }
+    fputs("\n", f);
+  }
+  fclose(f);
+  return PTG_OK;
+}
+
+/* GammaDeterm with ModeNum = 1, src/RTMCphon.f90:2499-2560, on the handle's
+   spectrum (the material's anphon). */
+extern "C" int orc_gamma_from_tbc(orc_handle* h, double temperature, double TBC, double* gamma) {
+  if (!h || !gamma) return PTG_ERR_INVALID;
+  const int nbranch = h->nb, nkpoint = h->nk;
+  std::vector<double> cap((size_t)nbranch * nkpoint, 0.0);
+  double wsum = 0.0;
+  for (double w : h->weight) wsum += w;
+  const int nqfbz = (int)(wsum / nbranch);
+  auto X = [&](const std::vector<double>& a, int b, int k) { return a[(size_t)b + (size_t)nbranch * k]; };
+  for (int ii = 0; ii < nkpoint; ++ii)
+    for (int jj = 0; jj < nbranch; ++jj) {
+      const double tmpX = HBAR * X(h->omega, jj, ii) / (KB * temperature);
+      cap[(size_t)jj + (size_t)nbranch * ii] =
+          (tmpX <= 1.0e-10) ? KB : KB * (((tmpX / 2) / sinh(tmpX / 2)) * ((tmpX / 2) / sinh(tmpX / 2)));
+    }
+  const double maxOmega = h->max_omega;
+  double tmpGamma = 1.0e-2;
+  for (int it = 1; it <= 10000; ++it) {
+    double tmpTBC = 0.0, tmpTBCa = 0.0, tmpdTBC = 0.0;
+    for (int jj = 0; jj < nkpoint; ++jj)
+      for (int kk = 0; kk < nbranch; ++kk) {
+        const double tmpH = 1 / (tmpGamma * (X(h->omega, kk, jj) / maxOmega) + 1);
+        tmpTBC = tmpTBC + X(h->weight, kk, jj) * X(cap, kk, jj) * X(h->vel, kk, jj) * tmpH / 2 / h->vol / nqfbz;
+      }
+    for (int jj = 0; jj < nkpoint; ++jj)
+      for (int kk = 0; kk < nbranch; ++kk) {
+        const double tmpH = 1;
+        tmpTBCa = tmpTBCa + X(h->weight, kk, jj) * X(cap, kk, jj) * X(h->vel, kk, jj) * tmpH / 2 / h->vol / nqfbz;
+      }
+    for (int jj = 0; jj < nkpoint; ++jj)
+      for (int kk = 0; kk < nbranch; ++kk) {
+        const double den = tmpGamma * (X(h->omega, kk, jj) / maxOmega) + 1;
+        const double tmpH = -(X(h->omega, kk, jj) / maxOmega) / (den * den);
+        tmpdTBC = tmpdTBC + X(h->weight, kk, jj) * X(cap, kk, jj) * X(h->vel, kk, jj) * tmpH / 2 / h->vol / nqfbz;
+      }
+    const double tmpF = tmpTBC / (1 - tmpTBC / tmpTBCa) - TBC;
+    const double one = 1 - tmpTBC / tmpTBCa;
+    const double tmpdF = tmpdTBC / (one * one);
+    const double differential = tmpF / tmpdF;
+    if (fabs(differential) <= 1.0e-6) break;
+    tmpGamma = tmpGamma - differential;
+  }
+  *gamma = tmpGamma;
+  return tmpGamma < 0.0 ? PTG_ERR_INVALID : PTG_OK;
+}

@@ -68,6 +68,13 @@ int orc_replay_task(orc_handle* h, const ptg_run* run, int64_t task, int64_t max
 int orc_kappa_from_counts(orc_handle* h, const ptg_run* run, const uint64_t* counts,
                           ptg_kappa_out* out);
 
+/* fileoutput's thermalproperty.out, effectiveMFP.out and
+   phononconductivity.out next to geofile, from the counts of a run. */
+int orc_write_outputs(orc_handle* h, const char* geofile, const ptg_run* run,
+                      const uint64_t* counts);
+/* GammaDeterm (ModeNum 1): gamma of T(omega) = 1/(gamma omega/omega_max + 1)
+   whose boundary conductance is TBC [W m^-2 K^-1], on the handle's spectrum. */
+int orc_gamma_from_tbc(orc_handle* h, double temperature, double TBC, double* gamma);
 /* Raw Philox4x32-10 block (for known-answer tests). */
 void orc_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 /* The oracle's log and sincos(2*pi*u) (checked against libm in tests). */

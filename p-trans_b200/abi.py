@@ -86,6 +86,7 @@ class PtgOptions(C.Structure):
         ("regen_threshold", C.c_int32), ("ref_quirks", C.c_int32), ("bvh_leaf", C.c_int32),
         ("max_flights", C.c_int64), ("lost_limit", C.c_double), ("chunk", C.c_int64),
         ("tune_flags", C.c_int32), ("fast_steps", C.c_int32), ("coop_lanes", C.c_int32),
+        ("long_flights", C.c_int32),
     ]
 
 
@@ -117,6 +118,7 @@ class PtgStats(C.Structure):
         ("max_traj_flights", C.c_uint64), ("drain_ms", C.c_double), ("tail_ms", C.c_double),
         ("full_flights", C.c_uint64), ("safe_balls", C.c_uint64),
         ("coop_rounds", C.c_uint64), ("coop_flights", C.c_uint64),
+        ("box_tests", C.c_uint64), ("surface_tests", C.c_uint64),
     ]
 
 
@@ -179,6 +181,18 @@ SIGNATURES = {
     "ptg_kappa_from_counts": (C.c_int, [C.POINTER(PtgGeometry), C.POINTER(PtgSpectrum),
                                         C.POINTER(PtgRun), U64P, C.POINTER(PtgKappaOut)]),
     "ptg_last_stats": (C.c_int, [C.c_void_p, C.POINTER(PtgStats)]),
+    "ptg_write_outputs": (C.c_int, [C.c_char_p, C.POINTER(PtgGeometry), C.POINTER(PtgSpectrum),
+                                    C.POINTER(PtgRun), U64P]),
+    "ptg_gamma_from_tbc": (C.c_int, [C.POINTER(PtgSpectrum), C.c_double, C.c_double, F64P]),
+    "ptg_fortran_format": (C.c_int, [C.c_int32, C.c_double, C.c_int32, C.c_int32, C.c_char_p,
+                                     C.c_int32]),
+    "ptg_trace": (C.c_int, [C.c_void_p, C.POINTER(PtgRun), C.c_int64, U64P, C.c_int64, C.POINTER(C.c_float),
+                            C.POINTER(C.c_int64), I32P]),
+    "ptg_write_trace": (C.c_int, [C.c_void_p, C.POINTER(PtgRun), C.c_int32, C.c_char_p]),
+    "ptg_get_options": (C.c_int, [C.c_void_p, C.POINTER(PtgOptions)]),
+    "ptg_set_options": (C.c_int, [C.c_void_p, C.POINTER(PtgOptions)]),
+    "ptg_autotune": (C.c_int, [C.c_void_p, C.POINTER(PtgRun), C.c_int32, C.POINTER(PtgOptions),
+                               F64P]),
     "ptg_replay_task": (C.c_int, [C.c_void_p, C.POINTER(PtgRun), C.c_int64, I32P, U32P, F64P]),
     "ptg_adjoint": (C.c_int, [C.c_void_p, C.POINTER(PtgRun), C.POINTER(PtgAdjointOut)]),
     "ptg_batch_create": (C.c_int, [C.POINTER(PtgBatchItem), C.c_int32, C.POINTER(PtgSpectrum),
@@ -544,6 +558,60 @@ class Handle:
         _check(self.lib.ptg_last_stats(self.h, C.byref(s)), "ptg_last_stats")
         return {k: getattr(s, k) for k, _ in PtgStats._fields_}
 
+    def trace(self, run: PtgRun, samples) -> list:
+        """ptg_trace: per sample (positions [npos, 3] float32, exit side)."""
+        smp = np.ascontiguousarray(samples, dtype=np.uint64)
+        n = smp.size
+        npos = np.zeros(n, np.int64)
+        ends = np.zeros(n, np.int32)
+        _check(self.lib.ptg_trace(self.h, C.byref(run), n, _ptr(smp, C.c_uint64), 0, None,
+                                  _ptr(npos, C.c_int64), _ptr(ends, C.c_int32)), "ptg_trace")
+        tot = int(npos.sum())
+        pos = np.zeros(3 * max(tot, 1), np.float32)
+        _check(self.lib.ptg_trace(self.h, C.byref(run), n, _ptr(smp, C.c_uint64), tot, _ptr(pos, C.c_float),
+                                  _ptr(npos, C.c_int64), _ptr(ends, C.c_int32)), "ptg_trace")
+        out, k = [], 0
+        for i in range(n):
+            out.append((pos[3 * k:3 * (k + npos[i])].reshape(-1, 3), int(ends[i])))
+            k += int(npos[i])
+        return out
+
+    def write_trace(self, run: PtgRun, particle_trace: int, path: str) -> None:
+        _check(self.lib.ptg_write_trace(self.h, C.byref(run), particle_trace, path.encode()), "ptg_write_trace")
+
+    def options(self) -> dict:
+        o = PtgOptions()
+        _check(self.lib.ptg_get_options(self.h, C.byref(o)), "ptg_get_options")
+        return {k: getattr(o, k) for k, _ in PtgOptions._fields_}
+
+    def set_options(self, **kw):
+        o = PtgOptions()
+        _check(self.lib.ptg_get_options(self.h, C.byref(o)), "ptg_get_options")
+        for k, v in kw.items():
+            setattr(o, k, v)
+        _check(self.lib.ptg_set_options(self.h, C.byref(o)), "ptg_set_options")
+
+    def autotune(self, run: PtgRun, reps: int = 2, cache: Optional[str] = None, key: str = "") -> dict:
+        """ptg_autotune; with `cache` (a JSON file) the options found for `key`
+        are stored there and reused (applied without timing) on later calls."""
+        import json
+        if cache and key and os.path.exists(cache):
+            data = json.load(open(cache))
+            if key in data:
+                self.set_options(**data[key]["options"])
+                return dict(data[key], cached=True)
+        o = PtgOptions()
+        ms = C.c_double(0.0)
+        _check(self.lib.ptg_autotune(self.h, C.byref(run), reps, C.byref(o), C.byref(ms)), "ptg_autotune")
+        res = {"options": {k: getattr(o, k) for k, _ in PtgOptions._fields_}, "kernel_ms": ms.value,
+               "cached": False}
+        if cache and key:
+            data = json.load(open(cache)) if os.path.exists(cache) else {}
+            data[key] = {"options": res["options"], "kernel_ms": res["kernel_ms"]}
+            with open(cache, "w") as f:
+                json.dump(data, f, indent=1, sort_keys=True)
+        return res
+
     def replay_task(self, run: PtgRun, task: int):
         npl = len(range(run.rank, run.np, run.nranks))
         es = np.zeros(npl, np.int32)
@@ -632,6 +700,35 @@ def kappa_from_counts(geometry: PtgGeometry, spectrum: Spectrum, run: PtgRun, co
     _check(st, "ptg_kappa_from_counts")
     return {"kappa": out.kappa, "kappa_stderr": out.kappa_stderr, "bin_T": bt[: run.nbins],
             "bin_T_stderr": be[: run.nbins], "emfp_nm": em}
+
+
+def write_outputs(geofile: str, geometry: PtgGeometry, spectrum: Spectrum, run: PtgRun,
+                  counts: np.ndarray) -> None:
+    """ptg_write_outputs: thermalproperty.out, effectiveMFP.out and
+    phononconductivity.out in the directory of geofile."""
+    lib = load_library()
+    cs = spectrum.to_c()
+    c = np.ascontiguousarray(counts, dtype=np.uint64)
+    _check(lib.ptg_write_outputs(geofile.encode(), C.byref(geometry), C.byref(cs), C.byref(run),
+                                 _ptr(c, C.c_uint64)), "ptg_write_outputs")
+
+
+def gamma_from_tbc(material: Spectrum, temperature: float, tbc: float):
+    """ptg_gamma_from_tbc: (status, gamma) for a conductance tbc [W m^-2 K^-1]."""
+    lib = load_library()
+    cs = material.to_c()
+    g = C.c_double(0.0)
+    st = lib.ptg_gamma_from_tbc(C.byref(cs), temperature, tbc, C.byref(g))
+    return st, g.value
+
+
+def fortran_format(kind: str, v: float, w: int, d: int = 0) -> str:
+    """The writer's rendering of an I / F / E edit descriptor."""
+    lib = load_library()
+    buf = C.create_string_buffer(256)
+    k = {"I": 0, "F": 1, "E": 2}[kind]
+    _check(lib.ptg_fortran_format(k, float(v), w, d, buf, 256), "ptg_fortran_format")
+    return buf.value.decode()
 
 
 def mcp_load(path: str):

@@ -79,12 +79,15 @@ struct ptg_handle {
       red_emfp, red_trans, red_result;
   /* adjoint: list of transmitted samples, per-sample weights, accumulators */
   DevBuf adj_list, adj_w, adj_acc;
+  /* trace replay: position offsets, counts, exit sides, positions */
+  DevBuf tr_off, tr_npos, tr_end, tr_pos;
   unsigned long long list_n = 0, mismatch = 0;
   ~ptg_handle() {
     for (DevBuf* b : owned) { b->release(); delete b; }
     DevBuf* all[] = {&blob, &task, &chunk, &counts, &lost, &stats, &queue, &red_coef, &red_K,
                      &red_W, &red_mfp, &red_bin, &red_grid, &red_tc, &red_kv, &red_bw, &red_bv,
-                     &red_emfp, &red_trans, &red_result, &adj_list, &adj_w, &adj_acc};
+                     &red_emfp, &red_trans, &red_result, &adj_list, &adj_w, &adj_acc,
+                     &tr_off, &tr_npos, &tr_end, &tr_pos};
     for (DevBuf* b : all) b->release();
     for (cudaEvent_t e : ev) if (e) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);
@@ -123,8 +126,8 @@ inline float4 i4(int a, int b, int c, int d) {
 namespace ptg {
 
 /* The FP32 geometry blob of a built geometry (host copy) and its layout. */
-int blob_from_geometry(const GeomSoA& G, std::vector<float4>* out, BlobLayout* lay_out,
-                       std::string* why) {
+int blob_from_geometry(const GeomSoA& G, int bvh_leaf, std::vector<float4>* out,
+                       BlobLayout* lay_out, std::string* why) {
   const int ns = G.nsurf(), ngt = G.ngrain_total();
   std::vector<float4> hot(2 * (size_t)ns), cold(3 * (size_t)ns), edges;
   std::vector<int> geom_id(ns);
@@ -206,6 +209,51 @@ int blob_from_geometry(const GeomSoA& G, std::vector<float4>* out, BlobLayout* l
       if (G.internal[s]) cand.push_back(s);
   }
   cb[ngt] = (int)cand.size();
+  /* BVH over the candidates of every large grain; its leaves reorder the
+     grain's candidate list */
+  std::vector<int> root(ngt, -1);
+  std::vector<float4> nodes;
+  if (bvh_leaf >= 0) {
+    const int leaf = bvh_leaf > 0 ? bvh_leaf : kBvhDefaultLeaf;
+    const double S = std::max(G.box[0], std::max(G.box[1], G.box[2]));
+    const double pad = 4.0 * S / 1048576.0;  /* 4 eps of the FP32 tests */
+    for (int g = 1; g < ngt; ++g) {
+      const int n = cb[g + 1] - cb[g];
+      if (n <= kBvhMinCand) continue;
+      std::vector<float> lo(3 * (size_t)n), hi(3 * (size_t)n);
+      for (int i = 0; i < n; ++i) {
+        const int s = cand[cb[g] + i];
+        double l[3], h[3];
+        if (G.shape[s] == PTG_SHAPE_POLYGON) {
+          for (int d = 0; d < 3; ++d) { l[d] = 1e300; h[d] = -1e300; }
+          const double* v = &G.vertex[3 * (size_t)G.vertex_begin[s]];
+          for (int k = 0; k < G.nvertex[s]; ++k)
+            for (int d = 0; d < 3; ++d) {
+              l[d] = std::min(l[d], v[3 * k + d]);
+              h[d] = std::max(h[d], v[3 * k + d]);
+            }
+        } else {
+          const double* c = &G.center[3 * s];
+          const double r = G.radius[s];
+          for (int d = 0; d < 3; ++d) { l[d] = c[d] - r; h[d] = c[d] + r; }
+          if (G.shape[s] == PTG_SHAPE_CYLINDER) { l[2] = 0.0; h[2] = G.box[2]; }
+        }
+        for (int d = 0; d < 3; ++d) {
+          /* rounded outwards after the pad */
+          lo[3 * i + d] = std::nextafter((float)(l[d] - pad), -3.0e38f);
+          hi[3 * i + d] = std::nextafter((float)(h[d] + pad), 3.0e38f);
+        }
+      }
+      std::vector<float4> gn;
+      std::vector<int> order;
+      const int node_base = (int)(nodes.size() / 2);
+      bvh_build(lo, hi, leaf, 30, cb[g], node_base, &gn, &order);
+      std::vector<int> seg(cand.begin() + cb[g], cand.begin() + cb[g + 1]);
+      for (int i = 0; i < n; ++i) cand[cb[g] + i] = seg[order[i]];
+      root[g] = node_base;
+      nodes.insert(nodes.end(), gn.begin(), gn.end());
+    }
+  }
   std::vector<float4> start;
   for (int g = 1; g <= G.ngrain; ++g) {
     if (!G.grain_incident[g]) continue;
@@ -227,7 +275,9 @@ int blob_from_geometry(const GeomSoA& G, std::vector<float4>* out, BlobLayout* l
   L.cand_begin = L.edge + (int)edges.size();
   L.cand = L.cand_begin + units_of_ints(cb.size());
   L.start = L.cand + units_of_ints(cand.size() ? cand.size() : 1);
-  L.total = L.start + (int)(start.size() ? start.size() : 1);
+  L.bvh_root = L.start + (int)(start.size() ? start.size() : 1);
+  L.bvh_node = L.bvh_root + units_of_ints(root.size());
+  L.total = L.bvh_node + (int)(nodes.size() ? nodes.size() : 1);
   L.nstart = (int)start.size();
   std::vector<float4> blob((size_t)L.total, make_float4(0, 0, 0, 0));
   std::copy(hot.begin(), hot.end(), blob.begin() + L.hot);
@@ -236,9 +286,21 @@ int blob_from_geometry(const GeomSoA& G, std::vector<float4>* out, BlobLayout* l
   memcpy(&blob[L.cand_begin], cb.data(), cb.size() * 4);
   if (!cand.empty()) memcpy(&blob[L.cand], cand.data(), cand.size() * 4);
   std::copy(start.begin(), start.end(), blob.begin() + L.start);
+  memcpy(&blob[L.bvh_root], root.data(), root.size() * 4);
+  std::copy(nodes.begin(), nodes.end(), blob.begin() + L.bvh_node);
   *out = std::move(blob);
   *lay_out = L;
   return PTG_OK;
+}
+
+bool handle_has_bvh(const ptg_handle* h) {
+  const GeomSoA& G = h->geom;
+  for (int g = 1; g < G.ngrain_total(); ++g) {
+    int n = 0;
+    for (int s = G.grain_begin[g]; s < G.grain_begin[g + 1]; ++s) n += G.internal[s] ? 1 : 0;
+    if (n > kBvhMinCand) return true;
+  }
+  return false;
 }
 
 }  // namespace ptg
@@ -250,7 +312,7 @@ int build_blob(ptg_handle* h) {
   std::vector<float4> blob;
   ptg::BlobLayout L;
   std::string why;
-  int st = ptg::blob_from_geometry(G, &blob, &L, &why);
+  int st = ptg::blob_from_geometry(G, h->opt.bvh_leaf, &blob, &L, &why);
   if (st != PTG_OK) { h->last_error = why; return st; }
   h->blob_bytes = blob.size() * 16;
   CU(h->blob.ensure(h->blob_bytes));
@@ -324,6 +386,11 @@ struct Transport {
   long long alist_n = 0;
   const float* wsample = nullptr;
   double* adj = nullptr;
+  /* trace replay (mode 3) */
+  float* trace = nullptr;
+  const long long* trace_off = nullptr;
+  long long* trace_npos = nullptr;
+  int* trace_end = nullptr;
 };
 
 int run_transport(ptg_handle* h, const Transport& T) {
@@ -431,6 +498,11 @@ int run_transport(ptg_handle* h, const Transport& T) {
     r.fast_lambda_max = (float)(0.1 * lmin);
     /* tune_flags bit 1 turns the cooperative tail off; 0 selects 8 lanes */
     r.coop_lanes = (h->opt.tune_flags & 2) ? 0 : (h->opt.coop_lanes > 0 ? std::min(h->opt.coop_lanes, 32) : 8);
+    /* busy-warp promotion only when asked for (it slows the warps that
+       carry a promoted phonon more than it shortens the tail on the
+       thin-film workload) */
+    r.long_flights = (r.coop_lanes == 0 || h->opt.long_flights <= 0) ? 0u
+                                                                     : (uint32_t)h->opt.long_flights;
     r.counts = h->counts.as<unsigned long long>();
     r.lost = h->lost.as<unsigned long long>();
     r.stats = h->stats.as<unsigned long long>();
@@ -441,8 +513,13 @@ int run_transport(ptg_handle* h, const Transport& T) {
     r.alist_n = T.alist_n;
     r.wsample = T.wsample;
     r.adj = T.adj;
+    r.trace = T.trace;
+    r.trace_off = T.trace_off;
+    r.trace_npos = T.trace_npos;
+    r.trace_end = T.trace_end;
     r.nsurf = h->geom.nsurf();
-    const int block = 256;
+    const int bs = h->opt.block_size;
+    const int block = (bs >= 32 && bs <= 256 && bs % 32 == 0) ? bs : 256;
     const size_t smem = h->g32.stage_smem ? h->blob_bytes : 0;
     int bps = 0;
     CU(ptg::persistent_occupancy(block, smem, &bps, T.mode));
@@ -450,7 +527,8 @@ int run_transport(ptg_handle* h, const Transport& T) {
     if (bps < 1) bps = 1;
     const int grid = h->num_sms * bps;
     CU(cudaEventRecord(h->ev[0], h->stream));
-    const bool work = (T.mode == ptg::MODE_ADJOINT) ? T.alist_n > 0 : r.nchunk > 0;
+    const bool work = (T.mode == ptg::MODE_ADJOINT || T.mode == ptg::MODE_TRACE) ? T.alist_n > 0
+                                                                                   : r.nchunk > 0;
     if (work) CU(ptg::launch_persistent_fp32(h->g32, r, grid, block, smem, h->stream, T.mode));
     CU(cudaEventRecord(h->ev[1], h->stream));
     h->last.grid = grid;
@@ -479,6 +557,8 @@ int finish_stats(ptg_handle* h) {
   h->last.safe_balls = st[9];
   h->last.coop_rounds = st[12];
   h->last.coop_flights = st[13];
+  h->last.box_tests = st[14];
+  h->last.surface_tests = st[15];
   h->list_n = st[10];
   h->mismatch = st[11];
   if (st[5] != ~0ull && st[7] >= st[5]) {
@@ -721,6 +801,35 @@ int ptg_set_spectrum(ptg_handle* h, const ptg_spectrum* spec) {
   return PTG_OK;
 }
 
+int ptg_get_options(const ptg_handle* h, ptg_options* out) {
+  if (!h || !out) return PTG_ERR_INVALID;
+  *out = h->opt;
+  return PTG_OK;
+}
+
+int ptg_set_options(ptg_handle* h, const ptg_options* opt) {
+  if (!h || !opt) return PTG_ERR_INVALID;
+  if (opt->device != h->device) { h->last_error = "options name another device"; return PTG_ERR_INVALID; }
+  if (opt->block_size != 0 && (opt->block_size < 32 || opt->block_size > 256 || opt->block_size % 32)) {
+    h->last_error = "block_size must be 0 or a multiple of 32 up to 256";
+    return PTG_ERR_INVALID;
+  }
+  const bool rebuild = opt->bvh_leaf != h->opt.bvh_leaf;
+  const ptg_options old = h->opt;
+  h->opt = *opt;
+  if (rebuild) {
+    if (cudaSetDevice(h->device) != cudaSuccess) { h->opt = old; return PTG_ERR_CUDA; }
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) { h->opt = old; return PTG_ERR_CUDA; }
+    const int st = build_blob(h);
+    if (st != PTG_OK) {
+      h->opt = old;
+      build_blob(h);
+      return st;
+    }
+  }
+  return PTG_OK;
+}
+
 void ptg_destroy(ptg_handle* h) {
   if (!h) return;
   cudaSetDevice(h->device);
@@ -892,6 +1001,107 @@ int ptg_kappa_from_counts(const ptg_geometry* geom, const ptg_spectrum* spec, co
   if (ptg::copy_spectrum(spec, &S, &why) != PTG_OK) return PTG_ERR_INVALID;
   if (!ptg::run_valid(S, run, &why)) return PTG_ERR_INVALID;
   return ptg::assemble_host(S, run, geom->box[0], counts, out, nullptr, nullptr);
+}
+
+int ptg_trace(ptg_handle* h, const ptg_run* run, int64_t n, const uint64_t* samples,
+              int64_t cap_positions, float* pos, int64_t* npos, int32_t* end_side) {
+  if (!h || !run || n < 1 || !samples || !npos || !end_side) return PTG_ERR_INVALID;
+  std::string why;
+  if (!ptg::run_valid(h->spec, run, &why)) { h->last_error = why; return PTG_ERR_INVALID; }
+  std::vector<ptg::TaskHost> tasks;
+  ptg::run_tasks(h->spec, run, &tasks);
+  const uint64_t total = (uint64_t)tasks.size() * (uint64_t)run->np;
+  for (int64_t i = 0; i < n; ++i)
+    if (samples[i] >= total) { h->last_error = "sample id beyond ntask * np"; return PTG_ERR_INVALID; }
+  CU(cudaSetDevice(h->device));
+  CU(h->adj_list.ensure(sizeof(unsigned long long) * n));
+  CU(h->tr_npos.ensure(sizeof(long long) * n));
+  CU(h->tr_end.ensure(sizeof(int) * n));
+  CU(h->tr_off.ensure(sizeof(long long) * (n + 1)));
+  CU(cudaMemcpyAsync(h->adj_list.p, samples, sizeof(unsigned long long) * n, cudaMemcpyHostToDevice,
+                     h->stream));
+  Transport T;
+  T.ntask = (int64_t)tasks.size();
+  T.np = run->np;
+  T.np_local = 0;  /* no chunk queue: the kernel walks the replay list */
+  T.seed = run->seed;
+  T.stream = run->stream;
+  T.precision = PTG_PREC_FP32;
+  T.tasks = &tasks;
+  T.mode = ptg::MODE_TRACE;
+  T.alist = h->adj_list.as<const unsigned long long>();
+  T.alist_n = (long long)n;
+  T.trace_off = h->tr_off.as<const long long>();
+  T.trace_npos = h->tr_npos.as<long long>();
+  T.trace_end = h->tr_end.as<int>();
+  /* pass 1: lengths and exits */
+  int st = run_transport(h, T);
+  if (st != PTG_OK) return st;
+  std::vector<long long> cnt(n);
+  std::vector<int> ends(n);
+  CU(cudaMemcpyAsync(cnt.data(), h->tr_npos.p, sizeof(long long) * n, cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaMemcpyAsync(ends.data(), h->tr_end.p, sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream));
+  st = finish_stats(h);
+  if (st != PTG_OK) return st;
+  long long sum = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    npos[i] = cnt[i];
+    end_side[i] = ends[i];
+    sum += cnt[i];
+  }
+  if (!pos) return PTG_OK;
+  if (sum > cap_positions) { h->last_error = "position buffer smaller than the trajectories"; return PTG_ERR_INVALID; }
+  /* pass 2: the same trajectories, positions recorded at exclusive offsets */
+  std::vector<long long> off(n + 1, 0);
+  for (int64_t i = 0; i < n; ++i) off[i + 1] = off[i] + cnt[i];
+  CU(h->tr_pos.ensure(sizeof(float) * 3 * (size_t)(sum > 0 ? sum : 1)));
+  CU(cudaMemcpyAsync(h->tr_off.p, off.data(), sizeof(long long) * (n + 1), cudaMemcpyHostToDevice,
+                     h->stream));
+  T.trace = h->tr_pos.as<float>();
+  st = run_transport(h, T);
+  if (st != PTG_OK) return st;
+  CU(cudaMemcpyAsync(pos, h->tr_pos.p, sizeof(float) * 3 * (size_t)sum, cudaMemcpyDeviceToHost,
+                     h->stream));
+  st = finish_stats(h);
+  if (st != PTG_OK) return st;
+  h->last.d2h_bytes += sizeof(float) * 3 * (size_t)sum;
+  return PTG_OK;
+}
+
+int ptg_write_trace(ptg_handle* h, const ptg_run* run, int32_t particle_trace, const char* path) {
+  if (!h || !run || particle_trace < 1 || !path) return PTG_ERR_INVALID;
+  std::string why;
+  if (!ptg::run_valid(h->spec, run, &why)) { h->last_error = why; return PTG_ERR_INVALID; }
+  const uint64_t total = (uint64_t)ptg::run_ntask(h->spec, run) * (uint64_t)run->np;
+  /* interval_trace of RayTrace, src/RTMCphon.f90:3373-3375 (one rank) */
+  uint64_t interval = total / (uint64_t)particle_trace;
+  if (interval < 1) interval = 1;
+  std::vector<uint64_t> samples;
+  for (uint64_t k = 0; k < (uint64_t)particle_trace && k * interval < total; ++k)
+    samples.push_back(k * interval);
+  const int64_t n = (int64_t)samples.size();
+  std::vector<int64_t> npos(n);
+  std::vector<int32_t> ends(n);
+  int st = ptg_trace(h, run, n, samples.data(), 0, nullptr, npos.data(), ends.data());
+  if (st != PTG_OK) return st;
+  int64_t sum = 0;
+  for (int64_t v : npos) sum += v;
+  std::vector<float> pos(3 * (size_t)(sum > 0 ? sum : 1));
+  st = ptg_trace(h, run, n, samples.data(), sum, pos.data(), npos.data(), ends.data());
+  if (st != PTG_OK) return st;
+  FILE* f = fopen(path, "w");
+  if (!f) return PTG_ERR_IO;
+  fprintf(f, "# Datatype = trace\n");
+  fprintf(f, "# particle_trace = %8d\n", (int)particle_trace);
+  fprintf(f, "# interval_trace = %8lld\n", (long long)interval);
+  fprintf(f, "\n");
+  size_t k = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    for (int64_t j = 0; j < npos[i]; ++j, ++k)
+      fprintf(f, " %15.8E %15.8E %15.8E\n", pos[3 * k], pos[3 * k + 1], pos[3 * k + 2]);
+    fprintf(f, "\n\n");
+  }
+  return fclose(f) == 0 ? PTG_OK : PTG_ERR_IO;
 }
 
 int ptg_adjoint(ptg_handle* h, const ptg_run* run, ptg_adjoint_out* out) {

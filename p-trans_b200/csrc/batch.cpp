@@ -121,7 +121,7 @@ extern "C" int ptg_batch_create(const ptg_batch_item* items, int32_t nitems,
     if (ptg::copy_geometry(it.geom, &G, &why) != PTG_OK) { delete b; return PTG_ERR_INVALID; }
     std::vector<float4> blob;
     ptg::BlobLayout L;
-    if (ptg::blob_from_geometry(G, &blob, &L, &why) != PTG_OK) { delete b; return PTG_ERR_INVALID; }
+    if (ptg::blob_from_geometry(G, o.bvh_leaf, &blob, &L, &why) != PTG_OK) { delete b; return PTG_ERR_INVALID; }
     blob_off[g] = all_blob.size();
     all_blob.insert(all_blob.end(), blob.begin(), blob.end());
     ptg::GeoEntry& e = entries[g];

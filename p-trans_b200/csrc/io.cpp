@@ -225,7 +225,8 @@ int parse_mcp(Lines& L, ptg_mcpbuf* b) {
     double v2[2];
     if (!L.next(&line) || !read_doubles(line, 2, v2)) return PTG_ERR_IO;
     /* for TBC the first value is the conductance in MW m^-2 K^-1; the caller
-       converts it to gamma with ptg_gamma_from_tbc (GammaDeterm, :2499-2599) */
+       converts it to gamma with ptg_gamma_from_tbc (GammaDeterm, :2499-2599)
+       before building the geometry */
     b->tt_trans[k] = kind == PTG_TRANS_TBC ? v2[0] * 1.0e6 : v2[0];
     b->tt_spec[k] = v2[1];
   }

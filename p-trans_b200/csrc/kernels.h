@@ -81,6 +81,8 @@ struct BlobLayout {
   int cand_begin;   /* int[ngrain_total+1]                                           */
   int cand;         /* int[ncand]                                                    */
   int start;        /* voronoi: float4 (generatrix, grain); bricks: int2 (surf, grain) */
+  int bvh_root;     /* int[ngrain_total]: root node of the grain's BVH, -1 linear scan */
+  int bvh_node;     /* float4[2*nnode]: (lo, a) (hi, b), see bvh.cpp                  */
   int total;        /* blob size in 16-byte units                                    */
   int nstart;
 };
@@ -125,6 +127,8 @@ struct RunF32 {
   float fast_lambda_max;      /* tasks with a smaller MFP use the fast path           */
   int32_t coop_lanes;         /* warps with at most this many live lanes advance them
                                  cooperatively, 32 flights a round (0: off)       */
+  uint32_t long_flights;      /* a phonon past this many flights goes cooperative
+                                 even in a busy warp (0: never)                    */
   unsigned long long* counts;
   unsigned long long* lost;
   /* flights, lost, capped, samples, max trajectory flights,
@@ -140,6 +144,12 @@ struct RunF32 {
   const float* wsample;       /* mode 2: d kappa / d T_task / np, per task         */
   double* adj;                /* mode 2: [kAdjBatches][nsurf + 1] accumulators     */
   int nsurf;
+  /* mode 3: per replayed sample, positions (3 floats) at trace_off[t] ..
+     trace_off[t+1] (trace NULL: counting pass), position count and exit */
+  float* trace;
+  const long long* trace_off;
+  long long* trace_npos;
+  int* trace_end;
   /* batched launch: geometry table and the geometry of every global task */
   const GeoEntry* geos;
   const int* task_geo;
@@ -149,7 +159,9 @@ struct RunF32 {
    whose spread gives the standard error of the adjoint estimates. */
 constexpr int kAdjBatches = 8;
 /* kernel modes: forward, forward + list of transmitted samples, adjoint replay */
-enum { MODE_FORWARD = 0, MODE_LIST = 1, MODE_ADJOINT = 2 };
+/* forward tallies; + list of transmitted samples; adjoint replay of a list;
+   trace replay of a list (one-lane full flights, positions recorded) */
+enum { MODE_FORWARD = 0, MODE_LIST = 1, MODE_ADJOINT = 2, MODE_TRACE = 3 };
 
 cudaError_t launch_persistent_fp32(const GeoF32& g, const RunF32& r, int grid, int block,
                                    size_t smem, cudaStream_t st, int mode = MODE_FORWARD);

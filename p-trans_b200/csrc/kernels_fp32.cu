@@ -88,6 +88,8 @@ struct Geo {
   __device__ __forceinline__ int cand_begin(int g) const { return ldi(lay.cand_begin, g); }
   __device__ __forceinline__ int cand(int k) const { return ldi(lay.cand, k); }
   __device__ __forceinline__ float4 start(int i) const { return ld(lay.start + i); }
+  __device__ __forceinline__ int bvh_root(int g) const { return ldi(lay.bvh_root, g); }
+  __device__ __forceinline__ float4 node(int i) const { return ld(lay.bvh_node + i); }
 };
 
 /* Square root from the hardware approximation (relative error ~2^-22). */
@@ -125,6 +127,10 @@ struct GeoBatch {
     return __ldg(reinterpret_cast<const int*>(base + lay.cand) + k);
   }
   __device__ __forceinline__ float4 start(int i) const { return ld(lay.start + i); }
+  __device__ __forceinline__ int bvh_root(int g) const {
+    return __ldg(reinterpret_cast<const int*>(base + lay.bvh_root) + g);
+  }
+  __device__ __forceinline__ float4 node(int i) const { return ld(lay.bvh_node + i); }
 };
 
 template <class G_t>
@@ -137,66 +143,156 @@ __device__ __forceinline__ bool inside_edges(const G_t& G, int e0, int ne, float
   return true;
 }
 
-/* Nearest surface among the candidates of a grain (not the box). */
+/* Candidate order does not change the nearest hit: the raw distance t
+   decides and equal distances go to the lower surface index, so a BVH and
+   the linear scan of the same grain find the same surface. */
+__device__ __forceinline__ bool closer(float t, int s, float tr, int sr) {
+  return t < tr || (t == tr && s < sr);
+}
+
+/* One candidate surface against the ray p + t d: updates the nearest raw
+   distance tr and surface sb. */
+template <class G_t>
+__device__ __forceinline__ void test_surface(const G_t& G, int s, float px, float py, float pz,
+                                             float dx, float dy, float dz, int last_geom,
+                                             float eps, float zmax, float& tr, int& sb) {
+  const float4 A = G.hotA(s);
+  const int4 B = G.hotB(s);
+  const int type = B.x & 0xff;
+  if (type == REC_POLY) {
+    const float cosa = fmaf(A.x, dx, fmaf(A.y, dy, A.z * dz));
+    if (cosa <= 0.0f) return;
+    const float t = __fdividef(A.w - fmaf(A.x, px, fmaf(A.y, py, A.z * pz)), cosa);
+    if (!(t >= -eps) || !closer(t, s, tr, sb)) return;
+    const float hx = fmaf(t, dx, px), hy = fmaf(t, dy, py), hz = fmaf(t, dz, pz);
+    if (!inside_edges(G, B.y, B.z, hx, hy, hz, eps)) return;
+    tr = t;
+    sb = s;
+  } else {
+    const bool interior = (B.x & REC_INTERIOR) != 0;
+    if (!interior && B.w == last_geom) return;
+    float wx = A.x - px, wy = A.y - py, wz, a, b, c, r;
+    if (type == REC_SPHERE) {
+      wz = A.z - pz;
+      r = A.w;
+      a = 1.0f;
+      b = fmaf(wx, dx, fmaf(wy, dy, wz * dz));
+      c = fmaf(wx, wx, fmaf(wy, wy, wz * wz)) - r * r;
+    } else {
+      r = A.z;
+      a = fmaf(dx, dx, dy * dy);
+      if (!(a > 0.0f)) return;
+      b = fmaf(wx, dx, wy * dy);
+      c = fmaf(wx, wx, wy * wy) - r * r;
+    }
+    /* roots of a t^2 - 2 b t + c = 0 */
+    const float disc = fmaf(b, b, -a * c);
+    if (!(disc >= 0.0f)) return;
+    const float sq = sqrtf(disc);
+    float t;
+    if (interior) {
+      /* far root (b + sq)/a, written without cancellation */
+      t = (b >= 0.0f) ? __fdividef(b + sq, a) : __fdividef(-c, sq - b);
+    } else {
+      /* near root (b - sq)/a = c / (b + sq), valid when approaching */
+      if (!(b > 0.0f)) return;
+      t = __fdividef(c, b + sq);
+      if (!(t >= -eps)) return;
+    }
+    if (!closer(t, s, tr, sb)) return;
+    if (type == REC_CYL) {
+      const float hz = fmaf(t, dz, pz);
+      if (hz < 0.0f || hz > zmax) return;
+    }
+    tr = t;
+    sb = s;
+  }
+}
+
+/* Entry distance of the ray into a node box (+inf when it misses the box
+   or enters beyond tmax); inverse direction components are finite. */
+__device__ __forceinline__ float box_entry(float4 lo, float4 hi, float px, float py, float pz,
+                                           float ix, float iy, float iz, float tmax, float eps) {
+  const float ax = (lo.x - px) * ix, bx = (hi.x - px) * ix;
+  const float ay = (lo.y - py) * iy, by = (hi.y - py) * iy;
+  const float az = (lo.z - pz) * iz, bz = (hi.z - pz) * iz;
+  const float t0 = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fminf(az, bz));
+  const float t1 = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz));
+  return (t0 <= t1 && t1 >= -eps && t0 <= tmax) ? t0 : 3.0e38f;
+}
+
+__device__ __forceinline__ float inv_dir(float d) {
+  return __fdividef(1.0f, fabsf(d) > 1.0e-20f ? d : copysignf(1.0e-20f, d));
+}
+
+/* Traversal depth bound: the builder limits the depth to 30. */
+constexpr int kBvhStack = 32;
+
+/* Nearest surface of a grain: its BVH when it has one, else every
+   candidate.  tb (the box-grain exit, >= 0) and sb are updated; tb stays
+   >= 0. */
 template <class G_t>
 __device__ __forceinline__ void scan_grain(const G_t& G, int grain, float px, float py, float pz,
                                            float dx, float dy, float dz, int last_geom, float eps,
-                                           float zmax, float& tb, int& sb) {
-  const int kb = G.cand_begin(grain), ke = G.cand_begin(grain + 1);
-  for (int k = kb; k < ke; ++k) {
-    const int s = G.cand(k);
-    const float4 A = G.hotA(s);
-    const int4 B = G.hotB(s);
-    const int type = B.x & 0xff;
-    if (type == REC_POLY) {
-      const float cosa = fmaf(A.x, dx, fmaf(A.y, dy, A.z * dz));
-      if (cosa <= 0.0f) continue;
-      const float t = __fdividef(A.w - fmaf(A.x, px, fmaf(A.y, py, A.z * pz)), cosa);
-      if (!(t >= -eps) || !(t < tb)) continue;
-      const float hx = fmaf(t, dx, px), hy = fmaf(t, dy, py), hz = fmaf(t, dz, pz);
-      if (!inside_edges(G, B.y, B.z, hx, hy, hz, eps)) continue;
-      tb = fmaxf(t, 0.0f);
-      sb = s;
-    } else {
-      const bool interior = (B.x & REC_INTERIOR) != 0;
-      if (!interior && B.w == last_geom) continue;
-      float wx = A.x - px, wy = A.y - py, wz, a, b, c, r;
-      if (type == REC_SPHERE) {
-        wz = A.z - pz;
-        r = A.w;
-        a = 1.0f;
-        b = fmaf(wx, dx, fmaf(wy, dy, wz * dz));
-        c = fmaf(wx, wx, fmaf(wy, wy, wz * wz)) - r * r;
+                                           float zmax, float& tb, int& sb, unsigned& nbox,
+                                           unsigned& nsurf) {
+  float tr = tb;
+  const int root = G.bvh_root(grain);
+  if (root < 0) {
+    const int kb = G.cand_begin(grain), ke = G.cand_begin(grain + 1);
+    nsurf += (unsigned)(ke - kb);
+    for (int k = kb; k < ke; ++k)
+      test_surface(G, G.cand(k), px, py, pz, dx, dy, dz, last_geom, eps, zmax, tr, sb);
+  } else {
+    const float ix = inv_dir(dx), iy = inv_dir(dy), iz = inv_dir(dz);
+    int stk[kBvhStack];
+    float stt[kBvhStack];
+    int sp = 0;
+    int node = root;
+    while (true) {
+      const float4 n1 = G.node(2 * node + 1);
+      const int cnt = __float_as_int(n1.w);
+      const int a = __float_as_int(G.node(2 * node).w);
+      bool descended = false;
+      if (cnt > 0) {
+        nsurf += (unsigned)cnt;
+        for (int k = a; k < a + cnt; ++k)
+          test_surface(G, G.cand(k), px, py, pz, dx, dy, dz, last_geom, eps, zmax, tr, sb);
       } else {
-        r = A.z;
-        a = fmaf(dx, dx, dy * dy);
-        if (!(a > 0.0f)) continue;
-        b = fmaf(wx, dx, wy * dy);
-        c = fmaf(wx, wx, wy * wy) - r * r;
+        nbox += 2u;
+        const float tl = box_entry(G.node(2 * a), G.node(2 * a + 1), px, py, pz, ix, iy, iz, tr, eps);
+        const float tg = box_entry(G.node(2 * a + 2), G.node(2 * a + 3), px, py, pz, ix, iy, iz, tr,
+                                   eps);
+        const bool hl = tl < 3.0e38f, hg = tg < 3.0e38f;
+        if (hl && hg) {
+          const bool lf = tl <= tg;
+          if (sp < kBvhStack) {
+            stk[sp] = lf ? a + 1 : a;
+            stt[sp] = lf ? tg : tl;
+            ++sp;
+          }
+          node = lf ? a : a + 1;
+          descended = true;
+        } else if (hl || hg) {
+          node = hl ? a : a + 1;
+          descended = true;
+        }
       }
-      /* roots of a t^2 - 2 b t + c = 0 */
-      const float disc = fmaf(b, b, -a * c);
-      if (!(disc >= 0.0f)) continue;
-      const float sq = sqrtf(disc);
-      float t;
-      if (interior) {
-        /* far root (b + sq)/a, written without cancellation */
-        t = (b >= 0.0f) ? __fdividef(b + sq, a) : __fdividef(-c, sq - b);
-      } else {
-        /* near root (b - sq)/a = c / (b + sq), valid when approaching */
-        if (!(b > 0.0f)) continue;
-        t = __fdividef(c, b + sq);
-        if (!(t >= -eps)) continue;
+      if (descended) continue;
+      /* next pushed node that can still hold a nearer hit */
+      bool found = false;
+      while (sp > 0) {
+        --sp;
+        if (stt[sp] <= tr) {
+          node = stk[sp];
+          found = true;
+          break;
+        }
       }
-      if (!(t < tb)) continue;
-      if (type == REC_CYL) {
-        const float hz = fmaf(t, dz, pz);
-        if (hz < 0.0f || hz > zmax) continue;
-      }
-      tb = fmaxf(t, 0.0f);
-      sb = s;
+      if (!found) break;
     }
   }
+  tb = fmaxf(tr, 0.0f);
 }
 
 /* Exit of the box grain along d from p: distance tb and face sb (0 x-,
@@ -219,33 +315,100 @@ __device__ __forceinline__ void slab_exit(float px, float py, float pz, float dx
   tb = fmaxf(tb, 0.0f);
 }
 
+/* Lower bound of the distance from p to one candidate surface (planes bound
+   polygons from below, the infinite cylinder bounds the clipped one). */
+template <class G_t>
+__device__ __forceinline__ float surface_lb(const G_t& G, int s, float px, float py, float pz) {
+  const float4 A = G.hotA(s);
+  const int type = G.hotB(s).x & 0xff;
+  if (type == REC_POLY) return fabsf(A.w - fmaf(A.x, px, fmaf(A.y, py, A.z * pz)));
+  if (type == REC_SPHERE) {
+    const float wx = px - A.x, wy = py - A.y, wz = pz - A.z;
+    return fabsf(sqrtf(fmaf(wx, wx, fmaf(wy, wy, wz * wz))) - A.w);
+  }
+  const float wx = px - A.x, wy = py - A.y;
+  return fabsf(sqrtf(fmaf(wx, wx, wy * wy)) - A.z);
+}
+
+/* Distance from p to a node box (0 inside). */
+__device__ __forceinline__ float box_dist(float4 lo, float4 hi, float px, float py, float pz) {
+  const float ex = fmaxf(fmaxf(lo.x - px, px - hi.x), 0.0f);
+  const float ey = fmaxf(fmaxf(lo.y - py, py - hi.y), 0.0f);
+  const float ez = fmaxf(fmaxf(lo.z - pz, pz - hi.z), 0.0f);
+  return sqrtf(fmaf(ex, ex, fmaf(ey, ey, ez * ez)));
+}
+
 /* Lower bound of the distance from p to every box face and to every
-   candidate surface of the grain (planes bound polygons from below, the
-   infinite cylinder bounds the clipped one). */
+   candidate surface of the grain, less 4 eps.  A grain with a BVH is
+   searched only within `cap` (the radius the safe ball needs), pruning
+   nodes farther than the bound found so far; a leaf contributes
+   max(distance to its box, nearest plane / quadric bound of its surfaces). */
 template <class G_t>
 __device__ __forceinline__ float safety(const G_t& G, int grain, float px, float py, float pz,
-                                        float X, float Y, float Z, float eps) {
+                                        float X, float Y, float Z, float eps, float cap) {
   float d = fminf(fminf(fminf(px, X - px), fminf(py, Y - py)), fminf(pz, Z - pz));
   if (grain > 0) {
-    const int kb = G.cand_begin(grain), ke = G.cand_begin(grain + 1);
-    for (int k = kb; k < ke; ++k) {
-      const int s = G.cand(k);
-      const float4 A = G.hotA(s);
-      const int type = G.hotB(s).x & 0xff;
-      float e;
-      if (type == REC_POLY) {
-        e = fabsf(A.w - fmaf(A.x, px, fmaf(A.y, py, A.z * pz)));
-      } else if (type == REC_SPHERE) {
-        const float wx = px - A.x, wy = py - A.y, wz = pz - A.z;
-        e = fabsf(sqrtf(fmaf(wx, wx, fmaf(wy, wy, wz * wz))) - A.w);
-      } else {
-        const float wx = px - A.x, wy = py - A.y;
-        e = fabsf(sqrtf(fmaf(wx, wx, wy * wy)) - A.z);
+    const int root = G.bvh_root(grain);
+    if (root < 0) {
+      const int kb = G.cand_begin(grain), ke = G.cand_begin(grain + 1);
+      for (int k = kb; k < ke; ++k) d = fminf(d, surface_lb(G, G.cand(k), px, py, pz));
+    } else {
+      d = fminf(d, cap);
+      int stk[kBvhStack];
+      float std_[kBvhStack];
+      int sp = 0;
+      int node = root;
+      while (true) {
+        const float4 n0 = G.node(2 * node), n1 = G.node(2 * node + 1);
+        const int cnt = __float_as_int(n1.w);
+        const int a = __float_as_int(n0.w);
+        bool descended = false;
+        if (cnt > 0) {
+          float e = 3.0e38f;
+          for (int k = a; k < a + cnt; ++k) e = fminf(e, surface_lb(G, G.cand(k), px, py, pz));
+          d = fminf(d, fmaxf(box_dist(n0, n1, px, py, pz), e));
+        } else {
+          const float dl = box_dist(G.node(2 * a), G.node(2 * a + 1), px, py, pz);
+          const float dg = box_dist(G.node(2 * a + 2), G.node(2 * a + 3), px, py, pz);
+          const bool lf = dl <= dg;
+          const float dn = lf ? dl : dg, df = lf ? dg : dl;
+          if (dn < d) {
+            if (df < d && sp < kBvhStack) {
+              stk[sp] = lf ? a + 1 : a;
+              std_[sp] = df;
+              ++sp;
+            }
+            node = lf ? a : a + 1;
+            descended = true;
+          }
+        }
+        if (descended) continue;
+        bool found = false;
+        while (sp > 0) {
+          --sp;
+          if (std_[sp] < d) {
+            node = stk[sp];
+            found = true;
+            break;
+          }
+        }
+        if (!found) break;
       }
-      d = fminf(d, e);
     }
   }
   return d - 4.0f * eps;
+}
+
+/* Trace replay: position after flight f of the sample in replay-list slot t
+   (f = 0: the emission point), when the host gave a position buffer. */
+__device__ __forceinline__ void trace_put(const RunF32& r, long long t, unsigned f, float px,
+                                          float py, float pz) {
+  if (!r.trace) return;
+  const long long at = r.trace_off[t] + f;
+  if (at >= r.trace_off[t + 1]) return;
+  r.trace[3 * at] = px;
+  r.trace[3 * at + 1] = py;
+  r.trace[3 * at + 2] = pz;
 }
 
 __device__ __forceinline__ unsigned lanemask_lt() {
@@ -312,6 +475,12 @@ constexpr int kAdjSmemDoubles = 2048;
 /* rounds of 32 flights one cooperative visit may take before the phonon's
    lane returns to the refill / tally step */
 constexpr int kCoopRounds = 8;
+/* rounds per visit of a long phonon in a warp whose other lanes are busy */
+constexpr int kCoopRoundsBusy = 4;
+
+/* safe-ball radius searched in a grain with a BVH, in units of the MFP: a
+   walk needs about (radius / MFP)^2 flights to leave the ball */
+constexpr float kBallCapMfp = 32.0f;
 
 template <bool SMEM, int MODE, bool BATCH>
 __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
@@ -342,6 +511,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   float adj_w = 0.0f, adj_len = 0.0f;   /* weight of the sample, path length */
   unsigned adj_npp = 0;                 /* intrinsic events of the sample   */
   int adj_b = 0;                        /* batch of the sample               */
+  long long tslot = 0;                  /* trace replay: index of the sample */
   unsigned long long my_mismatch = 0;
 
   /* warp-uniform chunk cursor */
@@ -358,6 +528,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   unsigned long long my_flights = 0, my_samples = 0, my_capped = 0, my_lost = 0, my_max = 0;
   unsigned my_full = 0, my_balls = 0;
   unsigned long long my_coop_rounds = 0, my_coop_flights = 0;
+  unsigned my_box_tests = 0, my_surf_tests = 0;  /* BVH node boxes, surfaces tested */
 
   while (true) {
     /* ---- refill idle lanes from the warp's chunk ---------------------- */
@@ -369,7 +540,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           int c = 0;
           if (lane == 0) c = atomicAdd(r.queue, 1);
           c = __shfl_sync(FULL, c, 0);
-          if (MODE == MODE_ADJOINT) {
+          if (MODE == MODE_ADJOINT || MODE == MODE_TRACE) {
             /* the replay list in chunks of 32 sample ids */
             if ((long long)c * 32 >= r.alist_n) {
               queue_done = true;
@@ -399,6 +570,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             adj_b = (int)(sample % kAdjBatches);
             adj_len = 0.0f;
             adj_npp = 0;
+          } else if (MODE == MODE_TRACE) {
+            tslot = ch_next + rank;
+            sample = r.alist[tslot];
+            task = (int)(sample / (uint64_t)r.np);
           } else if (BATCH) {
             const int64_t p = (int64_t)r.rank + (int64_t)(ch_next + rank) * r.nranks;
             task = ch_task;
@@ -468,6 +643,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           flight = 0;
           alive = true;
           my_samples += 1;
+          if (MODE == MODE_TRACE) trace_put(r, tslot, 0u, px, py, pz);
         }
         ch_next += take;
         ch_left -= take;
@@ -498,9 +674,15 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
     uint4 preR = make_uint4(0u, 0u, 0u, 0u);
     float pre_tb = 0.0f;
     int pre_sb = -1;
-    if (!BATCH && r.coop_lanes > 0) {
-      const unsigned todo0 = __ballot_sync(FULL, alive && lam < flmax);
-      if (todo0 && __popc(__ballot_sync(FULL, alive)) <= r.coop_lanes) {
+    if (!BATCH && MODE != MODE_TRACE && r.coop_lanes > 0) {
+      const unsigned elig = __ballot_sync(FULL, alive && lam < flmax);
+      const bool sparse = __popc(__ballot_sync(FULL, alive)) <= r.coop_lanes;
+      /* in a busy warp only phonons past long_flights flights go cooperative,
+         for fewer rounds, so the warp's other lanes keep moving */
+      const unsigned todo0 =
+          sparse ? elig : (elig & __ballot_sync(FULL, r.long_flights > 0 && flight >= r.long_flights));
+      const int max_rounds = sparse ? kCoopRounds : kCoopRoundsBusy;
+      if (todo0) {
         unsigned todo = todo0;
         while (todo) {
           const int L = __ffs(todo) - 1;
@@ -520,7 +702,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           uint4 sR = make_uint4(0u, 0u, 0u, 0u);
           float stb = 0.0f;
           int ssb = -1;
-          for (int round = 0; round < kCoopRounds; ++round) {
+          for (int round = 0; round < max_rounds; ++round) {
             ++crounds;
             const uint4 R = philox10(cfl + 1u + (uint32_t)lane, c1, cslo, cshi, key);
             /* direction and free path after a p-p event ending flight `lane` */
@@ -555,7 +737,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             slab_exit(qx, qy, qz, sdx, sdy, sdz, X, Y, Z, tb, sb);
             if (cgrain > 0)
               scan_grain(G, cgrain, qx, qy, qz, sdx, sdy, sdz, lane == 0 ? clast : -1, eps, Z,
-                         tb, sb);
+                         tb, sb, my_box_tests, my_surf_tests);
             const bool brk = !inbox || capd;
             const unsigned sm = __ballot_sync(FULL, brk || !(sfp < tb));
             const int j = sm ? __ffs(sm) - 1 : 32;
@@ -623,7 +805,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
          paths do not depend on the phonon state and are computed together;
          only the position / ball test chain is serial. ---- */
       int k = 0;
-      bool fast_more = br2 > 0.0f && !coop;
+      bool fast_more = MODE != MODE_TRACE && br2 > 0.0f && !coop;
       while (fast_more && k < r.fast_steps && flight + 4u <= r.max_flights) {
         uint4 B[4];
 #pragma unroll
@@ -684,7 +866,9 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           ++my_full;
           R = philox10(flight, c1, slo, shi, key);
           slab_exit(px, py, pz, dx, dy, dz, X, Y, Z, tb, sb);
-          if (grain > 0) scan_grain(G, grain, px, py, pz, dx, dy, dz, last_geom, eps, Z, tb, sb);
+          if (grain > 0)
+            scan_grain(G, grain, px, py, pz, dx, dy, dz, last_geom, eps, Z, tb, sb, my_box_tests,
+                       my_surf_tests);
           go = true;
         }
         if (go) {
@@ -708,8 +892,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             fp = -lam * __logf(u2);
             last_geom = -1;
             br2 = 0.0f;
-            if (r.fast_steps > 0 && lam < flmax) {
-              const float d = safety(G, grain, px, py, pz, X, Y, Z, eps);
+            if (MODE != MODE_TRACE && r.fast_steps > 0 && lam < flmax) {
+              const float d = safety(G, grain, px, py, pz, X, Y, Z, eps, kBallCapMfp * lam);
               ++my_balls;
               if (d > 0.0f) { bx = px; by = py; bz = pz; br2 = d * d; }
             }
@@ -823,6 +1007,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
               fp = -lam * __logf(u23f(R2.y));
             }
           }
+          if (MODE == MODE_TRACE) trace_put(r, tslot, flight, px, py, pz);
         }
       }
     }
@@ -845,6 +1030,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
         const unsigned long long at = base + __popc(m & lanemask_lt());
         if (put && at < r.tlist_cap) r.tlist[at] = ((unsigned long long)shi << 32) | slo;
       }
+    }
+    if (MODE == MODE_TRACE && fin) {
+      r.trace_npos[tslot] = (long long)flight + 1;
+      r.trace_end[tslot] = end_side;
     }
     if (MODE == MODE_ADJOINT && fin) {
       if (end_side == 2) {
@@ -869,11 +1058,14 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   /* warp totals */
   unsigned long long v0 = my_flights, v1 = my_lost, v2 = my_capped, v3 = my_samples, v4 = my_max;
   unsigned long long v5 = my_full, v6 = my_balls, v7 = my_coop_rounds, v8 = my_coop_flights;
+  unsigned long long v9 = my_box_tests, v10 = my_surf_tests;
   for (int o = 16; o > 0; o >>= 1) {
     v5 += __shfl_xor_sync(FULL, v5, o);
     v6 += __shfl_xor_sync(FULL, v6, o);
     v7 += __shfl_xor_sync(FULL, v7, o);
     v8 += __shfl_xor_sync(FULL, v8, o);
+    v9 += __shfl_xor_sync(FULL, v9, o);
+    v10 += __shfl_xor_sync(FULL, v10, o);
     v0 += __shfl_xor_sync(FULL, v0, o);
     v1 += __shfl_xor_sync(FULL, v1, o);
     v2 += __shfl_xor_sync(FULL, v2, o);
@@ -895,6 +1087,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
     if (v6) atomicAdd(r.stats + 9, v6);
     if (v7) atomicAdd(r.stats + 12, v7);
     if (v8) atomicAdd(r.stats + 13, v8);
+    if (v9) atomicAdd(r.stats + 14, v9);
+    if (v10) atomicAdd(r.stats + 15, v10);
   }
   if (MODE == MODE_ADJOINT && adj_in_smem) {
     __syncthreads();
@@ -946,14 +1140,16 @@ cudaError_t launch_persistent_batch(const RunF32& r, int grid, int block, cudaSt
 cudaError_t persistent_occupancy(int block, size_t smem, int* bps, int mode) {
   if (mode == MODE_LIST) return occupancy_mode<MODE_LIST>(block, smem, bps);
   if (mode == MODE_ADJOINT) return occupancy_mode<MODE_ADJOINT>(block, smem, bps);
+  if (mode == MODE_TRACE) return occupancy_mode<MODE_TRACE>(block, smem, bps);
   return occupancy_mode<MODE_FORWARD>(block, smem, bps);
 }
 
 cudaError_t launch_persistent_fp32(const GeoF32& g, const RunF32& r, int grid, int block,
                                    size_t smem, cudaStream_t st, int mode) {
-  if (block != kBlock) return cudaErrorInvalidConfiguration;
+  if (block > kBlock || block % 32) return cudaErrorInvalidConfiguration;
   if (mode == MODE_LIST) return launch_mode<MODE_LIST>(g, r, grid, block, smem, st);
   if (mode == MODE_ADJOINT) return launch_mode<MODE_ADJOINT>(g, r, grid, block, smem, st);
+  if (mode == MODE_TRACE) return launch_mode<MODE_TRACE>(g, r, grid, block, smem, st);
   return launch_mode<MODE_FORWARD>(g, r, grid, block, smem, st);
 }
 

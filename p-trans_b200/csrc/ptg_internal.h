@@ -85,9 +85,21 @@ struct NoallocView {
 };
 int handle_noalloc_view(ptg_handle* h, NoallocView* v);
 
-/* FP32 geometry blob (host copy) of a built geometry. */
-int blob_from_geometry(const GeomSoA& G, std::vector<float4>* out, BlobLayout* lay,
+/* FP32 geometry blob (host copy) of a built geometry; grains with more than
+   kBvhMinCand candidates get a BVH with leaves of bvh_leaf surfaces
+   (bvh_leaf < 0: none, linear candidate scans everywhere). */
+constexpr int kBvhMinCand = 32;
+constexpr int kBvhDefaultLeaf = 4;
+int blob_from_geometry(const GeomSoA& G, int bvh_leaf, std::vector<float4>* out, BlobLayout* lay,
                        std::string* why);
+/* Binned-SAH BVH over boxes lo/hi (3 floats each): nodes (2 float4 each,
+   children and leaf ranges absolute: node_base, cand_base added) and the
+   primitive order of the leaves.  Returns the node count. */
+int bvh_build(const std::vector<float>& lo, const std::vector<float>& hi, int leaf, int max_depth,
+              int cand_base, int node_base, std::vector<float4>* nodes, std::vector<int>* order);
+/* True when some grain of the handle's geometry has more than kBvhMinCand
+   candidate surfaces (a BVH unless bvh_leaf < 0). */
+bool handle_has_bvh(const ptg_handle* h);
 /* Host FP64 kappa assembly (see api.cpp). */
 int assemble_host(const SpecSoA& S, const ptg_run* run, double box_x, const uint64_t* counts,
                   ptg_kappa_out* out, std::vector<double>* wtask, double* dk_ds_an);

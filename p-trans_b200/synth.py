@@ -268,3 +268,135 @@ def film_batch(n: int = 256, seed: int = 0, n_modes: int = 2000, nangle: int = 1
         nps.append(max(1, int(round(samples / (n_modes * (nangle - 1))))))
         models.append(m)
     return models, nps
+
+
+def _clip_cell(faces, labels, nrm, c, label, tol):
+    """Clips a convex polyhedron (outward vertex loops `faces` with `labels`)
+    to the half-space nrm . x <= c; the cut face gets `label`."""
+    out_f, out_l, cut = [], [], []
+    for f, lab in zip(faces, labels):
+        d = [float(np.dot(nrm, v)) - c for v in f]
+        if max(d) <= tol:
+            out_f.append(f)
+            out_l.append(lab)
+            continue
+        if min(d) >= -tol:
+            for v, dv in zip(f, d):
+                if abs(dv) <= tol:
+                    cut.append(v)
+            continue
+        loop = []
+        n = len(f)
+        for i in range(n):
+            a, b = f[i], f[(i + 1) % n]
+            da, db = d[i], d[(i + 1) % n]
+            if da <= tol:
+                loop.append(a)
+                if abs(da) <= tol:
+                    cut.append(a)
+            if (da < -tol and db > tol) or (da > tol and db < -tol):
+                p = a + (b - a) * (da / (da - db))
+                loop.append(p)
+                cut.append(p)
+        if len(loop) >= 3:
+            out_f.append(loop)
+            out_l.append(lab)
+    # cap polygon: the cut points, counter-clockwise seen along +nrm
+    pts = []
+    for p in cut:
+        if not any(np.linalg.norm(p - q) <= 10 * tol for q in pts):
+            pts.append(p)
+    if len(pts) >= 3:
+        ctr = np.mean(pts, axis=0)
+        u = pts[0] - ctr
+        u = u / np.linalg.norm(u)
+        w = np.cross(nrm, u)
+        ang = [math.atan2(float(np.dot(p - ctr, w)), float(np.dot(p - ctr, u))) for p in pts]
+        out_f.append([pts[i] for i in np.argsort(ang)])
+        out_l.append(label)
+    return out_f, out_l
+
+
+def voronoi_box(n_grains: int = 5, box=(1000.0, 1000.0, 1000.0), seed: int = 0, trans: float = 0.5,
+                spec: float = 0.0, p_wall: float = 0.0, generators=None) -> Model:
+    """Voronoi polycrystal in the box: seeded generators (uniform in the inner
+    90% of the box), every cell the box clipped by the bisector planes of the
+    other generators.  Facets on the box are Boundary facets (grain_to 0, the
+    box's CellSpecularity applies), facets between cells carry material 1 and
+    the neighbour's grain id, with the (1,1) transmission-table entry
+    (T = trans, p = spec) as in Examples/04_voronoi_5grain.mcp."""
+    L = np.asarray(box, np.float64)
+    rng = np.random.default_rng(seed)
+    gens = (np.asarray(generators, np.float64) if generators is not None
+            else L * (0.05 + 0.9 * rng.random((n_grains, 3))))
+    n = len(gens)
+    tol = 1e-9 * float(L.max())
+    faces0 = [[np.array(v, np.float64) for v in f] for f in _box_faces(0, L[0], 0, L[1], 0, L[2])]
+    nfacet, nv, verts, mto, gto = [], [], [], [], []
+    for i in range(n):
+        faces, labels = list(faces0), [-1] * 6
+        for j in range(n):
+            if j == i:
+                continue
+            nrm = gens[j] - gens[i]
+            nrm = nrm / np.linalg.norm(nrm)
+            c = float(np.dot(nrm, 0.5 * (gens[i] + gens[j])))
+            faces, labels = _clip_cell(faces, labels, nrm, c, j, tol)
+        kept = 0
+        for f, lab in zip(faces, labels):
+            fv = []
+            for v in f:
+                v = v.copy()
+                for d in range(3):  # exact box coordinates on box facets
+                    if abs(v[d]) <= tol:
+                        v[d] = 0.0
+                    elif abs(v[d] - L[d]) <= tol:
+                        v[d] = L[d]
+                fv.append(v)
+            nv.append(len(fv))
+            verts.extend(fv)
+            mto.append(MATERIAL_BOUNDARY if lab < 0 else 1)
+            gto.append(0 if lab < 0 else lab + 1)
+            kept += 1
+        nfacet.append(kept)
+    kind, tt, ts = _table(trans, spec)
+    return Model(
+        box=tuple(float(x) for x in L), kind_grain=GRAIN_VORONOI, grain_shape=[SHAPE_POLYGON] * n,
+        grain_generatrix=gens.ravel(), grain_diameter=[0.0] * n, grain_material=[1] * n,
+        grain_nfacet=nfacet, facet_nvertex=nv, facet_vertex=np.array(verts, np.float64).ravel(),
+        surf_material_to=mto, surf_grain_to=gto,
+        cellspec=(1.0, 1.0, p_wall, p_wall, p_wall, p_wall), tt_kind=kind, tt_trans=tt, tt_spec=ts)
+
+
+def cube_lattice(n: int = 16, l: float = 1000.0, fill: float = 0.5, trans: float = 0.0,
+                 spec: float = 0.0, p_wall: float = 0.0, triangles: bool = True) -> Model:
+    """Simple-cubic lattice of n^3 cubic inclusions (bricks) in an l^3 box:
+    pitch l/n, cube side fill * pitch, every cube face as two triangles
+    (12 per cube: n = 16 gives 49152 triangles) or as one quad.  The matrix
+    (fill grain) sees every inclusion facet, the case a BVH is for."""
+    pitch = l / n
+    a = 0.5 * fill * pitch
+    faces_all, nf, gens = [], [], []
+    for ix in range(n):
+        for iy in range(n):
+            for iz in range(n):
+                cx, cy, cz = (ix + 0.5) * pitch, (iy + 0.5) * pitch, (iz + 0.5) * pitch
+                faces = _box_faces(cx - a, cx + a, cy - a, cy + a, cz - a, cz + a)
+                if triangles:
+                    tri = []
+                    for f in faces:
+                        tri.append([f[0], f[1], f[2]])
+                        tri.append([f[0], f[2], f[3]])
+                    faces = tri
+                faces_all.extend(faces)
+                nf.append(len(faces))
+                gens.append((cx, cy, cz))
+    ng = len(nf)
+    kind, tt, ts = _table(trans, spec)
+    return Model(
+        box=(l, l, l), kind_grain=GRAIN_BRICKS, grain_shape=[SHAPE_POLYGON] * ng,
+        grain_generatrix=np.array(gens).ravel(), grain_diameter=[0.0] * ng, grain_material=[1] * ng,
+        grain_nfacet=nf, facet_nvertex=[len(f) for f in faces_all],
+        facet_vertex=np.array([v for f in faces_all for v in f], np.float64).ravel(),
+        surf_material_to=[MATERIAL_INTERNAL] * len(faces_all), surf_grain_to=[0] * len(faces_all),
+        cellspec=(1.0, 1.0, p_wall, p_wall, p_wall, p_wall), tt_kind=kind, tt_trans=tt, tt_spec=ts)

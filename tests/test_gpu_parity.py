@@ -28,6 +28,9 @@ def geometries():
                                         t=0.5, p=0.3, p_wall=0.2),
         "brick_quads": synth.brick_box(t=0.5, p=0.3, p_wall=0.1),
         "brick_tris": synth.brick_box(t=0.7, p=0.0, p_wall=0.5, triangles=True),
+        "lattice_tris": synth.cube_lattice(n=3, l=300.0, fill=0.5, trans=0.3, spec=0.2, p_wall=0.3),
+        "voronoi": synth.voronoi_box(6, box=(300.0, 200.0, 200.0), seed=4, trans=0.5, spec=0.1,
+                                     p_wall=0.2),
     }
 
 
@@ -182,8 +185,9 @@ def test_rank_partition_is_exact_fp32():
                                   "nanowire_mixed"])
 @pytest.mark.parametrize("cap", [0, 40])
 def test_cooperative_tail_takes_the_same_trajectories(name, cap):
-    """Warp-cooperative rounds (every warp, coop_lanes = 32) and the one-lane
-    path (tune_flags bit 1) give identical per-task counts, lost counts and
+    """Warp-cooperative rounds (every warp with coop_lanes = 32; only phonons
+    past 16 flights with long_flights = 16) and the one-lane path
+    (tune_flags bit 1) give identical per-task counts, lost counts and
     flight totals: a flight advances the position with the same rounding on
     every path, so the trajectory depends only on its Philox counter."""
     m = geometries()[name]
@@ -192,18 +196,85 @@ def test_cooperative_tail_takes_the_same_trajectories(name, cap):
     run = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=5, np_=257, seed=21, precision=A.PREC_FP32)
     out = {}
     for key, opts in (("lane", dict(tune_flags=2)), ("coop", dict(coop_lanes=32)),
-                      ("tail", dict()), ("coop_nofast", dict(coop_lanes=32, tune_flags=1))):
+                      ("tail", dict()), ("coop_nofast", dict(coop_lanes=32, tune_flags=1)),
+                      ("long", dict(coop_lanes=1, long_flights=16))):
         with A.Handle(gb.view, spec, max_flights=cap, **opts) as h:
             k = h.kappa(run, want_counts=True)
             out[key] = (k["counts"], k["lost"], h.stats())
     base_counts, base_lost, base_st = out["lane"]
     assert base_st["coop_rounds"] == 0
-    for key in ("coop", "tail", "coop_nofast"):
+    for key in ("coop", "tail", "coop_nofast", "long"):
         counts, lost, st = out[key]
         np.testing.assert_array_equal(counts, base_counts, err_msg=key)
         assert lost == base_lost, key
         assert st["flights"] == base_st["flights"], key
         assert st["max_traj_flights"] == base_st["max_traj_flights"], key
     assert out["coop"][2]["coop_rounds"] > 0 and out["coop"][2]["coop_flights"] > 0
+    assert out["long"][2]["coop_rounds"] > 0
     if cap:
         assert base_lost > 0
+
+
+
+def _many_spheres(n=40, l=400.0, seed=0):
+    rng = np.random.default_rng(seed)
+    c, r = [], []
+    while len(c) < n:
+        rr = rng.uniform(8.0, 20.0)
+        p = rng.uniform(rr + 5.0, l - rr - 5.0, 3)
+        if all(np.linalg.norm(p - q) > rr + s + 2.0 for q, s in zip(c, r)):
+            c.append(p)
+            r.append(rr)
+    return synth.spheres_in_box(l=l, centres=[tuple(x) for x in c], radii=r, t=0.4, p=0.3, p_wall=0.2)
+
+
+@pytest.mark.parametrize("name", ["lattice", "spheres", "holes"])
+def test_bvh_and_linear_scan_take_the_same_trajectories(name):
+    """A grain with more than 32 candidates gets a BVH; its nearest hit is the
+    linear scan's (nearest raw distance, ties to the lower surface index) and
+    the BVH-pruned safe ball does not change the trajectory, so counts,
+    lost counts and flight totals are identical for every leaf size and with
+    no BVH at all (bvh_leaf = -1)."""
+    m = {"lattice": lambda: synth.cube_lattice(n=4, l=400.0, fill=0.5, trans=0.3, spec=0.2, p_wall=0.3),
+         "spheres": _many_spheres,
+         "holes": lambda: synth.film_with_holes(lx=600.0, ly=600.0, lz=100.0, nholes=40, radius=20.0,
+                                                seed=5, p_hole=0.3, t_hole=0.2)}[name]()
+    spec = synth.spectrum(10, seed=7, mfp_lo=2e-9, mfp_hi=1e-6)
+    gb = A.GeomBuf(m)
+    run = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=5, np_=203, seed=3, precision=A.PREC_FP32)
+    ref = None
+    for leaf in (-1, 1, 4, 8):
+        with A.Handle(gb.view, spec, bvh_leaf=leaf) as h:
+            k = h.kappa(run, want_counts=True)
+            st = h.stats()
+        cur = (k["counts"], k["lost"], st["flights"], st["max_traj_flights"])
+        if ref is None:
+            ref = cur
+            continue
+        np.testing.assert_array_equal(cur[0], ref[0], err_msg=f"leaf {leaf}")
+        assert cur[1:] == ref[1:], leaf
+
+
+def test_autotune_keeps_results_and_caches(tmp_path):
+    """ptg_autotune leaves valid options on the handle, every option it tries
+    gives the same counts (trajectories depend only on Philox counters), and
+    the Python cache reapplies the stored options without timing."""
+    m = synth.cube_lattice(n=4, l=400.0, fill=0.5, trans=0.3, spec=0.2, p_wall=0.3)
+    spec = synth.spectrum(10, seed=9, mfp_lo=2e-9, mfp_hi=1e-6)
+    gb = A.GeomBuf(m)
+    run = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=5, np_=101, seed=4, precision=A.PREC_FP32)
+    cache = str(tmp_path / "tune.json")
+    with A.Handle(gb.view, spec) as h:
+        base = h.kappa(run, want_counts=True)["counts"]
+        res = h.autotune(run, reps=1, cache=cache, key="lattice4")
+        o = h.options()
+        assert not res["cached"] and res["kernel_ms"] > 0
+        assert o["block_size"] in (0, 128, 256) and o["bvh_leaf"] in (0, 1, 2, 4, 8, 16)
+        np.testing.assert_array_equal(h.kappa(run, want_counts=True)["counts"], base)
+        with pytest.raises(A.PtgError) as e:
+            h.set_options(block_size=100)
+        assert e.value.status == A.PTG_ERR_INVALID
+    with A.Handle(gb.view, spec) as h:
+        again = h.autotune(run, cache=cache, key="lattice4")
+        assert again["cached"] and h.options() == o
+        np.testing.assert_array_equal(h.kappa(run, want_counts=True)["counts"], base)

@@ -48,6 +48,8 @@ def models():
         "brick_quads": synth.brick_box(t=0.5, p=0.25),
         "brick_tris": synth.brick_box(t=0.5, p=0.25, triangles=True),
         "fluct": _with(synth.brick_box(t=0.5, p=0.5), specfluc=0.2, fluct_seed=77),
+        "voronoi": synth.voronoi_box(7, box=(300.0, 200.0, 250.0), seed=2, trans=0.5, spec=0.2),
+        "lattice": synth.cube_lattice(n=3, l=300.0, fill=0.4, trans=0.2, spec=0.1),
     }
 
 
@@ -158,3 +160,168 @@ def test_reference_examples_parse():
         g = A.GeomBuf(m).numpy()
         assert g["nsurf"] == w["built_nsurf"], name
         assert int(g["internal"].sum()) == w["built_internal"], name
+
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_voronoi_cells_tile_the_box(seed):
+    """The generated Voronoi cells are closed, outward-oriented polyhedra that
+    tile the box (volumes by the divergence theorem sum to the box volume),
+    every internal facet i->j has its twin j->i of equal area, and box facets
+    lie exactly on a box plane (so the builder marks them non-internal)."""
+    box = (400.0, 300.0, 200.0)
+    m = synth.voronoi_box(9, box=box, seed=seed)
+    v = m.facet_vertex.reshape(-1, 3)
+    k = f = 0
+    vols, area = [], {}
+    for g, nf in enumerate(m.grain_nfacet):
+        vol = 0.0
+        for _ in range(nf):
+            nv = m.facet_nvertex[f]
+            P = v[k:k + nv]
+            k += nv
+            a = 0.5 * sum(np.cross(P[i], P[(i + 1) % nv]) for i in range(nv))
+            vol += float(np.dot(P[0], a)) / 3.0
+            to = int(m.surf_grain_to[f])
+            if to == 0:
+                assert any(np.all(P[:, d] == 0.0) or np.all(P[:, d] == box[d]) for d in range(3))
+            else:
+                area[(g + 1, to)] = float(np.linalg.norm(a))
+            f += 1
+        assert vol > 0.0
+        vols.append(vol)
+    assert abs(sum(vols) - np.prod(box)) < 1e-9 * np.prod(box)
+    for (a, b), x in area.items():
+        assert abs(area[(b, a)] - x) < 1e-9 * max(x, 1.0)
+
+
+def test_struct_layouts_agree_with_the_header(tmp_path):
+    """Every ctypes mirror in abi.py has the C struct's size and field
+    offsets (a C program compiled against include/ptrans_gpu.h prints them),
+    and the Fortran ptg_options type lists the header's fields in order."""
+    import ctypes
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    pairs = {"ptg_model": A.PtgModel, "ptg_spectrum": A.PtgSpectrum, "ptg_geometry": A.PtgGeometry,
+             "ptg_options": A.PtgOptions, "ptg_run": A.PtgRun, "ptg_kappa_out": A.PtgKappaOut,
+             "ptg_stats": A.PtgStats, "ptg_adjoint_out": A.PtgAdjointOut,
+             "ptg_batch_item": A.PtgBatchItem, "ptg_batch_out": A.PtgBatchOut}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
+    expect = []
+    for cname, cls in pairs.items():
+        lines.append(f'  printf("%zu\\n", sizeof({cname}));')
+        expect.append(ctypes.sizeof(cls))
+        for fname, _ in cls._fields_:
+            lines.append(f'  printf("%zu\\n", offsetof({cname}, {fname}));')
+            expect.append(getattr(cls, fname).offset)
+    lines.append("  return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c99", "-o", str(exe), str(src)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True,
+                                          text=True).stdout.split()]
+    assert got == expect
+    txt = open(HEADER).read()
+    body = txt[txt.index("typedef struct ptg_options {"):txt.index("} ptg_options;")]
+    c_fields = re.findall(r"\b(?:int32_t|int64_t|double)\s+(\w+)\s*;", body)
+    f90 = open(os.path.join(ROOT, "p-trans_b200", "fortran", "ptrans_gpu.f90")).read()
+    ftype = f90[f90.index("type, bind(C), public :: ptg_options"):f90.index("end type ptg_options")]
+    f_fields = []
+    for line in ftype.splitlines()[1:]:
+        if "::" in line:
+            f_fields += [x.split("=")[0].strip() for x in line.split("::")[1].split(",")]
+    assert f_fields == c_fields
+    assert [n for n, _ in A.PtgOptions._fields_] == c_fields
+
+
+@pytest.mark.parametrize("kind,v,w,d,text", [
+    ("E", 1.0, 15, 6, "   0.100000E+01"),
+    ("E", -1234.5, 15, 6, "  -0.123450E+04"),
+    ("E", 0.0, 15, 6, "   0.000000E+00"),
+    ("E", 9.9999996, 15, 6, "   0.100000E+02"),
+    ("E", 3.0e-9, 15, 6, "   0.300000E-08"),
+    ("E", 1.0e-120, 20, 10, "    0.1000000000-119"),
+    ("E", 6.2831853e13, 20, 10, "    0.6283185300E+14"),
+    ("F", 10.302305849, 20, 10, "       10.3023058490"),
+    ("F", 0.5, 20, 10, "        0.5000000000"),
+    ("F", 300.0, 0, 6, "300.000000"),
+    ("I", 500, 6, 0, "   500"),
+    ("I", 20000, 3, 0, "***"),
+    ("I", 7, 5, 0, "    7"),
+])
+def test_fortran_edit_descriptors(kind, v, w, d, text):
+    """The writer renders I, F and E descriptors as gfortran does: E with a
+    0.d mantissa and a 2-digit exponent (3 digits without the E), F with its
+    leading zero, asterisks when the field is too narrow."""
+    assert A.fortran_format(kind, v, w, d) == text
+
+
+def _two_branch_spectrum(nk=40, seed=3, ties=True):
+    rng = np.random.default_rng(seed)
+    nb = 2
+    f = rng.uniform(0.5, 15.0, nb * nk)
+    if ties:
+        f[5] = f[7]          # equal frequencies in one branch (m = ib + nb*ik: both branch 1)
+        f[2] = f[3]          # and across branches
+    v = np.exp(rng.normal(np.log(4000.0), 0.5, nb * nk))
+    mfp = np.exp(rng.uniform(np.log(2e-9), np.log(2e-6), nb * nk))
+    return A.Spectrum(omega=f * synth.THZ, tau=mfp / v * 1e12, vel=v, weight=np.ones(nb * nk), nbranch=nb,
+                      rtemp=300.0, vol=4e-29, mfp=mfp)
+
+
+@pytest.mark.parametrize("kind", ["per_mode", "matthiessen", "grid"])
+def test_writers_match_the_oracle_restatement(orc, tmp_path, kind):
+    """ptg_write_outputs writes the same bytes as the oracle's restatement of
+    fileoutput for the same counts: sorted records with tied effective MFPs
+    (zero counts) and tied frequencies, two branches, every MFP rule."""
+    m = synth.film_with_holes(lx=200.0, ly=200.0, lz=100.0, nholes=2, radius=30.0, seed=1)
+    spec = _two_branch_spectrum()
+    kw = {"per_mode": dict(kind_mfp=A.MFP_PER_MODE),
+          "matthiessen": dict(kind_mfp=A.MFP_MATTHIESSEN),
+          "grid": dict(kind_mfp=A.MFP_GRID, mfp_grid=[5.0, 50.0, 500.0])}[kind]
+    run = A.make_run(nangle=7, np_=6, seed=11, precision=A.PREC_FP64, temperature=300.0, **kw)
+    o = orc.Oracle(model=m, spectrum=spec)
+    counts, _, _ = o.counts(run)
+    gb = A.GeomBuf(m)
+    (tmp_path / "a").mkdir()
+    (tmp_path / "b").mkdir()
+    A.write_outputs(str(tmp_path / "a" / "structure.mcp"), gb.view, spec, run, counts)
+    o.write_outputs(str(tmp_path / "b" / "structure.mcp"), run, counts)
+    for name in ("thermalproperty.out", "effectiveMFP.out", "phononconductivity.out"):
+        a = (tmp_path / "a" / name).read_bytes()
+        b = (tmp_path / "b" / name).read_bytes()
+        assert a == b, name
+    em = (tmp_path / "a" / "effectiveMFP.out").read_text().splitlines()
+    assert len(em) == 6 + spec.nmode
+    effs = [float(line[25:40]) for line in em[6:]]
+    assert effs == sorted(effs)
+    if kind == "per_mode":
+        assert effs.count(0.0) >= 2   # zero counts: tied keys, the exchange-sort path
+    pc = (tmp_path / "a" / "phononconductivity.out").read_text().splitlines()
+    assert pc[1] == "# Nb = " + A.fortran_format("I", len(set(spec.omega)) - 1, 6)
+
+
+@pytest.mark.parametrize("tbc_mw", [50.0, 300.0, 2000.0])
+def test_gamma_from_tbc_matches_oracle_and_target(orc, tbc_mw):
+    """ptg_gamma_from_tbc equals the oracle's GammaDeterm restatement bit for
+    bit, and the gamma it returns reproduces the conductance: with
+    T = 1/(gamma w/w_max + 1), G_T / (1 - G_T / G_1) = TBC (Newton's stop at
+    |step| <= 1e-6 in gamma)."""
+    spec = _two_branch_spectrum(nk=60, seed=8, ties=False)
+    T = 300.0
+    tbc = tbc_mw * 1e6
+    st, g = A.gamma_from_tbc(spec, T, tbc)
+    ost, og = orc.Oracle(model=synth.nanowire(), spectrum=spec).gamma_from_tbc(T, tbc)
+    assert st == ost == 0 and g == og and g > 0
+    hbar, kB = 1.054571e-34, 1.3806503e-23
+    x = hbar * spec.omega / (kB * T)
+    C = kB * ((x / 2) / np.sinh(x / 2)) ** 2
+    nq = int(spec.weight.sum() / spec.nbranch)
+    base = spec.weight * C * spec.vel / 2 / spec.vol / nq
+    G1 = base.sum()
+    GT = (base / (g * spec.omega / spec.omega.max() + 1)).sum()
+    assert abs(GT / (1 - GT / G1) - tbc) < 1e-5 * tbc
