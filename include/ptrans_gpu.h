@@ -56,6 +56,12 @@ extern "C" {
 #define PTG_SHAPE_POLYGON   1
 #define PTG_SHAPE_SPHERE    2
 #define PTG_SHAPE_CYLINDER  3   /* infinite cylinder, axis parallel to z */
+/* extension: a right circular cylinder of finite length with flat end caps
+   and any axis.  In ptg_geometry its surface record holds the two end
+   points of the axis as a closed vertex list (nvertex = 2: A, B, A), the
+   centre (A+B)/2 and the radius; in ptg_model the grain's generatrix is the
+   centre and grain_axis the vector B - A. */
+#define PTG_SHAPE_CAPPED    4
 /* src/RTMCphon.f90:77-79 */
 #define PTG_TRANS_VALUE     1
 #define PTG_TRANS_GAMMA     2
@@ -112,6 +118,8 @@ typedef struct ptg_model {
   const double* surf_spec;          /* [nsurf_model] or NULL: per-surface       */
                                     /*   specularity override (extension)       */
   uint64_t fluct_seed;              /* seed of the specularity fluctuation      */
+  const double* grain_axis;         /* [3*ngrain] or NULL: axis vector B - A of */
+                                    /*   PTG_SHAPE_CAPPED grains (extension)    */
 } ptg_model;
 
 /* Per-mode bulk phonon data as held in Anphon_type after loadAnphon

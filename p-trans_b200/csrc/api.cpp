@@ -278,6 +278,7 @@ int blob_from_geometry(const GeomSoA& G, int bvh_leaf, std::vector<float4>* out,
   L.bvh_root = L.start + (int)(start.size() ? start.size() : 1);
   L.bvh_node = L.bvh_root + units_of_ints(root.size());
   L.total = L.bvh_node + (int)(nodes.size() ? nodes.size() : 1);
+  L.nbvh = (int)(nodes.size() / 2);
   L.nstart = (int)start.size();
   std::vector<float4> blob((size_t)L.total, make_float4(0, 0, 0, 0));
   std::copy(hot.begin(), hot.end(), blob.begin() + L.hot);
@@ -332,6 +333,7 @@ int build_blob(ptg_handle* h) {
   g32.igrain_fill = G.igrain_fill;
   g32.nmaterial = G.nmaterial;
   g32.stage_smem = h->blob_bytes <= 96 * 1024 ? 1 : 0;
+  g32.has_bvh = L.nbvh > 0 ? 1 : 0;
   return PTG_OK;
 }
 
@@ -522,7 +524,7 @@ int run_transport(ptg_handle* h, const Transport& T) {
     const int block = (bs >= 32 && bs <= 256 && bs % 32 == 0) ? bs : 256;
     const size_t smem = h->g32.stage_smem ? h->blob_bytes : 0;
     int bps = 0;
-    CU(ptg::persistent_occupancy(block, smem, &bps, T.mode));
+    CU(ptg::persistent_occupancy(block, smem, &bps, T.mode, h->g32.has_bvh != 0));
     if (h->opt.blocks_per_sm > 0 && h->opt.blocks_per_sm < bps) bps = h->opt.blocks_per_sm;
     if (bps < 1) bps = 1;
     const int grid = h->num_sms * bps;

@@ -51,6 +51,7 @@ struct ptg_batch {
   double* host_result = nullptr;              /* pinned */
   unsigned long long* host_stats = nullptr;   /* pinned */
   int launch_grid = 0;
+  bool bvh = false;   /* some geometry has a BVH: the kernel built for it */
   ~ptg_batch() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
@@ -127,6 +128,7 @@ extern "C" int ptg_batch_create(const ptg_batch_item* items, int32_t nitems,
     ptg::GeoEntry& e = entries[g];
     memset(&e, 0, sizeof(e));
     e.lay = L;
+    if (L.nbvh > 0) b->bvh = true;
     for (int d = 0; d < 3; ++d) e.box[d] = (float)G.box[d];
     e.scope[0] = (float)G.scope[0];
     e.scope[1] = (float)G.scope[1];
@@ -277,7 +279,7 @@ extern "C" int ptg_batch_create(const ptg_batch_item* items, int32_t nitems,
   rb.dS_geo = b->dS_geo.as<const double>();
   rb.tnorm_geo = b->tnorm_geo.as<const double>();
   int bps = 0;
-  BCU(ptg::persistent_batch_occupancy(256, &bps));
+  BCU(ptg::persistent_batch_occupancy(256, &bps, b->bvh));
   if (o.blocks_per_sm > 0 && o.blocks_per_sm < bps) bps = o.blocks_per_sm;
   if (bps < 1) bps = 1;
   b->launch_grid = b->num_sms * bps;
@@ -293,7 +295,7 @@ extern "C" int ptg_batch_create(const ptg_batch_item* items, int32_t nitems,
   if (ce == cudaSuccess) ce = cudaMemsetAsync(dstats, 0, sizeof(unsigned long long) * 16, b->stream);
   if (ce == cudaSuccess) ce = cudaMemsetAsync(dstats + 5, 0xFF, sizeof(unsigned long long) * 2, b->stream);
   if (ce == cudaSuccess) ce = cudaMemsetAsync(b->queue.p, 0, sizeof(int) * 4, b->stream);
-  if (ce == cudaSuccess && r.nchunk > 0) ce = ptg::launch_persistent_batch(r, b->launch_grid, 256, b->stream);
+  if (ce == cudaSuccess && r.nchunk > 0) ce = ptg::launch_persistent_batch(r, b->launch_grid, 256, b->stream, b->bvh);
   if (ce == cudaSuccess) ce = ptg::launch_kappa_reduce_batch(rb, b->stream);
   if (ce == cudaSuccess)
     ce = cudaMemcpyAsync(b->host_result, b->result.p, sizeof(double) * nres, cudaMemcpyDeviceToHost,

@@ -83,6 +83,7 @@ struct BlobLayout {
   int start;        /* voronoi: float4 (generatrix, grain); bricks: int2 (surf, grain) */
   int bvh_root;     /* int[ngrain_total]: root node of the grain's BVH, -1 linear scan */
   int bvh_node;     /* float4[2*nnode]: (lo, a) (hi, b), see bvh.cpp                  */
+  int nbvh;         /* BVH nodes in the blob (0: every grain scans linearly)          */
   int total;        /* blob size in 16-byte units                                    */
   int nstart;
 };
@@ -96,6 +97,7 @@ struct GeoF32 {
   int periodic_mask;   /* bit f set: box face f is periodic              */
   int kind_grain, igrain_fill, nmaterial;
   int stage_smem;      /* 1: copy the blob to shared memory (bulk copy)  */
+  int has_bvh;         /* 1: some grain has a BVH (kernels built for it)  */
 };
 
 /* One geometry of a batched launch (device table, read through the cache). */
@@ -166,11 +168,12 @@ enum { MODE_FORWARD = 0, MODE_LIST = 1, MODE_ADJOINT = 2, MODE_TRACE = 3 };
 cudaError_t launch_persistent_fp32(const GeoF32& g, const RunF32& r, int grid, int block,
                                    size_t smem, cudaStream_t st, int mode = MODE_FORWARD);
 /* Batched launch over several geometries (forward mode, geometry in global memory). */
-cudaError_t launch_persistent_batch(const RunF32& r, int grid, int block, cudaStream_t st);
-cudaError_t persistent_batch_occupancy(int block, int* blocks_per_sm);
+cudaError_t launch_persistent_batch(const RunF32& r, int grid, int block, cudaStream_t st,
+                                    bool bvh);
+cudaError_t persistent_batch_occupancy(int block, int* blocks_per_sm, bool bvh);
 /* Residency of the persistent kernel for a block size and shared memory. */
 cudaError_t persistent_occupancy(int block, size_t smem, int* blocks_per_sm,
-                                 int mode = MODE_FORWARD);
+                                 int mode = MODE_FORWARD, bool bvh = false);
 
 /* ---------------- FP64 kappa reduction ---------------------------------- */
 

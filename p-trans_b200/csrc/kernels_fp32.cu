@@ -228,69 +228,80 @@ __device__ __forceinline__ float inv_dir(float d) {
 /* Traversal depth bound: the builder limits the depth to 30. */
 constexpr int kBvhStack = 32;
 
-/* Nearest surface of a grain: its BVH when it has one, else every
-   candidate.  tb (the box-grain exit, >= 0) and sb are updated; tb stays
-   >= 0. */
+/* BVH traversal of a grain (root >= 0): ordered descent, the far child
+   pushed with its entry distance and popped only while it can still hold a
+   nearer hit.  Kept out of line so the linear scan that every small grain
+   uses stays compact in the instruction cache. */
 template <class G_t>
+__device__ __noinline__ void scan_bvh(const G_t& G, int root, float px, float py, float pz,
+                                      float dx, float dy, float dz, int last_geom, float eps,
+                                      float zmax, float& tr, int& sb, unsigned& nbox,
+                                      unsigned& nsurf) {
+  const float ix = inv_dir(dx), iy = inv_dir(dy), iz = inv_dir(dz);
+  int stk[kBvhStack];
+  float stt[kBvhStack];
+  int sp = 0;
+  int node = root;
+  while (true) {
+    const float4 n1 = G.node(2 * node + 1);
+    const int cnt = __float_as_int(n1.w);
+    const int a = __float_as_int(G.node(2 * node).w);
+    bool descended = false;
+    if (cnt > 0) {
+      nsurf += (unsigned)cnt;
+      for (int k = a; k < a + cnt; ++k)
+        test_surface(G, G.cand(k), px, py, pz, dx, dy, dz, last_geom, eps, zmax, tr, sb);
+    } else {
+      nbox += 2u;
+      const float tl = box_entry(G.node(2 * a), G.node(2 * a + 1), px, py, pz, ix, iy, iz, tr, eps);
+      const float tg = box_entry(G.node(2 * a + 2), G.node(2 * a + 3), px, py, pz, ix, iy, iz, tr,
+                                 eps);
+      const bool hl = tl < 3.0e38f, hg = tg < 3.0e38f;
+      if (hl && hg) {
+        const bool lf = tl <= tg;
+        if (sp < kBvhStack) {
+          stk[sp] = lf ? a + 1 : a;
+          stt[sp] = lf ? tg : tl;
+          ++sp;
+        }
+        node = lf ? a : a + 1;
+        descended = true;
+      } else if (hl || hg) {
+        node = hl ? a : a + 1;
+        descended = true;
+      }
+    }
+    if (descended) continue;
+    bool found = false;
+    while (sp > 0) {
+      --sp;
+      if (stt[sp] <= tr) {
+        node = stk[sp];
+        found = true;
+        break;
+      }
+    }
+    if (!found) break;
+  }
+}
+
+/* Nearest surface of a grain: its BVH when it has one (kernels built with
+   BVH = true; the others never look for one), else every candidate.  tb
+   (the box-grain exit, >= 0) and sb are updated; tb stays >= 0. */
+template <bool BVH, class G_t>
 __device__ __forceinline__ void scan_grain(const G_t& G, int grain, float px, float py, float pz,
                                            float dx, float dy, float dz, int last_geom, float eps,
                                            float zmax, float& tb, int& sb, unsigned& nbox,
                                            unsigned& nsurf) {
   float tr = tb;
-  const int root = G.bvh_root(grain);
+  const int root = BVH ? G.bvh_root(grain) : -1;
   if (root < 0) {
     const int kb = G.cand_begin(grain), ke = G.cand_begin(grain + 1);
     nsurf += (unsigned)(ke - kb);
     for (int k = kb; k < ke; ++k)
       test_surface(G, G.cand(k), px, py, pz, dx, dy, dz, last_geom, eps, zmax, tr, sb);
   } else {
-    const float ix = inv_dir(dx), iy = inv_dir(dy), iz = inv_dir(dz);
-    int stk[kBvhStack];
-    float stt[kBvhStack];
-    int sp = 0;
-    int node = root;
-    while (true) {
-      const float4 n1 = G.node(2 * node + 1);
-      const int cnt = __float_as_int(n1.w);
-      const int a = __float_as_int(G.node(2 * node).w);
-      bool descended = false;
-      if (cnt > 0) {
-        nsurf += (unsigned)cnt;
-        for (int k = a; k < a + cnt; ++k)
-          test_surface(G, G.cand(k), px, py, pz, dx, dy, dz, last_geom, eps, zmax, tr, sb);
-      } else {
-        nbox += 2u;
-        const float tl = box_entry(G.node(2 * a), G.node(2 * a + 1), px, py, pz, ix, iy, iz, tr, eps);
-        const float tg = box_entry(G.node(2 * a + 2), G.node(2 * a + 3), px, py, pz, ix, iy, iz, tr,
-                                   eps);
-        const bool hl = tl < 3.0e38f, hg = tg < 3.0e38f;
-        if (hl && hg) {
-          const bool lf = tl <= tg;
-          if (sp < kBvhStack) {
-            stk[sp] = lf ? a + 1 : a;
-            stt[sp] = lf ? tg : tl;
-            ++sp;
-          }
-          node = lf ? a : a + 1;
-          descended = true;
-        } else if (hl || hg) {
-          node = hl ? a : a + 1;
-          descended = true;
-        }
-      }
-      if (descended) continue;
-      /* next pushed node that can still hold a nearer hit */
-      bool found = false;
-      while (sp > 0) {
-        --sp;
-        if (stt[sp] <= tr) {
-          node = stk[sp];
-          found = true;
-          break;
-        }
-      }
-      if (!found) break;
-    }
+    scan_bvh(G, root, px, py, pz, dx, dy, dz, last_geom, eps, zmax, tr, sb, nbox, nsurf);
   }
   tb = fmaxf(tr, 0.0f);
 }
@@ -338,62 +349,71 @@ __device__ __forceinline__ float box_dist(float4 lo, float4 hi, float px, float 
   return sqrtf(fmaf(ex, ex, fmaf(ey, ey, ez * ez)));
 }
 
+/* BVH range query for the safe ball: the smallest lower bound of the
+   distance from p to a surface of the grain, searched below d (nodes
+   farther than the bound so far are pruned; a leaf contributes
+   max(distance to its box, nearest plane / quadric bound of its surfaces)).
+   Out of line, like scan_bvh. */
+template <class G_t>
+__device__ __noinline__ float safety_bvh(const G_t& G, int root, float px, float py, float pz,
+                                         float d) {
+  int stk[kBvhStack];
+  float std_[kBvhStack];
+  int sp = 0;
+  int node = root;
+  while (true) {
+    const float4 n0 = G.node(2 * node), n1 = G.node(2 * node + 1);
+    const int cnt = __float_as_int(n1.w);
+    const int a = __float_as_int(n0.w);
+    bool descended = false;
+    if (cnt > 0) {
+      float e = 3.0e38f;
+      for (int k = a; k < a + cnt; ++k) e = fminf(e, surface_lb(G, G.cand(k), px, py, pz));
+      d = fminf(d, fmaxf(box_dist(n0, n1, px, py, pz), e));
+    } else {
+      const float dl = box_dist(G.node(2 * a), G.node(2 * a + 1), px, py, pz);
+      const float dg = box_dist(G.node(2 * a + 2), G.node(2 * a + 3), px, py, pz);
+      const bool lf = dl <= dg;
+      const float dn = lf ? dl : dg, df = lf ? dg : dl;
+      if (dn < d) {
+        if (df < d && sp < kBvhStack) {
+          stk[sp] = lf ? a + 1 : a;
+          std_[sp] = df;
+          ++sp;
+        }
+        node = lf ? a : a + 1;
+        descended = true;
+      }
+    }
+    if (descended) continue;
+    bool found = false;
+    while (sp > 0) {
+      --sp;
+      if (std_[sp] < d) {
+        node = stk[sp];
+        found = true;
+        break;
+      }
+    }
+    if (!found) break;
+  }
+  return d;
+}
+
 /* Lower bound of the distance from p to every box face and to every
    candidate surface of the grain, less 4 eps.  A grain with a BVH is
-   searched only within `cap` (the radius the safe ball needs), pruning
-   nodes farther than the bound found so far; a leaf contributes
-   max(distance to its box, nearest plane / quadric bound of its surfaces). */
-template <class G_t>
+   searched only within `cap` (the radius the safe ball needs). */
+template <bool BVH, class G_t>
 __device__ __forceinline__ float safety(const G_t& G, int grain, float px, float py, float pz,
                                         float X, float Y, float Z, float eps, float cap) {
   float d = fminf(fminf(fminf(px, X - px), fminf(py, Y - py)), fminf(pz, Z - pz));
   if (grain > 0) {
-    const int root = G.bvh_root(grain);
+    const int root = BVH ? G.bvh_root(grain) : -1;
     if (root < 0) {
       const int kb = G.cand_begin(grain), ke = G.cand_begin(grain + 1);
       for (int k = kb; k < ke; ++k) d = fminf(d, surface_lb(G, G.cand(k), px, py, pz));
     } else {
-      d = fminf(d, cap);
-      int stk[kBvhStack];
-      float std_[kBvhStack];
-      int sp = 0;
-      int node = root;
-      while (true) {
-        const float4 n0 = G.node(2 * node), n1 = G.node(2 * node + 1);
-        const int cnt = __float_as_int(n1.w);
-        const int a = __float_as_int(n0.w);
-        bool descended = false;
-        if (cnt > 0) {
-          float e = 3.0e38f;
-          for (int k = a; k < a + cnt; ++k) e = fminf(e, surface_lb(G, G.cand(k), px, py, pz));
-          d = fminf(d, fmaxf(box_dist(n0, n1, px, py, pz), e));
-        } else {
-          const float dl = box_dist(G.node(2 * a), G.node(2 * a + 1), px, py, pz);
-          const float dg = box_dist(G.node(2 * a + 2), G.node(2 * a + 3), px, py, pz);
-          const bool lf = dl <= dg;
-          const float dn = lf ? dl : dg, df = lf ? dg : dl;
-          if (dn < d) {
-            if (df < d && sp < kBvhStack) {
-              stk[sp] = lf ? a + 1 : a;
-              std_[sp] = df;
-              ++sp;
-            }
-            node = lf ? a : a + 1;
-            descended = true;
-          }
-        }
-        if (descended) continue;
-        bool found = false;
-        while (sp > 0) {
-          --sp;
-          if (std_[sp] < d) {
-            node = stk[sp];
-            found = true;
-            break;
-          }
-        }
-        if (!found) break;
-      }
+      d = safety_bvh(G, root, px, py, pz, fminf(d, cap));
     }
   }
   return d - 4.0f * eps;
@@ -482,7 +502,7 @@ constexpr int kCoopRoundsBusy = 4;
    walk needs about (radius / MFP)^2 flights to leave the ball */
 constexpr float kBallCapMfp = 32.0f;
 
-template <bool SMEM, int MODE, bool BATCH>
+template <bool SMEM, int MODE, bool BATCH, bool BVH>
 __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   typename std::conditional<BATCH, GeoBatch, Geo<SMEM>>::type G;
   G.lay = gp.lay;
@@ -696,6 +716,9 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           const uint32_t cslo = __shfl_sync(FULL, slo, L), cshi = __shfl_sync(FULL, shi, L);
           const int cgrain = __shfl_sync(FULL, grain, L);
           int clast = __shfl_sync(FULL, last_geom, L);
+          /* the phonon's safe ball: flights ending inside it skip the test */
+          float cbx = __shfl_sync(FULL, bx, L), cby = __shfl_sync(FULL, by, L);
+          float cbz = __shfl_sync(FULL, bz, L), cbr2 = __shfl_sync(FULL, br2, L);
           float clen = 0.0f;
           unsigned cnpp = 0, ctaken = 0, crounds = 0;
           int stop = 0;  /* 0 round limit, 1 surface hit, 2 lost or capped */
@@ -732,14 +755,24 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             const bool inbox = qx >= -eps && qx <= X + eps && qy >= -eps && qy <= Y + eps &&
                                qz >= -eps && qz <= Z + eps;
             const bool capd = (unsigned long long)cfl + (unsigned)lane >= r.max_flights;
-            float tb;
-            int sb;
-            slab_exit(qx, qy, qz, sdx, sdy, sdz, X, Y, Z, tb, sb);
-            if (cgrain > 0)
-              scan_grain(G, cgrain, qx, qy, qz, sdx, sdy, sdz, lane == 0 ? clast : -1, eps, Z,
-                         tb, sb, my_box_tests, my_surf_tests);
+            /* a flight that starts and ends in the safe ball stays in it (the
+               ball is convex and holds no surface) and ends in a p-p event;
+               the others take the intersection test */
+            const float ex = fmaf(sfp, sdx, qx) - cbx, ey = fmaf(sfp, sdy, qy) - cby;
+            const float ez = fmaf(sfp, sdz, qz) - cbz;
+            const float sx = qx - cbx, sy = qy - cby, sz = qz - cbz;
+            const bool in_ball = fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < cbr2 &&
+                                 fmaf(sx, sx, fmaf(sy, sy, sz * sz)) < cbr2;
+            float tb = 3.0e38f;
+            int sb = -1;
+            if (!in_ball) {
+              slab_exit(qx, qy, qz, sdx, sdy, sdz, X, Y, Z, tb, sb);
+              if (cgrain > 0)
+                scan_grain<BVH>(G, cgrain, qx, qy, qz, sdx, sdy, sdz, lane == 0 ? clast : -1, eps,
+                                Z, tb, sb, my_box_tests, my_surf_tests);
+            }
             const bool brk = !inbox || capd;
-            const unsigned sm = __ballot_sync(FULL, brk || !(sfp < tb));
+            const unsigned sm = __ballot_sync(FULL, brk || (!in_ball && !(sfp < tb)));
             const int j = sm ? __ffs(sm) - 1 : 32;
             if (MODE == MODE_ADJOINT) {
               float l = lane < j ? sfp : 0.0f;
@@ -771,11 +804,18 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             cdx = __shfl_sync(FULL, nx, 31); cdy = __shfl_sync(FULL, ny, 31);
             cdz = __shfl_sync(FULL, nz, 31); cfp = __shfl_sync(FULL, nf, 31);
             cfl += 32u;
+            /* a new ball where the walk left the old one */
+            if (!__shfl_sync(FULL, in_ball, 31) && r.fast_steps > 0) {
+              const float d = safety<BVH>(G, cgrain, cpx, cpy, cpz, X, Y, Z, eps, kBallCapMfp * clam);
+              cbx = cpx; cby = cpy; cbz = cpz;
+              cbr2 = d > 0.0f ? d * d : 0.0f;
+            }
             clast = -1;
           }
           if (lane == L) {
             px = cpx; py = cpy; pz = cpz;
             dx = cdx; dy = cdy; dz = cdz; fp = cfp;
+            bx = cbx; by = cby; bz = cbz; br2 = cbr2;
             flight = cfl;
             last_geom = clast;
             if (MODE == MODE_ADJOINT) {
@@ -867,7 +907,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           R = philox10(flight, c1, slo, shi, key);
           slab_exit(px, py, pz, dx, dy, dz, X, Y, Z, tb, sb);
           if (grain > 0)
-            scan_grain(G, grain, px, py, pz, dx, dy, dz, last_geom, eps, Z, tb, sb, my_box_tests,
+            scan_grain<BVH>(G, grain, px, py, pz, dx, dy, dz, last_geom, eps, Z, tb, sb, my_box_tests,
                        my_surf_tests);
           go = true;
         }
@@ -893,7 +933,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             last_geom = -1;
             br2 = 0.0f;
             if (MODE != MODE_TRACE && r.fast_steps > 0 && lam < flmax) {
-              const float d = safety(G, grain, px, py, pz, X, Y, Z, eps, kBallCapMfp * lam);
+              const float d = safety<BVH>(G, grain, px, py, pz, X, Y, Z, eps, kBallCapMfp * lam);
               ++my_balls;
               if (d > 0.0f) { bx = px; by = py; bz = pz; br2 = d * d; }
             }
@@ -1099,58 +1139,72 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
 
 }  // namespace
 
-template <int MODE>
+template <int MODE, bool BVH>
 cudaError_t occupancy_mode(int block, size_t smem, int* bps) {
   if (smem > 0)
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_persistent<true, MODE, false>,
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_persistent<true, MODE, false, BVH>,
                                                          block, smem);
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_persistent<false, MODE, false>,
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_persistent<false, MODE, false, BVH>,
                                                        block, 0);
 }
 
-template <int MODE>
+template <int MODE, bool BVH>
 cudaError_t launch_mode(const GeoF32& g, const RunF32& r, int grid, int block, size_t smem,
                         cudaStream_t st) {
   if (g.stage_smem && smem > 0) {
     if (smem > 48 * 1024) {
-      cudaError_t e = cudaFuncSetAttribute(k_persistent<true, MODE, false>,
+      cudaError_t e = cudaFuncSetAttribute(k_persistent<true, MODE, false, BVH>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (e != cudaSuccess) return e;
     }
-    k_persistent<true, MODE, false><<<grid, block, smem, st>>>(g, r);
+    k_persistent<true, MODE, false, BVH><<<grid, block, smem, st>>>(g, r);
   } else {
-    k_persistent<false, MODE, false><<<grid, block, 0, st>>>(g, r);
+    k_persistent<false, MODE, false, BVH><<<grid, block, 0, st>>>(g, r);
   }
   return cudaGetLastError();
 }
 
-cudaError_t persistent_batch_occupancy(int block, int* bps) {
+cudaError_t persistent_batch_occupancy(int block, int* bps, bool bvh) {
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      bps, k_persistent<false, MODE_FORWARD, true>, block, 0);
+      bps, bvh ? k_persistent<false, MODE_FORWARD, true, true> : k_persistent<false, MODE_FORWARD, true, false>,
+      block, 0);
 }
 
-cudaError_t launch_persistent_batch(const RunF32& r, int grid, int block, cudaStream_t st) {
+cudaError_t launch_persistent_batch(const RunF32& r, int grid, int block, cudaStream_t st, bool bvh) {
   if (block != kBlock) return cudaErrorInvalidConfiguration;
   GeoF32 g;
   memset(&g, 0, sizeof(g));
-  k_persistent<false, MODE_FORWARD, true><<<grid, block, 0, st>>>(g, r);
+  if (bvh) k_persistent<false, MODE_FORWARD, true, true><<<grid, block, 0, st>>>(g, r);
+  else k_persistent<false, MODE_FORWARD, true, false><<<grid, block, 0, st>>>(g, r);
   return cudaGetLastError();
 }
 
-cudaError_t persistent_occupancy(int block, size_t smem, int* bps, int mode) {
-  if (mode == MODE_LIST) return occupancy_mode<MODE_LIST>(block, smem, bps);
-  if (mode == MODE_ADJOINT) return occupancy_mode<MODE_ADJOINT>(block, smem, bps);
-  if (mode == MODE_TRACE) return occupancy_mode<MODE_TRACE>(block, smem, bps);
-  return occupancy_mode<MODE_FORWARD>(block, smem, bps);
+template <bool BVH>
+cudaError_t occupancy_bvh(int block, size_t smem, int* bps, int mode) {
+  if (mode == MODE_LIST) return occupancy_mode<MODE_LIST, BVH>(block, smem, bps);
+  if (mode == MODE_ADJOINT) return occupancy_mode<MODE_ADJOINT, BVH>(block, smem, bps);
+  if (mode == MODE_TRACE) return occupancy_mode<MODE_TRACE, BVH>(block, smem, bps);
+  return occupancy_mode<MODE_FORWARD, BVH>(block, smem, bps);
+}
+
+cudaError_t persistent_occupancy(int block, size_t smem, int* bps, int mode, bool bvh) {
+  return bvh ? occupancy_bvh<true>(block, smem, bps, mode) : occupancy_bvh<false>(block, smem, bps, mode);
+}
+
+template <bool BVH>
+cudaError_t launch_bvh(const GeoF32& g, const RunF32& r, int grid, int block, size_t smem,
+                       cudaStream_t st, int mode) {
+  if (mode == MODE_LIST) return launch_mode<MODE_LIST, BVH>(g, r, grid, block, smem, st);
+  if (mode == MODE_ADJOINT) return launch_mode<MODE_ADJOINT, BVH>(g, r, grid, block, smem, st);
+  if (mode == MODE_TRACE) return launch_mode<MODE_TRACE, BVH>(g, r, grid, block, smem, st);
+  return launch_mode<MODE_FORWARD, BVH>(g, r, grid, block, smem, st);
 }
 
 cudaError_t launch_persistent_fp32(const GeoF32& g, const RunF32& r, int grid, int block,
                                    size_t smem, cudaStream_t st, int mode) {
   if (block > kBlock || block % 32) return cudaErrorInvalidConfiguration;
-  if (mode == MODE_LIST) return launch_mode<MODE_LIST>(g, r, grid, block, smem, st);
-  if (mode == MODE_ADJOINT) return launch_mode<MODE_ADJOINT>(g, r, grid, block, smem, st);
-  if (mode == MODE_TRACE) return launch_mode<MODE_TRACE>(g, r, grid, block, smem, st);
-  return launch_mode<MODE_FORWARD>(g, r, grid, block, smem, st);
+  return g.has_bvh ? launch_bvh<true>(g, r, grid, block, smem, st, mode)
+                   : launch_bvh<false>(g, r, grid, block, smem, st, mode);
 }
 
 }  // namespace ptg

@@ -18,8 +18,8 @@ def test_trace_replays_the_forward_trajectories(tmp_path):
     m = synth.film_with_holes(lx=200.0, ly=150.0, lz=80.0, nholes=2, radius=25.0, seed=3,
                               p_hole=0.2, t_hole=0.0, p_z=0.4)
     spec = synth.spectrum(4, seed=2, mfp_lo=3e-9, mfp_hi=3e-7)
-    run = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=4, np_=50, seed=17, precision=A.PREC_FP32)
-    ntask = 4 * 3
+    run = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=5, np_=50, seed=17, precision=A.PREC_FP32)
+    ntask = 4 * 4
     gb = A.GeomBuf(m)
     with A.Handle(gb.view, spec) as h:
         fwd = h.kappa(run, want_counts=True)
