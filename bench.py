@@ -328,6 +328,65 @@ def run_structure(args):
     return 0
 
 
+def run_c3(args):
+    """C3: 64 spheres (r ~ U(20, 80) nm) and 16 capped cylinders of random
+    axis (r = 30 nm, length ~ U(100, 400) nm) as voids in a 1000^3 nm box,
+    per-surface specularity p ~ U(0, 1), diffuse walls; 20000-mode spectrum,
+    64 bins, per-mode MFP runs.  Forward kappa (device time) and the adjoint
+    (forward listing pass + replay, wall time of the call) with the number of
+    resolved derivatives dkappa/dp_k."""
+    import torch
+    torch.cuda.set_device(0)
+    pkg = load_pkg()
+    A, synth = pkg.abi, pkg.synth
+    model = synth.spheres_cylinders_box(64, 16, l=1000.0, seed=0)
+    spec = synth.spectrum(20000, seed=0)
+    gb = A.GeomBuf(model)
+    npt = args.np
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda:0")
+    bins = dict(temperature=300.0, nbins=64, bin_omega=(0.0, 15.0 * 2 * math.pi * 1e12))
+    run = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=11, np_=npt, seed=12345, precision=A.PREC_FP32, **bins)
+    with A.Handle(gb.view, spec) as h:
+        for _ in range(args.warmup):
+            h.kappa(run)
+        ms = fl = 0.0
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            out = h.kappa(run)
+            st = h.stats()
+            ms += st["kernel_ms"] + st["reduce_ms"]
+            fl += st["flights"]
+        h.adjoint(run)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        adj = h.adjoint(run)
+        adj_s = time.perf_counter() - t0
+        h.kappa(A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=11, np_=2, seed=12345, precision=A.PREC_FP64, **bins))
+        s64 = h.stats()
+        h.kappa(A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=11, np_=2, seed=12345, precision=A.PREC_FP32, **bins))
+        s32 = h.stats()
+    v = fl / (ms * 1e-3)
+    dk, de = adj["dk_dp"], adj["dk_dp_stderr"]
+    v64 = s64["flights"] / ((s64["kernel_ms"] + s64["reduce_ms"]) * 1e-3)
+    v32s = s32["flights"] / ((s32["kernel_ms"] + s32["reduce_ms"]) * 1e-3)
+    print(json.dumps({
+        "metric": "phonon free-flights/s, C3 spheres + random-axis capped cylinders, forward + adjoint",
+        "value": v, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "64 spheres r~U(20,80) + 16 capped cylinders r=30, random axes, length~U(100,400), "
+                               "voids in 1000^3 nm, per-surface p~U(0,1), diffuse walls; 20000 modes, 64 bins",
+                   "particles_per_task": npt, "samples": 20000 * 10 * npt},
+        "flights_per_step": fl / args.steps, "kappa": out["kappa"], "kappa_stderr": out["kappa_stderr"],
+        "adjoint": {"wall_s": adj_s, "kappa": adj["kappa"], "replayed": adj["replayed"],
+                    "mismatched": adj["mismatched"], "surface_records": int(dk.size),
+                    "resolved_3sigma": int(np.sum(np.abs(dk) > 3 * de)), "dk_dscale": adj["dk_dscale"],
+                    "dk_dscale_stderr": adj["dk_dscale_stderr"]},
+        "plain_fp64": {"value": v64, "unit": UNIT, "sample": "all modes, 2 particles per (mode, angle) task",
+                       "fp32_same_sample": v32s, "speedup_fp32_over_fp64_same_sample": v32s / v64}}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -337,9 +396,9 @@ def main():
     ap.add_argument("--np", type=int, default=500, help="particles per (mode, angle) per GPU")
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="thinfilm", choices=["thinfilm", "c5", "voronoi", "mesh"],
-                    help="thinfilm: the metric's configuration; c5: 256-film batched screening; "
-                         "voronoi / mesh: the C4 structures")
+    ap.add_argument("--workload", default="thinfilm", choices=["thinfilm", "c3", "c5", "voronoi", "mesh"],
+                    help="thinfilm: the metric's configuration; c3: spheres + capped cylinders with "
+                         "the adjoint; c5: 256-film batched screening; voronoi / mesh: the C4 structures")
     ap.add_argument("--fp64-subset", type=int, default=16,
                     help="c5: films timed one by one with the plain FP64 kernel")
     args = ap.parse_args()
@@ -349,6 +408,8 @@ def main():
         return run_c5(args)
     if args.workload in ("voronoi", "mesh"):
         return run_structure(args)
+    if args.workload == "c3":
+        return run_c3(args)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -258,6 +258,17 @@ int orc_build_model(const ptg_model* m, const ptg_spectrum* sp, orc_handle** out
         }
         if (all_xle0) { gr.incident = 1; s.incident = 1; s.internal = 0; }
         if (all_xle0 || all_xgeX || all_yle0 || all_ygeY || all_zle0 || all_zgeZ) s.internal = 0;
+      } else if (shape == PTG_SHAPE_CAPPED) {
+        /* extension: capped cylinder, axis end points c -/+ axis/2 (closed) */
+        if (!m->grain_axis) { orc_free(h); return PTG_ERR_INVALID; }
+        const double* ax = m->grain_axis + 3 * (ig - 1);
+        s.nvertex = 2;
+        s.vertex.resize(9);
+        for (int d = 0; d < 3; ++d) {
+          s.vertex[d] = s.center[d] - 0.5 * ax[d];
+          s.vertex[3 + d] = s.center[d] + 0.5 * ax[d];
+          s.vertex[6 + d] = s.vertex[d];
+        }
       } else {
         s.nvertex = 0;
       }
@@ -525,12 +536,89 @@ bool dist_cylinder(const double* R0, const double* D, const Surf& s, double boxz
   return true;
 }
 
+/* Axis of a capped cylinder from its end points A (vertex 0) and B
+   (vertex 1): unit axis a, half length hl. */
+void capped_axis(const Surf& s, double* a, double* hl) {
+  double e[3];
+  for (int d = 0; d < 3; ++d) e[d] = s.vertex[3 + d] - s.vertex[d];
+  const double len = sqrt(dot3(e, e));
+  for (int d = 0; d < 3; ++d) a[d] = e[d] / len;
+  *hl = 0.5 * len;
+}
+
+/* Extension: ray against a capped cylinder (centre c, unit axis a, radius r,
+   half length hl), written like the reference's quadric tests: the nearest
+   strictly positive distance over the lateral surface (axial coordinate
+   within the caps) and the two cap discs (radial distance within r). */
+bool dist_capped(const double* R0, const double* D, const Surf& s, double* L) {
+  double a[3], hl;
+  capped_axis(s, a, &hl);
+  double w[3];
+  for (int d = 0; d < 3; ++d) w[d] = R0[d] - s.center[d];
+  const double s0 = dot3(w, a), ds = dot3(D, a);
+  double wp[3], dp[3];
+  for (int d = 0; d < 3; ++d) {
+    wp[d] = w[d] - s0 * a[d];
+    dp[d] = D[d] - ds * a[d];
+  }
+  const double r2 = s.radius * s.radius;
+  double best = 0.0;
+  bool hit = false;
+  const double A2 = dot3(dp, dp);
+  if (A2 > 0.0) {
+    const double B = dot3(wp, dp), C = dot3(wp, wp) - r2;
+    const double disc = B * B - A2 * C;
+    if (disc >= 0.0) {
+      const double sq = sqrt(disc);
+      const double t[2] = {(-B - sq) / A2, (-B + sq) / A2};
+      for (int i = 0; i < 2; ++i) {
+        if (!(t[i] > 0.0) || (hit && !(t[i] < best))) continue;
+        if (fabs(s0 + t[i] * ds) <= hl) { best = t[i]; hit = true; }
+      }
+    }
+  }
+  if (ds != 0.0) {
+    for (int i = 0; i < 2; ++i) {
+      const double c = (i == 0) ? -hl : hl;
+      const double t = (c - s0) / ds;
+      if (!(t > 0.0) || (hit && !(t < best))) continue;
+      double q[3];
+      for (int d = 0; d < 3; ++d) q[d] = wp[d] + t * dp[d];
+      if (dot3(q, q) <= r2) { best = t; hit = true; }
+    }
+  }
+  if (!hit) return false;
+  *L = best;
+  return true;
+}
+
+/* Outward normal of the capped-cylinder piece nearest to R: a cap (+-a) when
+   the axial distance to it is smaller than the radial distance to the
+   mantle, else the radial direction. */
+void capped_normal(const Surf& s, const double* R, double* N) {
+  double a[3], hl;
+  capped_axis(s, a, &hl);
+  double w[3];
+  for (int d = 0; d < 3; ++d) w[d] = R[d] - s.center[d];
+  const double sa = dot3(w, a);
+  double wp[3];
+  for (int d = 0; d < 3; ++d) wp[d] = w[d] - sa * a[d];
+  const double rho = sqrt(dot3(wp, wp));
+  if (fabs(fabs(sa) - hl) < fabs(rho - s.radius)) {
+    const double sg = (sa < 0.0) ? -1.0 : 1.0;
+    for (int d = 0; d < 3; ++d) N[d] = sg * a[d];
+  } else {
+    for (int d = 0; d < 3; ++d) N[d] = wp[d] / rho;
+  }
+}
+
 bool surface_distance(const orc_handle* h, const double* R0, const double* D, const Surf& s,
                       double* L) {
   switch (s.shape) {
     case PTG_SHAPE_POLYGON: return dist_polygon(R0, D, s, L);
     case PTG_SHAPE_SPHERE: return dist_sphere(R0, D, s, L);
     case PTG_SHAPE_CYLINDER: return dist_cylinder(R0, D, s, h->box[2], L);
+    case PTG_SHAPE_CAPPED: return dist_capped(R0, D, s, L);
   }
   return false;
 }
@@ -539,6 +627,10 @@ bool surface_distance(const orc_handle* h, const double* R0, const double* D, co
 void surface_normal(const Surf& s, const double* R, double* N) {
   if (s.shape == PTG_SHAPE_POLYGON) {
     for (int d = 0; d < 3; ++d) N[d] = s.normal[d];
+    return;
+  }
+  if (s.shape == PTG_SHAPE_CAPPED) {
+    capped_normal(s, R, N);
     return;
   }
   double Rcs[3];
@@ -563,7 +655,18 @@ void surface_rotation(const Surf& s, const double* R, double* Rm) {
     return;
   }
   double n[3];
-  if (s.shape == PTG_SHAPE_SPHERE) {
+  if (s.shape == PTG_SHAPE_CAPPED) {
+    /* frame around the piece's normal, built like the sphere's */
+    capped_normal(s, R, n);
+    for (int d = 0; d < 3; ++d) Rm[6 + d] = n[d];
+    if (fabs(n[2]) == 1.0 || (n[0] * n[0] == 0.0 && n[1] * n[1] == 0.0)) {
+      Rm[3] = 0; Rm[4] = 1; Rm[5] = 0; Rm[0] = 1; Rm[1] = 0; Rm[2] = 0;
+    } else {
+      double q = sqrt(n[0] * n[0] + n[1] * n[1]);
+      Rm[3] = -n[1] / q; Rm[4] = n[0] / q; Rm[5] = 0.0;
+      cross3(&Rm[3], &Rm[6], &Rm[0]);
+    }
+  } else if (s.shape == PTG_SHAPE_SPHERE) {
     double Rcs[3];
     for (int d = 0; d < 3; ++d) Rcs[d] = R[d] - s.center[d];
     double inv = 1.0 / sqrt(dot3(Rcs, Rcs));

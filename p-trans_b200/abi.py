@@ -32,7 +32,7 @@ PTG_ERR_NOMEM = 6
 PTG_ERR_IO = 7
 PTG_ERR_UNSUPPORTED = 8
 
-SHAPE_POLYGON, SHAPE_SPHERE, SHAPE_CYLINDER = 1, 2, 3
+SHAPE_POLYGON, SHAPE_SPHERE, SHAPE_CYLINDER, SHAPE_CAPPED = 1, 2, 3, 4
 TRANS_VALUE, TRANS_GAMMA, TRANS_TBC = 1, 2, 3
 MFP_MATTHIESSEN, MFP_GRID, MFP_PER_MODE = 1, 2, 3
 GRAIN_VORONOI, GRAIN_BRICKS = 1, 2
@@ -55,7 +55,7 @@ class PtgModel(C.Structure):
         ("grain_shape", I32P), ("grain_generatrix", F64P), ("grain_diameter", F64P),
         ("grain_material", I32P), ("grain_nfacet", I32P), ("facet_nvertex", I32P),
         ("facet_vertex", F64P), ("surf_material_to", I32P), ("surf_grain_to", I32P),
-        ("surf_spec", F64P), ("fluct_seed", C.c_uint64),
+        ("surf_spec", F64P), ("fluct_seed", C.c_uint64), ("grain_axis", F64P),
     ]
 
 
@@ -266,6 +266,7 @@ class Model:
     nt2: int = 1
     surf_spec: Optional[np.ndarray] = None
     fluct_seed: int = 0
+    grain_axis: Optional[np.ndarray] = None
 
     def __post_init__(self):
         i32 = lambda a: np.ascontiguousarray(np.asarray(a, dtype=np.int32).ravel())
@@ -284,6 +285,8 @@ class Model:
         self.tt_spec = f64(self.tt_spec)
         if self.surf_spec is not None:
             self.surf_spec = f64(self.surf_spec)
+        if self.grain_axis is not None:
+            self.grain_axis = f64(self.grain_axis)
 
     @property
     def ngrain(self) -> int:
@@ -315,6 +318,7 @@ class Model:
         m.surf_grain_to = _ptr(self.surf_grain_to, C.c_int32)
         m.surf_spec = _ptr(self.surf_spec, C.c_double)
         m.fluct_seed = self.fluct_seed
+        m.grain_axis = _ptr(self.grain_axis, C.c_double)
         m._keep = self  # arrays stay alive with the struct
         return m
 

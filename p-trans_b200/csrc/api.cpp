@@ -138,7 +138,13 @@ int blob_from_geometry(const GeomSoA& G, int bvh_leaf, std::vector<float4>* out,
     for (int s = fb; s < fe; ++s) {
       if (G.shape[s] == PTG_SHAPE_POLYGON) continue;
       for (int t = G.grain_begin[1]; t < fb; ++t) {
-        if (G.shape[t] == G.shape[s] && G.radius[t] == G.radius[s] &&
+        bool same_axis = true;
+        if (G.shape[s] == PTG_SHAPE_CAPPED && G.shape[t] == PTG_SHAPE_CAPPED) {
+          const double* vs = &G.vertex[3 * (size_t)G.vertex_begin[s]];
+          const double* vt = &G.vertex[3 * (size_t)G.vertex_begin[t]];
+          for (int d = 0; d < 6; ++d) same_axis = same_axis && vs[d] == vt[d];
+        }
+        if (G.shape[t] == G.shape[s] && G.radius[t] == G.radius[s] && same_axis &&
             G.center[3 * t] == G.center[3 * s] && G.center[3 * t + 1] == G.center[3 * s + 1] &&
             G.center[3 * t + 2] == G.center[3 * s + 2]) {
           geom_id[s] = t;
@@ -194,6 +200,15 @@ int blob_from_geometry(const GeomSoA& G, int bvh_leaf, std::vector<float4>* out,
         const int interior = (g != G.igrain_fill) ? ptg::REC_INTERIOR : 0;
         hot[2 * s] = f4(c[0], c[1], c[2], G.radius[s]);
         hot[2 * s + 1] = i4(ptg::REC_SPHERE | interior, 0, 0, geom_id[s]);
+      } else if (G.shape[s] == PTG_SHAPE_CAPPED) {
+        const int interior = (g != G.igrain_fill) ? ptg::REC_INTERIOR : 0;
+        const double* v = &G.vertex[3 * (size_t)G.vertex_begin[s]];
+        double e[3] = {v[3] - v[0], v[4] - v[1], v[5] - v[2]};
+        const double len = sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+        const int e0 = (int)edges.size();
+        edges.push_back(f4(e[0] / len, e[1] / len, e[2] / len, 0.5 * len));
+        hot[2 * s] = f4(c[0], c[1], c[2], G.radius[s]);
+        hot[2 * s + 1] = i4(ptg::REC_CAP | interior, e0, 0, geom_id[s]);
       } else {
         const int interior = (g != G.igrain_fill) ? ptg::REC_INTERIOR : 0;
         hot[2 * s] = f4(c[0], c[1], G.radius[s], 0.0);
@@ -232,6 +247,18 @@ int blob_from_geometry(const GeomSoA& G, int bvh_leaf, std::vector<float4>* out,
               l[d] = std::min(l[d], v[3 * k + d]);
               h[d] = std::max(h[d], v[3 * k + d]);
             }
+        } else if (G.shape[s] == PTG_SHAPE_CAPPED) {
+          /* extent per axis: half length times |a_d| + radius times sin */
+          const double* c = &G.center[3 * s];
+          const double* v = &G.vertex[3 * (size_t)G.vertex_begin[s]];
+          double e[3] = {v[3] - v[0], v[4] - v[1], v[5] - v[2]};
+          const double len = sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+          for (int d = 0; d < 3; ++d) {
+            const double ad = fabs(e[d]) / len;
+            const double ext = 0.5 * len * ad + G.radius[s] * sqrt(std::max(0.0, 1.0 - ad * ad));
+            l[d] = c[d] - ext;
+            h[d] = c[d] + ext;
+          }
         } else {
           const double* c = &G.center[3 * s];
           const double r = G.radius[s];
@@ -279,6 +306,8 @@ int blob_from_geometry(const GeomSoA& G, int bvh_leaf, std::vector<float4>* out,
   L.bvh_node = L.bvh_root + units_of_ints(root.size());
   L.total = L.bvh_node + (int)(nodes.size() ? nodes.size() : 1);
   L.nbvh = (int)(nodes.size() / 2);
+  L.ncap = 0;
+  for (int s = 0; s < ns; ++s) L.ncap += G.shape[s] == PTG_SHAPE_CAPPED ? 1 : 0;
   L.nstart = (int)start.size();
   std::vector<float4> blob((size_t)L.total, make_float4(0, 0, 0, 0));
   std::copy(hot.begin(), hot.end(), blob.begin() + L.hot);
@@ -333,7 +362,7 @@ int build_blob(ptg_handle* h) {
   g32.igrain_fill = G.igrain_fill;
   g32.nmaterial = G.nmaterial;
   g32.stage_smem = h->blob_bytes <= 96 * 1024 ? 1 : 0;
-  g32.has_bvh = L.nbvh > 0 ? 1 : 0;
+  g32.has_ext = (L.nbvh > 0 || L.ncap > 0) ? 1 : 0;
   return PTG_OK;
 }
 
@@ -524,7 +553,7 @@ int run_transport(ptg_handle* h, const Transport& T) {
     const int block = (bs >= 32 && bs <= 256 && bs % 32 == 0) ? bs : 256;
     const size_t smem = h->g32.stage_smem ? h->blob_bytes : 0;
     int bps = 0;
-    CU(ptg::persistent_occupancy(block, smem, &bps, T.mode, h->g32.has_bvh != 0));
+    CU(ptg::persistent_occupancy(block, smem, &bps, T.mode, h->g32.has_ext != 0));
     if (h->opt.blocks_per_sm > 0 && h->opt.blocks_per_sm < bps) bps = h->opt.blocks_per_sm;
     if (bps < 1) bps = 1;
     const int grid = h->num_sms * bps;

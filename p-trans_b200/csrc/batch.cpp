@@ -51,7 +51,7 @@ struct ptg_batch {
   double* host_result = nullptr;              /* pinned */
   unsigned long long* host_stats = nullptr;   /* pinned */
   int launch_grid = 0;
-  bool bvh = false;   /* some geometry has a BVH: the kernel built for it */
+  bool bvh = false;   /* a BVH or capped cylinders: the kernel built for them */
   ~ptg_batch() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
@@ -128,7 +128,7 @@ extern "C" int ptg_batch_create(const ptg_batch_item* items, int32_t nitems,
     ptg::GeoEntry& e = entries[g];
     memset(&e, 0, sizeof(e));
     e.lay = L;
-    if (L.nbvh > 0) b->bvh = true;
+    if (L.nbvh > 0 || L.ncap > 0) b->bvh = true;
     for (int d = 0; d < 3; ++d) e.box[d] = (float)G.box[d];
     e.scope[0] = (float)G.scope[0];
     e.scope[1] = (float)G.scope[1];

@@ -11,6 +11,7 @@
  *   setupSurfaceGeometry       :1433-1491  (centre, averaged normal, frame)
  */
 #include <math.h>
+#include <algorithm>
 #include <string.h>
 
 #include <string>
@@ -264,8 +265,12 @@ int build_geometry(const ptg_model* m, GeomSoA* out, std::string* why) {
     GrainRec& g = grains[ig];
     for (int d = 0; d < 3; ++d) g.gen[d] = m->grain_generatrix[3 * (ig - 1) + d];
     const int shape = bricks ? m->grain_shape[ig - 1] : PTG_SHAPE_POLYGON;
-    if (shape < PTG_SHAPE_POLYGON || shape > PTG_SHAPE_CYLINDER) {
+    if (shape < PTG_SHAPE_POLYGON || shape > PTG_SHAPE_CAPPED) {
       *why = "unknown grain shape";
+      return PTG_ERR_INVALID;
+    }
+    if (shape == PTG_SHAPE_CAPPED && !m->grain_axis) {
+      *why = "capped cylinders need grain_axis";
       return PTG_ERR_INVALID;
     }
     const int32_t mat1 = m->grain_material[ig - 1];
@@ -308,6 +313,18 @@ int build_geometry(const ptg_model* m, GeomSoA* out, std::string* why) {
         if (lo[0] || hi[0] || lo[1] || hi[1] || lo[2] || hi[2]) s.internal = 0;
       } else {
         if (!finite3(s.center)) { *why = "non-finite centre"; return PTG_ERR_INVALID; }
+        if (shape == PTG_SHAPE_CAPPED) {
+          /* axis end points A = c - axis/2, B = c + axis/2, closed list */
+          const double* ax = m->grain_axis + 3 * (ig - 1);
+          if (!finite3(ax) || !(dot(ax, ax) > 0.0)) { *why = "capped cylinder axis must be > 0"; return PTG_ERR_INVALID; }
+          s.nvertex = 2;
+          s.v.resize(9);
+          for (int d = 0; d < 3; ++d) {
+            s.v[d] = s.center[d] - 0.5 * ax[d];
+            s.v[3 + d] = s.center[d] + 0.5 * ax[d];
+            s.v[6 + d] = s.v[d];
+          }
+        }
       }
       const int32_t mto = m->surf_material_to[mpos];
       s.gout = m->surf_grain_to[mpos];
@@ -348,12 +365,14 @@ int build_geometry(const ptg_model* m, GeomSoA* out, std::string* why) {
         for (int d = 0; d < 3; ++d) s.center[d] = sj.center[d];
         s.radius = sj.radius;
         s.nvertex = sj.nvertex;
-        if (s.nvertex > 0) {
+        if (s.shape == PTG_SHAPE_POLYGON && s.nvertex > 0) {
           const int n = s.nvertex;
           s.v.resize(3 * (n + 1));
           for (int i = 0; i <= n; ++i)
             for (int d = 0; d < 3; ++d) s.v[3 * i + d] = sj.v[3 * (n - i) + d];
           polygon_setup(s);
+        } else if (s.shape == PTG_SHAPE_CAPPED) {
+          s.v = sj.v;  /* the same axis: one cylinder seen from the matrix */
         }
         s.gout = sj.gin;
         if (!table_ok(m, s.mat2, s.mat1)) { *why = "transmission table index out of range"; return PTG_ERR_INVALID; }
@@ -374,6 +393,15 @@ int build_geometry(const ptg_model* m, GeomSoA* out, std::string* why) {
               double x = s.v[3 * i + ax];
               if (!(x > 0.0 && x < m->box[ax])) { *why = "a brick touches a periodic face"; return PTG_ERR_INVALID; }
             }
+          } else if (s.shape == PTG_SHAPE_CAPPED) {
+            /* extent of the capped cylinder along this axis */
+            const double a = s.v[3 + ax] - s.v[ax];
+            double l2 = 0.0;
+            for (int d = 0; d < 3; ++d) l2 += (s.v[3 + d] - s.v[d]) * (s.v[3 + d] - s.v[d]);
+            const double ca = fabs(a) / sqrt(l2);
+            const double ext = 0.5 * fabs(a) + s.radius * sqrt(std::max(0.0, 1.0 - ca * ca));
+            const double c = s.center[ax];
+            if (!(c - ext > 0.0 && c + ext < m->box[ax])) { *why = "a brick touches a periodic face"; return PTG_ERR_INVALID; }
           } else if (!(s.shape == PTG_SHAPE_CYLINDER && ax == 2)) {
             double c = s.center[ax];
             if (!(c - s.radius > 0.0 && c + s.radius < m->box[ax])) { *why = "a brick touches a periodic face"; return PTG_ERR_INVALID; }
@@ -451,8 +479,18 @@ int copy_geometry(const ptg_geometry* g, GeomSoA* out, std::string* why) {
   out->material2.assign(g->material2, g->material2 + ns);
   for (int k = 0; k < ns; ++k) {
     const int sh = out->shape[k];
-    if (sh < PTG_SHAPE_POLYGON || sh > PTG_SHAPE_CYLINDER) { *why = "unknown surface shape"; return PTG_ERR_INVALID; }
-    if (sh == PTG_SHAPE_POLYGON) {
+    if (sh < PTG_SHAPE_POLYGON || sh > PTG_SHAPE_CAPPED) { *why = "unknown surface shape"; return PTG_ERR_INVALID; }
+    if (sh == PTG_SHAPE_CAPPED) {
+      if (out->nvertex[k] != 2 || out->vertex_begin[k] < 0 || out->vertex_begin[k] + 3 > nvt ||
+          !(out->radius[k] > 0.0)) {
+        *why = "capped cylinder needs 2 axis end points and a radius > 0";
+        return PTG_ERR_INVALID;
+      }
+      const double* v = &out->vertex[3 * (size_t)out->vertex_begin[k]];
+      double l2 = 0.0;
+      for (int d = 0; d < 3; ++d) l2 += (v[3 + d] - v[d]) * (v[3 + d] - v[d]);
+      if (!(l2 > 0.0)) { *why = "capped cylinder axis must be > 0"; return PTG_ERR_INVALID; }
+    } else if (sh == PTG_SHAPE_POLYGON) {
       if (out->nvertex[k] < 3 || out->vertex_begin[k] < 0 ||
           out->vertex_begin[k] + out->nvertex[k] + 1 > nvt) {
         *why = "polygon vertex range out of bounds";

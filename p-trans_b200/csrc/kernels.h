@@ -70,7 +70,8 @@ cudaError_t launch_plain_fp64(const Geo64& g, const Run64& r, cudaStream_t st, i
 /* ---------------- persistent FP32 kernel -------------------------------- */
 
 /* Surface record types in the FP32 blob. */
-enum { REC_POLY = 1, REC_SPHERE = 2, REC_CYL = 3 };
+/* REC_CAP: capped cylinder, its (unit axis, half length) in the edge array */
+enum { REC_POLY = 1, REC_SPHERE = 2, REC_CYL = 3, REC_CAP = 4 };
 enum { REC_INTERIOR = 1 << 8 };
 
 /* Offsets (in 16-byte units) of the sections of the FP32 geometry blob. */
@@ -84,6 +85,7 @@ struct BlobLayout {
   int bvh_root;     /* int[ngrain_total]: root node of the grain's BVH, -1 linear scan */
   int bvh_node;     /* float4[2*nnode]: (lo, a) (hi, b), see bvh.cpp                  */
   int nbvh;         /* BVH nodes in the blob (0: every grain scans linearly)          */
+  int ncap;         /* capped-cylinder records in the blob                            */
   int total;        /* blob size in 16-byte units                                    */
   int nstart;
 };
@@ -97,7 +99,8 @@ struct GeoF32 {
   int periodic_mask;   /* bit f set: box face f is periodic              */
   int kind_grain, igrain_fill, nmaterial;
   int stage_smem;      /* 1: copy the blob to shared memory (bulk copy)  */
-  int has_bvh;         /* 1: some grain has a BVH (kernels built for it)  */
+  int has_ext;         /* 1: a BVH or capped cylinders (kernels built for  */
+                       /*    them; the others leave both out)             */
 };
 
 /* One geometry of a batched launch (device table, read through the cache). */

@@ -150,16 +150,89 @@ __device__ __forceinline__ bool closer(float t, int s, float tr, int sr) {
   return t < tr || (t == tr && s < sr);
 }
 
+/* Capped cylinder (centre A.xyz, radius A.w; unit axis E.xyz, half length
+   E.w) against the ray p + t d.  From inside (interior record) the exit:
+   the mantle's far root when its axial coordinate lies within the caps, or
+   the cap the ray leaves through when the crossing lies within the radius.
+   From outside the entry: the mantle's near root (approaching) within the
+   caps, or the cap facing the ray within the radius; the cylinder just left
+   is excluded, as for the other quadrics.  Tolerance eps on both limits. */
+template <class G_t>
+__device__ __forceinline__ void capped_test(const G_t& G, int s, float4 A, int4 B, float px,
+                                            float py, float pz, float dx, float dy, float dz,
+                                            int last_geom, float eps, float& tr, int& sb) {
+  const bool interior = (B.x & REC_INTERIOR) != 0;
+  if (!interior && B.w == last_geom) return;
+  const float4 E = G.edge(B.y);
+  const float wx = A.x - px, wy = A.y - py, wz = A.z - pz;   /* centre - p */
+  const float sw = fmaf(wx, E.x, fmaf(wy, E.y, wz * E.z));
+  const float s0 = -sw;                                      /* axial coordinate of p */
+  const float ds = fmaf(dx, E.x, fmaf(dy, E.y, dz * E.z));
+  const float upx = fmaf(-sw, E.x, wx), upy = fmaf(-sw, E.y, wy), upz = fmaf(-sw, E.z, wz);
+  const float vpx = fmaf(-ds, E.x, dx), vpy = fmaf(-ds, E.y, dy), vpz = fmaf(-ds, E.z, dz);
+  const float a = fmaf(vpx, vpx, fmaf(vpy, vpy, vpz * vpz));
+  const float b = fmaf(upx, vpx, fmaf(upy, vpy, upz * vpz));
+  const float c = fmaf(upx, upx, fmaf(upy, upy, upz * upz)) - A.w * A.w;
+  const float hl = E.w + eps, rr = (A.w + eps) * (A.w + eps);
+  float t = 3.0e38f;
+  /* mantle: roots of a t^2 - 2 b t + c = 0 */
+  if (a > 0.0f) {
+    const float disc = fmaf(b, b, -a * c);
+    if (disc >= 0.0f) {
+      const float sq = sqrtf(disc);
+      float tl = 3.0e38f;
+      if (interior) tl = (b >= 0.0f) ? __fdividef(b + sq, a) : __fdividef(-c, sq - b);
+      else if (b > 0.0f) tl = __fdividef(c, b + sq);
+      if (tl >= -eps && fabsf(fmaf(tl, ds, s0)) <= hl) t = tl;
+    }
+  }
+  /* caps */
+  if (ds != 0.0f) {
+    float tc;
+    if (interior) tc = __fdividef((ds > 0.0f ? E.w : -E.w) - s0, ds);
+    else if (s0 < -E.w && ds > 0.0f) tc = __fdividef(-E.w - s0, ds);
+    else if (s0 > E.w && ds < 0.0f) tc = __fdividef(E.w - s0, ds);
+    else tc = 3.0e38f;
+    if (tc >= -eps && tc < t) {
+      const float qx = fmaf(-tc, vpx, upx), qy = fmaf(-tc, vpy, upy), qz = fmaf(-tc, vpz, upz);
+      if (fmaf(qx, qx, fmaf(qy, qy, qz * qz)) <= rr) t = tc;
+    }
+  }
+  if (!(t < 3.0e38f) || !closer(t, s, tr, sb)) return;
+  tr = t;
+  sb = s;
+}
+
+/* Outward normal of the capped-cylinder piece nearer to p: a cap (+-axis)
+   when the axial distance to it is the smaller, else the mantle's radial
+   direction. */
+__device__ __forceinline__ void capped_normal(float4 A, float4 E, float px, float py, float pz,
+                                              float& nx, float& ny, float& nz) {
+  const float wx = px - A.x, wy = py - A.y, wz = pz - A.z;
+  const float sa = fmaf(wx, E.x, fmaf(wy, E.y, wz * E.z));
+  const float ux = fmaf(-sa, E.x, wx), uy = fmaf(-sa, E.y, wy), uz = fmaf(-sa, E.z, wz);
+  const float rho = sqrtf(fmaf(ux, ux, fmaf(uy, uy, uz * uz)));
+  if (fabsf(fabsf(sa) - E.w) < fabsf(rho - A.w)) {
+    const float sg = sa < 0.0f ? -1.0f : 1.0f;
+    nx = sg * E.x; ny = sg * E.y; nz = sg * E.z;
+  } else {
+    const float inv = __frcp_rn(rho);
+    nx = ux * inv; ny = uy * inv; nz = uz * inv;
+  }
+}
+
 /* One candidate surface against the ray p + t d: updates the nearest raw
    distance tr and surface sb. */
-template <class G_t>
+template <bool EXT, class G_t>
 __device__ __forceinline__ void test_surface(const G_t& G, int s, float px, float py, float pz,
                                              float dx, float dy, float dz, int last_geom,
                                              float eps, float zmax, float& tr, int& sb) {
   const float4 A = G.hotA(s);
   const int4 B = G.hotB(s);
   const int type = B.x & 0xff;
-  if (type == REC_POLY) {
+  if (EXT && type == REC_CAP) {
+    capped_test(G, s, A, B, px, py, pz, dx, dy, dz, last_geom, eps, tr, sb);
+  } else if (type == REC_POLY) {
     const float cosa = fmaf(A.x, dx, fmaf(A.y, dy, A.z * dz));
     if (cosa <= 0.0f) return;
     const float t = __fdividef(A.w - fmaf(A.x, px, fmaf(A.y, py, A.z * pz)), cosa);
@@ -232,7 +305,7 @@ constexpr int kBvhStack = 32;
    pushed with its entry distance and popped only while it can still hold a
    nearer hit.  Kept out of line so the linear scan that every small grain
    uses stays compact in the instruction cache. */
-template <class G_t>
+template <bool EXT, class G_t>
 __device__ __noinline__ void scan_bvh(const G_t& G, int root, float px, float py, float pz,
                                       float dx, float dy, float dz, int last_geom, float eps,
                                       float zmax, float& tr, int& sb, unsigned& nbox,
@@ -250,7 +323,7 @@ __device__ __noinline__ void scan_bvh(const G_t& G, int root, float px, float py
     if (cnt > 0) {
       nsurf += (unsigned)cnt;
       for (int k = a; k < a + cnt; ++k)
-        test_surface(G, G.cand(k), px, py, pz, dx, dy, dz, last_geom, eps, zmax, tr, sb);
+        test_surface<EXT>(G, G.cand(k), px, py, pz, dx, dy, dz, last_geom, eps, zmax, tr, sb);
     } else {
       nbox += 2u;
       const float tl = box_entry(G.node(2 * a), G.node(2 * a + 1), px, py, pz, ix, iy, iz, tr, eps);
@@ -286,22 +359,23 @@ __device__ __noinline__ void scan_bvh(const G_t& G, int root, float px, float py
 }
 
 /* Nearest surface of a grain: its BVH when it has one (kernels built with
-   BVH = true; the others never look for one), else every candidate.  tb
+   EXT = true, for structures with a BVH or capped cylinders; the others
+   never look for either), else every candidate.  tb
    (the box-grain exit, >= 0) and sb are updated; tb stays >= 0. */
-template <bool BVH, class G_t>
+template <bool EXT, class G_t>
 __device__ __forceinline__ void scan_grain(const G_t& G, int grain, float px, float py, float pz,
                                            float dx, float dy, float dz, int last_geom, float eps,
                                            float zmax, float& tb, int& sb, unsigned& nbox,
                                            unsigned& nsurf) {
   float tr = tb;
-  const int root = BVH ? G.bvh_root(grain) : -1;
+  const int root = EXT ? G.bvh_root(grain) : -1;
   if (root < 0) {
     const int kb = G.cand_begin(grain), ke = G.cand_begin(grain + 1);
     nsurf += (unsigned)(ke - kb);
     for (int k = kb; k < ke; ++k)
-      test_surface(G, G.cand(k), px, py, pz, dx, dy, dz, last_geom, eps, zmax, tr, sb);
+      test_surface<EXT>(G, G.cand(k), px, py, pz, dx, dy, dz, last_geom, eps, zmax, tr, sb);
   } else {
-    scan_bvh(G, root, px, py, pz, dx, dy, dz, last_geom, eps, zmax, tr, sb, nbox, nsurf);
+    scan_bvh<EXT>(G, root, px, py, pz, dx, dy, dz, last_geom, eps, zmax, tr, sb, nbox, nsurf);
   }
   tb = fmaxf(tr, 0.0f);
 }
@@ -328,11 +402,22 @@ __device__ __forceinline__ void slab_exit(float px, float py, float pz, float dx
 
 /* Lower bound of the distance from p to one candidate surface (planes bound
    polygons from below, the infinite cylinder bounds the clipped one). */
-template <class G_t>
+template <bool EXT, class G_t>
 __device__ __forceinline__ float surface_lb(const G_t& G, int s, float px, float py, float pz) {
   const float4 A = G.hotA(s);
-  const int type = G.hotB(s).x & 0xff;
+  const int4 B = G.hotB(s);
+  const int type = B.x & 0xff;
   if (type == REC_POLY) return fabsf(A.w - fmaf(A.x, px, fmaf(A.y, py, A.z * pz)));
+  if (EXT && type == REC_CAP) {
+    /* inside: the nearer of mantle and caps; outside: the larger excess */
+    const float4 E = G.edge(B.y);
+    const float wx = px - A.x, wy = py - A.y, wz = pz - A.z;
+    const float sa = fmaf(wx, E.x, fmaf(wy, E.y, wz * E.z));
+    const float ux = fmaf(-sa, E.x, wx), uy = fmaf(-sa, E.y, wy), uz = fmaf(-sa, E.z, wz);
+    const float er = sqrtf(fmaf(ux, ux, fmaf(uy, uy, uz * uz))) - A.w;
+    const float ea = fabsf(sa) - E.w;
+    return (er <= 0.0f && ea <= 0.0f) ? fminf(-er, -ea) : fmaxf(er, ea);
+  }
   if (type == REC_SPHERE) {
     const float wx = px - A.x, wy = py - A.y, wz = pz - A.z;
     return fabsf(sqrtf(fmaf(wx, wx, fmaf(wy, wy, wz * wz))) - A.w);
@@ -354,7 +439,7 @@ __device__ __forceinline__ float box_dist(float4 lo, float4 hi, float px, float 
    farther than the bound so far are pruned; a leaf contributes
    max(distance to its box, nearest plane / quadric bound of its surfaces)).
    Out of line, like scan_bvh. */
-template <class G_t>
+template <bool EXT, class G_t>
 __device__ __noinline__ float safety_bvh(const G_t& G, int root, float px, float py, float pz,
                                          float d) {
   int stk[kBvhStack];
@@ -368,7 +453,7 @@ __device__ __noinline__ float safety_bvh(const G_t& G, int root, float px, float
     bool descended = false;
     if (cnt > 0) {
       float e = 3.0e38f;
-      for (int k = a; k < a + cnt; ++k) e = fminf(e, surface_lb(G, G.cand(k), px, py, pz));
+      for (int k = a; k < a + cnt; ++k) e = fminf(e, surface_lb<EXT>(G, G.cand(k), px, py, pz));
       d = fminf(d, fmaxf(box_dist(n0, n1, px, py, pz), e));
     } else {
       const float dl = box_dist(G.node(2 * a), G.node(2 * a + 1), px, py, pz);
@@ -403,17 +488,17 @@ __device__ __noinline__ float safety_bvh(const G_t& G, int root, float px, float
 /* Lower bound of the distance from p to every box face and to every
    candidate surface of the grain, less 4 eps.  A grain with a BVH is
    searched only within `cap` (the radius the safe ball needs). */
-template <bool BVH, class G_t>
+template <bool EXT, class G_t>
 __device__ __forceinline__ float safety(const G_t& G, int grain, float px, float py, float pz,
                                         float X, float Y, float Z, float eps, float cap) {
   float d = fminf(fminf(fminf(px, X - px), fminf(py, Y - py)), fminf(pz, Z - pz));
   if (grain > 0) {
-    const int root = BVH ? G.bvh_root(grain) : -1;
+    const int root = EXT ? G.bvh_root(grain) : -1;
     if (root < 0) {
       const int kb = G.cand_begin(grain), ke = G.cand_begin(grain + 1);
-      for (int k = kb; k < ke; ++k) d = fminf(d, surface_lb(G, G.cand(k), px, py, pz));
+      for (int k = kb; k < ke; ++k) d = fminf(d, surface_lb<EXT>(G, G.cand(k), px, py, pz));
     } else {
-      d = safety_bvh(G, root, px, py, pz, fminf(d, cap));
+      d = safety_bvh<EXT>(G, root, px, py, pz, fminf(d, cap));
     }
   }
   return d - 4.0f * eps;
@@ -502,7 +587,7 @@ constexpr int kCoopRoundsBusy = 4;
    walk needs about (radius / MFP)^2 flights to leave the ball */
 constexpr float kBallCapMfp = 32.0f;
 
-template <bool SMEM, int MODE, bool BATCH, bool BVH>
+template <bool SMEM, int MODE, bool BATCH, bool EXT>
 __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   typename std::conditional<BATCH, GeoBatch, Geo<SMEM>>::type G;
   G.lay = gp.lay;
@@ -768,7 +853,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             if (!in_ball) {
               slab_exit(qx, qy, qz, sdx, sdy, sdz, X, Y, Z, tb, sb);
               if (cgrain > 0)
-                scan_grain<BVH>(G, cgrain, qx, qy, qz, sdx, sdy, sdz, lane == 0 ? clast : -1, eps,
+                scan_grain<EXT>(G, cgrain, qx, qy, qz, sdx, sdy, sdz, lane == 0 ? clast : -1, eps,
                                 Z, tb, sb, my_box_tests, my_surf_tests);
             }
             const bool brk = !inbox || capd;
@@ -806,7 +891,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             cfl += 32u;
             /* a new ball where the walk left the old one */
             if (!__shfl_sync(FULL, in_ball, 31) && r.fast_steps > 0) {
-              const float d = safety<BVH>(G, cgrain, cpx, cpy, cpz, X, Y, Z, eps, kBallCapMfp * clam);
+              const float d = safety<EXT>(G, cgrain, cpx, cpy, cpz, X, Y, Z, eps, kBallCapMfp * clam);
               cbx = cpx; cby = cpy; cbz = cpz;
               cbr2 = d > 0.0f ? d * d : 0.0f;
             }
@@ -907,7 +992,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           R = philox10(flight, c1, slo, shi, key);
           slab_exit(px, py, pz, dx, dy, dz, X, Y, Z, tb, sb);
           if (grain > 0)
-            scan_grain<BVH>(G, grain, px, py, pz, dx, dy, dz, last_geom, eps, Z, tb, sb, my_box_tests,
+            scan_grain<EXT>(G, grain, px, py, pz, dx, dy, dz, last_geom, eps, Z, tb, sb, my_box_tests,
                        my_surf_tests);
           go = true;
         }
@@ -933,7 +1018,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             last_geom = -1;
             br2 = 0.0f;
             if (MODE != MODE_TRACE && r.fast_steps > 0 && lam < flmax) {
-              const float d = safety<BVH>(G, grain, px, py, pz, X, Y, Z, eps, kBallCapMfp * lam);
+              const float d = safety<EXT>(G, grain, px, py, pz, X, Y, Z, eps, kBallCapMfp * lam);
               ++my_balls;
               if (d > 0.0f) { bx = px; by = py; bz = pz; br2 = d * d; }
             }
@@ -982,9 +1067,13 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
                 ax2 = C1.x; ay2 = C1.y; az2 = C1.z;
               } else {
                 const float4 A = G.hotA(sb);
-                float rx = px - A.x, ry = py - A.y, rz = (type == REC_SPHERE) ? pz - A.z : 0.0f;
-                const float inv = rsqrtf(fmaf(rx, rx, fmaf(ry, ry, rz * rz)));
-                nx = rx * inv; ny = ry * inv; nz = rz * inv;
+                if (EXT && type == REC_CAP) {
+                  capped_normal(A, G.edge(B.y), px, py, pz, nx, ny, nz);
+                } else {
+                  float rx = px - A.x, ry = py - A.y, rz = (type == REC_SPHERE) ? pz - A.z : 0.0f;
+                  const float inv = rsqrtf(fmaf(rx, rx, fmaf(ry, ry, rz * rz)));
+                  nx = rx * inv; ny = ry * inv; nz = rz * inv;
+                }
                 const float q2 = fmaf(nx, nx, ny * ny);
                 if (q2 > 1.0e-12f) {
                   const float q = rsqrtf(q2);
@@ -1139,27 +1228,27 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
 
 }  // namespace
 
-template <int MODE, bool BVH>
+template <int MODE, bool EXT>
 cudaError_t occupancy_mode(int block, size_t smem, int* bps) {
   if (smem > 0)
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_persistent<true, MODE, false, BVH>,
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_persistent<true, MODE, false, EXT>,
                                                          block, smem);
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_persistent<false, MODE, false, BVH>,
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_persistent<false, MODE, false, EXT>,
                                                        block, 0);
 }
 
-template <int MODE, bool BVH>
+template <int MODE, bool EXT>
 cudaError_t launch_mode(const GeoF32& g, const RunF32& r, int grid, int block, size_t smem,
                         cudaStream_t st) {
   if (g.stage_smem && smem > 0) {
     if (smem > 48 * 1024) {
-      cudaError_t e = cudaFuncSetAttribute(k_persistent<true, MODE, false, BVH>,
+      cudaError_t e = cudaFuncSetAttribute(k_persistent<true, MODE, false, EXT>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (e != cudaSuccess) return e;
     }
-    k_persistent<true, MODE, false, BVH><<<grid, block, smem, st>>>(g, r);
+    k_persistent<true, MODE, false, EXT><<<grid, block, smem, st>>>(g, r);
   } else {
-    k_persistent<false, MODE, false, BVH><<<grid, block, 0, st>>>(g, r);
+    k_persistent<false, MODE, false, EXT><<<grid, block, 0, st>>>(g, r);
   }
   return cudaGetLastError();
 }
@@ -1179,31 +1268,31 @@ cudaError_t launch_persistent_batch(const RunF32& r, int grid, int block, cudaSt
   return cudaGetLastError();
 }
 
-template <bool BVH>
+template <bool EXT>
 cudaError_t occupancy_bvh(int block, size_t smem, int* bps, int mode) {
-  if (mode == MODE_LIST) return occupancy_mode<MODE_LIST, BVH>(block, smem, bps);
-  if (mode == MODE_ADJOINT) return occupancy_mode<MODE_ADJOINT, BVH>(block, smem, bps);
-  if (mode == MODE_TRACE) return occupancy_mode<MODE_TRACE, BVH>(block, smem, bps);
-  return occupancy_mode<MODE_FORWARD, BVH>(block, smem, bps);
+  if (mode == MODE_LIST) return occupancy_mode<MODE_LIST, EXT>(block, smem, bps);
+  if (mode == MODE_ADJOINT) return occupancy_mode<MODE_ADJOINT, EXT>(block, smem, bps);
+  if (mode == MODE_TRACE) return occupancy_mode<MODE_TRACE, EXT>(block, smem, bps);
+  return occupancy_mode<MODE_FORWARD, EXT>(block, smem, bps);
 }
 
 cudaError_t persistent_occupancy(int block, size_t smem, int* bps, int mode, bool bvh) {
   return bvh ? occupancy_bvh<true>(block, smem, bps, mode) : occupancy_bvh<false>(block, smem, bps, mode);
 }
 
-template <bool BVH>
+template <bool EXT>
 cudaError_t launch_bvh(const GeoF32& g, const RunF32& r, int grid, int block, size_t smem,
                        cudaStream_t st, int mode) {
-  if (mode == MODE_LIST) return launch_mode<MODE_LIST, BVH>(g, r, grid, block, smem, st);
-  if (mode == MODE_ADJOINT) return launch_mode<MODE_ADJOINT, BVH>(g, r, grid, block, smem, st);
-  if (mode == MODE_TRACE) return launch_mode<MODE_TRACE, BVH>(g, r, grid, block, smem, st);
-  return launch_mode<MODE_FORWARD, BVH>(g, r, grid, block, smem, st);
+  if (mode == MODE_LIST) return launch_mode<MODE_LIST, EXT>(g, r, grid, block, smem, st);
+  if (mode == MODE_ADJOINT) return launch_mode<MODE_ADJOINT, EXT>(g, r, grid, block, smem, st);
+  if (mode == MODE_TRACE) return launch_mode<MODE_TRACE, EXT>(g, r, grid, block, smem, st);
+  return launch_mode<MODE_FORWARD, EXT>(g, r, grid, block, smem, st);
 }
 
 cudaError_t launch_persistent_fp32(const GeoF32& g, const RunF32& r, int grid, int block,
                                    size_t smem, cudaStream_t st, int mode) {
   if (block > kBlock || block % 32) return cudaErrorInvalidConfiguration;
-  return g.has_bvh ? launch_bvh<true>(g, r, grid, block, smem, st, mode)
+  return g.has_ext ? launch_bvh<true>(g, r, grid, block, smem, st, mode)
                    : launch_bvh<false>(g, r, grid, block, smem, st, mode);
 }
 

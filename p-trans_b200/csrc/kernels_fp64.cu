@@ -60,6 +60,79 @@ __device__ bool in_polygon(const double* v, int n, const double* Rh) {
   return true;
 }
 
+/* Capped cylinder (extension): unit axis and half length from the axis end
+   points A = vertex 0, B = vertex 1. */
+__device__ void capped_axis(const Geo64& g, int k, double* a, double* hl) {
+  const double* v = g.vertex + 3 * (size_t)g.vbegin[k];
+  double e[3] = {v[3] - v[0], v[4] - v[1], v[5] - v[2]};
+  const double len = sqrt(dot3(e, e));
+  for (int d = 0; d < 3; ++d) a[d] = e[d] / len;
+  *hl = 0.5 * len;
+}
+
+/* Nearest strictly positive hit of the lateral surface (within the caps)
+   and the two cap discs (within the radius). */
+__device__ bool capped_distance(const Geo64& g, int k, const double* R0, const double* D,
+                                double* L) {
+  double a[3], hl;
+  capped_axis(g, k, a, &hl);
+  const double* C = g.center + 3 * k;
+  double w[3] = {R0[0] - C[0], R0[1] - C[1], R0[2] - C[2]};
+  const double s0 = dot3(w, a), ds = dot3(D, a);
+  double wp[3], dp[3];
+  for (int d = 0; d < 3; ++d) {
+    wp[d] = w[d] - s0 * a[d];
+    dp[d] = D[d] - ds * a[d];
+  }
+  const double r2 = g.radius[k] * g.radius[k];
+  double best = 0.0;
+  bool hit = false;
+  const double A2 = dot3(dp, dp);
+  if (A2 > 0.0) {
+    const double B = dot3(wp, dp), Cc = dot3(wp, wp) - r2;
+    const double disc = B * B - A2 * Cc;
+    if (disc >= 0.0) {
+      const double sq = sqrt(disc);
+      const double t[2] = {(-B - sq) / A2, (-B + sq) / A2};
+      for (int i = 0; i < 2; ++i) {
+        if (!(t[i] > 0.0) || (hit && !(t[i] < best))) continue;
+        if (fabs(s0 + t[i] * ds) <= hl) { best = t[i]; hit = true; }
+      }
+    }
+  }
+  if (ds != 0.0) {
+    for (int i = 0; i < 2; ++i) {
+      const double c = (i == 0) ? -hl : hl;
+      const double t = (c - s0) / ds;
+      if (!(t > 0.0) || (hit && !(t < best))) continue;
+      double q[3];
+      for (int d = 0; d < 3; ++d) q[d] = wp[d] + t * dp[d];
+      if (dot3(q, q) <= r2) { best = t; hit = true; }
+    }
+  }
+  if (!hit) return false;
+  *L = best;
+  return true;
+}
+
+/* Outward normal of the nearer piece: cap (+-axis) or mantle (radial). */
+__device__ void capped_normal(const Geo64& g, int k, const double* R, double* N) {
+  double a[3], hl;
+  capped_axis(g, k, a, &hl);
+  const double* C = g.center + 3 * k;
+  double w[3] = {R[0] - C[0], R[1] - C[1], R[2] - C[2]};
+  const double sa = dot3(w, a);
+  double wp[3];
+  for (int d = 0; d < 3; ++d) wp[d] = w[d] - sa * a[d];
+  const double rho = sqrt(dot3(wp, wp));
+  if (fabs(fabs(sa) - hl) < fabs(rho - g.radius[k])) {
+    const double sg = (sa < 0.0) ? -1.0 : 1.0;
+    for (int d = 0; d < 3; ++d) N[d] = sg * a[d];
+  } else {
+    for (int d = 0; d < 3; ++d) N[d] = wp[d] / rho;
+  }
+}
+
 /* calcSurfaceDistance dispatch, src/RTMCphon.f90:2883-3088 */
 __device__ bool surface_distance(const Geo64& g, int k, const double* R0, const double* D,
                                  double* L) {
@@ -78,6 +151,7 @@ __device__ bool surface_distance(const Geo64& g, int k, const double* R0, const 
     *L = Lh;
     return true;
   }
+  if (sh == 4) return capped_distance(g, k, R0, D, L);
   const double* C = g.center + 3 * k;
   const double r = g.radius[k];
   const double r2 = r * r;
@@ -128,6 +202,10 @@ __device__ void surface_normal(const Geo64& g, int k, const double* R, double* N
     N[0] = g.normal[3 * k]; N[1] = g.normal[3 * k + 1]; N[2] = g.normal[3 * k + 2];
     return;
   }
+  if (sh == 4) {
+    capped_normal(g, k, R, N);
+    return;
+  }
   const double* C = g.center + 3 * k;
   double Rcs[3];
   if (sh == 2) {
@@ -151,7 +229,9 @@ __device__ void surface_rotation(const Geo64& g, int k, const double* R, double*
   }
   const double* C = g.center + 3 * k;
   double n[3];
-  if (sh == 2) {
+  if (sh == 4) {
+    capped_normal(g, k, R, n);
+  } else if (sh == 2) {
     double Rcs[3] = {R[0] - C[0], R[1] - C[1], R[2] - C[2]};
     const double inv = 1.0 / sqrt(dot3(Rcs, Rcs));
     for (int d = 0; d < 3; ++d) n[d] = Rcs[d] * inv;
@@ -161,7 +241,7 @@ __device__ void surface_rotation(const Geo64& g, int k, const double* R, double*
     for (int d = 0; d < 3; ++d) n[d] = Nn[d] * inv;
   }
   Rm[6] = n[0]; Rm[7] = n[1]; Rm[8] = n[2];
-  const double pole = (sh == 2) ? fabs(n[2]) : fabs(n[0]);
+  const double pole = (sh == 3) ? fabs(n[0]) : fabs(n[2]);
   if (pole == 1.0 || (n[0] * n[0] == 0.0 && n[1] * n[1] == 0.0)) {
     Rm[3] = 0; Rm[4] = 1; Rm[5] = 0; Rm[0] = 1; Rm[1] = 0; Rm[2] = 0;
   } else {

@@ -173,7 +173,7 @@ extern "C" int ptg_transmission_noalloc(ptg_handle* h, double mfp_nm, int32_t na
   const int block = 256;
   const size_t smem = v.g32.stage_smem ? v.blob_bytes : 0;
   int bps = 0;
-  if (ptg::persistent_occupancy(block, smem, &bps, ptg::MODE_FORWARD, v.g32.has_bvh != 0) !=
+  if (ptg::persistent_occupancy(block, smem, &bps, ptg::MODE_FORWARD, v.g32.has_ext != 0) !=
       cudaSuccess)
     return PTG_ERR_CUDA;
   if (v.opt.blocks_per_sm > 0 && v.opt.blocks_per_sm < bps) bps = v.opt.blocks_per_sm;

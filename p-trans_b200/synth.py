@@ -22,7 +22,7 @@ from typing import Optional
 
 import numpy as np
 
-from .abi import (FACE_PERIODIC, GRAIN_BRICKS, GRAIN_VORONOI, MATERIAL_BOUNDARY, MATERIAL_INTERNAL,
+from .abi import (FACE_PERIODIC, GRAIN_BRICKS, GRAIN_VORONOI, MATERIAL_BOUNDARY, MATERIAL_INTERNAL, SHAPE_CAPPED,
                   SHAPE_CYLINDER, SHAPE_POLYGON, SHAPE_SPHERE, TRANS_VALUE, Model, Spectrum)
 
 THZ = 2.0 * math.pi * 1.0e12
@@ -400,3 +400,63 @@ def cube_lattice(n: int = 16, l: float = 1000.0, fill: float = 0.5, trans: float
         facet_vertex=np.array([v for f in faces_all for v in f], np.float64).ravel(),
         surf_material_to=[MATERIAL_INTERNAL] * len(faces_all), surf_grain_to=[0] * len(faces_all),
         cellspec=(1.0, 1.0, p_wall, p_wall, p_wall, p_wall), tt_kind=kind, tt_trans=tt, tt_spec=ts)
+
+
+def spheres_cylinders_box(n_spheres: int = 64, n_cylinders: int = 16, l: float = 1000.0, seed: int = 0,
+                          r_sphere=(20.0, 80.0), r_cylinder: float = 30.0, length=(100.0, 400.0),
+                          trans: float = 0.0, p_wall: float = 0.0, per_surface_p: bool = True,
+                          gap: float = 2.0) -> Model:
+    """Spheres (radius ~ U(r_sphere)) and capped cylinders of random axis
+    (radius r_cylinder, length ~ U(length)) in an l^3 box, placed by
+    rejection so that no two objects' bounding spheres come closer than gap
+    and every object stays inside the box.  Inclusions transmit with
+    `trans`; with per_surface_p every surface gets its own specularity
+    p ~ U(0, 1) (the model's per-surface override), else p = 0."""
+    rng = np.random.default_rng(seed)
+    placed = []   # (centre, bounding radius)
+    shapes, gens, diam, axes = [], [], [], []
+
+    def fits(c, rb, ext):
+        if np.any(c - ext <= gap) or np.any(c + ext >= l - gap):
+            return False
+        return all(np.linalg.norm(c - q) > rb + rq + gap for q, rq in placed)
+
+    for _ in range(n_cylinders):
+        for _attempt in range(100000):
+            u = rng.normal(size=3)
+            a = u / np.linalg.norm(u)
+            ln = rng.uniform(*length)
+            c = rng.uniform(0.0, l, 3)
+            ext = 0.5 * ln * np.abs(a) + r_cylinder * np.sqrt(np.maximum(0.0, 1.0 - a * a))
+            rb = math.hypot(r_cylinder, 0.5 * ln)
+            if fits(c, rb, ext):
+                placed.append((c, rb))
+                shapes.append(SHAPE_CAPPED)
+                gens.append(c)
+                diam.append(2.0 * r_cylinder)
+                axes.append(a * ln)
+                break
+        else:
+            raise RuntimeError("could not place a cylinder")
+    for _ in range(n_spheres):
+        for _attempt in range(100000):
+            r = rng.uniform(*r_sphere)
+            c = rng.uniform(0.0, l, 3)
+            if fits(c, r, np.full(3, r)):
+                placed.append((c, r))
+                shapes.append(SHAPE_SPHERE)
+                gens.append(c)
+                diam.append(2.0 * r)
+                axes.append(np.zeros(3))
+                break
+        else:
+            raise RuntimeError("could not place a sphere")
+    n = len(shapes)
+    kind, tt, ts = _table(trans, 0.0)
+    spec = rng.uniform(0.0, 1.0, n) if per_surface_p else None
+    return Model(
+        box=(l, l, l), kind_grain=GRAIN_BRICKS, grain_shape=shapes, grain_generatrix=np.array(gens).ravel(),
+        grain_diameter=diam, grain_material=[1] * n, grain_nfacet=[1] * n, facet_nvertex=[], facet_vertex=[],
+        surf_material_to=[MATERIAL_INTERNAL] * n, surf_grain_to=[0] * n,
+        cellspec=(1.0, 1.0, p_wall, p_wall, p_wall, p_wall), tt_kind=kind, tt_trans=tt, tt_spec=ts,
+        surf_spec=spec, grain_axis=np.array(axes).ravel())

@@ -31,6 +31,9 @@ def geometries():
         "lattice_tris": synth.cube_lattice(n=3, l=300.0, fill=0.5, trans=0.3, spec=0.2, p_wall=0.3),
         "voronoi": synth.voronoi_box(6, box=(300.0, 200.0, 200.0), seed=4, trans=0.5, spec=0.1,
                                      p_wall=0.2),
+        "capped": synth.spheres_cylinders_box(n_spheres=4, n_cylinders=5, l=300.0, seed=3,
+                                              r_sphere=(15.0, 35.0), r_cylinder=20.0, length=(50.0, 150.0),
+                                              trans=0.3, p_wall=0.2),
     }
 
 
@@ -182,7 +185,7 @@ def test_rank_partition_is_exact_fp32():
 
 
 @pytest.mark.parametrize("name", ["film_periodic", "film_mirror_transmit", "spheres", "brick_tris",
-                                  "nanowire_mixed"])
+                                  "nanowire_mixed", "capped"])
 @pytest.mark.parametrize("cap", [0, 40])
 def test_cooperative_tail_takes_the_same_trajectories(name, cap):
     """Warp-cooperative rounds (every warp with coop_lanes = 32; only phonons
@@ -228,7 +231,7 @@ def _many_spheres(n=40, l=400.0, seed=0):
     return synth.spheres_in_box(l=l, centres=[tuple(x) for x in c], radii=r, t=0.4, p=0.3, p_wall=0.2)
 
 
-@pytest.mark.parametrize("name", ["lattice", "spheres", "holes"])
+@pytest.mark.parametrize("name", ["lattice", "spheres", "holes", "capped"])
 def test_bvh_and_linear_scan_take_the_same_trajectories(name):
     """A grain with more than 32 candidates gets a BVH; its nearest hit is the
     linear scan's (nearest raw distance, ties to the lower surface index) and
@@ -238,7 +241,10 @@ def test_bvh_and_linear_scan_take_the_same_trajectories(name):
     m = {"lattice": lambda: synth.cube_lattice(n=4, l=400.0, fill=0.5, trans=0.3, spec=0.2, p_wall=0.3),
          "spheres": _many_spheres,
          "holes": lambda: synth.film_with_holes(lx=600.0, ly=600.0, lz=100.0, nholes=40, radius=20.0,
-                                                seed=5, p_hole=0.3, t_hole=0.2)}[name]()
+                                                seed=5, p_hole=0.3, t_hole=0.2),
+         "capped": lambda: synth.spheres_cylinders_box(n_spheres=12, n_cylinders=30, l=600.0, seed=6,
+                                                       r_sphere=(10.0, 30.0), r_cylinder=15.0,
+                                                       length=(40.0, 120.0), trans=0.3, p_wall=0.2)}[name]()
     spec = synth.spectrum(10, seed=7, mfp_lo=2e-9, mfp_hi=1e-6)
     gb = A.GeomBuf(m)
     run = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=5, np_=203, seed=3, precision=A.PREC_FP32)

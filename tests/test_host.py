@@ -50,6 +50,9 @@ def models():
         "fluct": _with(synth.brick_box(t=0.5, p=0.5), specfluc=0.2, fluct_seed=77),
         "voronoi": synth.voronoi_box(7, box=(300.0, 200.0, 250.0), seed=2, trans=0.5, spec=0.2),
         "lattice": synth.cube_lattice(n=3, l=300.0, fill=0.4, trans=0.2, spec=0.1),
+        "capped": synth.spheres_cylinders_box(n_spheres=5, n_cylinders=6, l=400.0, seed=2,
+                                              r_sphere=(15.0, 40.0), r_cylinder=20.0, length=(60.0, 200.0),
+                                              trans=0.3),
     }
 
 
