@@ -607,6 +607,9 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   float flmax = r.fast_lambda_max;
   /* adjoint replay: per-block accumulators */
   __shared__ double adj_sh[MODE == MODE_ADJOINT ? kAdjSmemDoubles : 1];
+  /* cooperative rounds: one row of 32 (free path, direction) per warp */
+  __shared__ float4 coop_rows[(BATCH || MODE == MODE_TRACE) ? 1 : kBlock / 32][32];
+  float4* const wrow = coop_rows[(BATCH || MODE == MODE_TRACE) ? 0 : (threadIdx.x >> 5)];
   const int adj_stride = r.nsurf + 1;
   const bool adj_in_smem = (MODE == MODE_ADJOINT) && kAdjBatches * adj_stride <= kAdjSmemDoubles;
   if (MODE == MODE_ADJOINT && adj_in_smem) {
@@ -820,23 +823,26 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             sincos2pi(u23f(R.y), &sp, &cp);
             const float nx = ct, ny = st * cp, nz = st * sp;
             const float nf = -clam * __logf(u23f(R.z));
-            /* flight `lane` starts with the state the previous flight drew */
-            float sdx = __shfl_up_sync(FULL, nx, 1), sdy = __shfl_up_sync(FULL, ny, 1);
-            float sdz = __shfl_up_sync(FULL, nz, 1), sfp = __shfl_up_sync(FULL, nf, 1);
-            if (lane == 0) { sdx = cdx; sdy = cdy; sdz = cdz; sfp = cfp; }
+            /* flight `lane` starts with the state the previous flight drew:
+               the warp's row of shared memory holds (free path, direction)
+               of every flight of the round, so the start points are summed
+               from broadcast loads issued ahead of the fma chain */
+            if (lane < 31) wrow[lane + 1] = make_float4(nf, nx, ny, nz);
+            if (lane == 0) wrow[0] = make_float4(cfp, cdx, cdy, cdz);
+            __syncwarp();
+            const float4 mine = wrow[lane];
+            const float sfp = mine.x, sdx = mine.y, sdy = mine.z, sdz = mine.w;
             float qx = cpx, qy = cpy, qz = cpz;
 #pragma unroll
             for (int i = 0; i < 31; ++i) {
-              const float a = __shfl_sync(FULL, sfp, i);
-              const float ex = __shfl_sync(FULL, sdx, i);
-              const float ey = __shfl_sync(FULL, sdy, i);
-              const float ez = __shfl_sync(FULL, sdz, i);
+              const float4 v = wrow[i];
               if (i < lane) {
-                qx = fmaf(a, ex, qx);
-                qy = fmaf(a, ey, qy);
-                qz = fmaf(a, ez, qz);
+                qx = fmaf(v.x, v.y, qx);
+                qy = fmaf(v.x, v.z, qy);
+                qz = fmaf(v.x, v.w, qz);
               }
             }
+            __syncwarp();  /* the next round rewrites the row */
             const bool inbox = qx >= -eps && qx <= X + eps && qy >= -eps && qy <= Y + eps &&
                                qz >= -eps && qz <= Z + eps;
             const bool capd = (unsigned long long)cfl + (unsigned)lane >= r.max_flights;
