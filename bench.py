@@ -54,11 +54,11 @@ def load_pkg():
     return mod
 
 
-def workload(pkg, n_modes=2000, np_per_task=500):
+def workload(pkg, n_modes=2000, np_per_task=500, mfp_lo=1e-9):
     A, synth = pkg.abi, pkg.synth
     model = synth.film_with_holes(lx=300.0, ly=300.0, lz=145.0, nholes=3, radius=50.0, seed=0,
                                   periodic_y=True, p_hole=0.0, t_hole=0.0, p_z=0.0)
-    spec = synth.spectrum(n_modes, seed=0)
+    spec = synth.spectrum(n_modes, seed=0, mfp_lo=mfp_lo)
     cfg = {"workload": "thin film 300x300x145 nm, 3 z-holes r=50 nm (voids, diffuse), y periodic, "
                        "z diffuse; 2000-mode Si-like spectrum, 64 bins; per-mode MFP runs",
            "modes": n_modes, "bins": 64, "nangle": 11, "particles_per_task": np_per_task,
@@ -396,6 +396,9 @@ def main():
     ap.add_argument("--np", type=int, default=500, help="particles per (mode, angle) per GPU")
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--mfp-lo", type=float, default=1e-9,
+                    help="smallest bulk MFP of the spectrum [m]; 1e-9 is the metric's spectrum "
+                         "(larger values remove the diffusive tail, for throughput diagnostics)")
     ap.add_argument("--workload", default="thinfilm", choices=["thinfilm", "c3", "c5", "voronoi", "mesh"],
                     help="thinfilm: the metric's configuration; c3: spheres + capped cylinders with "
                          "the adjoint; c5: 256-film batched screening; voronoi / mesh: the C4 structures")
@@ -424,7 +427,9 @@ def main():
 
     pkg = load_pkg()
     A = pkg.abi
-    model, spec, cfg = workload(pkg, np_per_task=args.np)
+    model, spec, cfg = workload(pkg, np_per_task=args.np, mfp_lo=args.mfp_lo)
+    if args.mfp_lo != 1e-9:
+        cfg["workload"] += f"; bulk MFPs from {args.mfp_lo:g} m (diagnostic, not the metric's spectrum)"
     gb = A.GeomBuf(model)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
 
