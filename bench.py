@@ -531,6 +531,12 @@ def main():
             "flights_per_step": per_launch_flights,
             "tail": {"max_trajectory_flights": st["max_traj_flights"], "queue_drain_ms": st["drain_ms"],
                      "tail_ms": st["tail_ms"]},
+            # how the flights were taken: with the full intersection test by
+            # one lane, as p-p flights of cooperative rounds, or the rest (the
+            # safe-ball fast path and the hit that ends a cooperative round)
+            "paths": {"full_test": st["full_flights"], "cooperative": st["coop_flights"],
+                      "fast_or_round_end": st["flights"] - st["full_flights"] - st["coop_flights"],
+                      "coop_rounds": st["coop_rounds"], "safe_balls": st["safe_balls"]},
             "kappa": out["kappa"] if out else None,
             "kappa_stderr": out["kappa_stderr"] if out else None,
             "kappa_rel_stderr": (out["kappa_stderr"] / out["kappa"]) if out and out["kappa"] else None,

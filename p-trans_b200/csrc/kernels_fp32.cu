@@ -242,43 +242,34 @@ __device__ __forceinline__ void test_surface(const G_t& G, int s, float px, floa
     tr = t;
     sb = s;
   } else {
+    /* sphere or z cylinder, written with selects: the lanes of a warp test
+       the same surface with different rays, so the only branch is the one
+       around the square root (a ray that misses) */
     const bool interior = (B.x & REC_INTERIOR) != 0;
-    if (!interior && B.w == last_geom) return;
-    float wx = A.x - px, wy = A.y - py, wz, a, b, c, r;
-    if (type == REC_SPHERE) {
-      wz = A.z - pz;
-      r = A.w;
-      a = 1.0f;
-      b = fmaf(wx, dx, fmaf(wy, dy, wz * dz));
-      c = fmaf(wx, wx, fmaf(wy, wy, wz * wz)) - r * r;
-    } else {
-      r = A.z;
-      a = fmaf(dx, dx, dy * dy);
-      if (!(a > 0.0f)) return;
-      b = fmaf(wx, dx, wy * dy);
-      c = fmaf(wx, wx, wy * wy) - r * r;
-    }
+    const bool sph = type == REC_SPHERE;
+    const float wx = A.x - px, wy = A.y - py;
+    const float wz = sph ? A.z - pz : 0.0f, ez = sph ? dz : 0.0f;
+    const float r = sph ? A.w : A.z;
+    const float a = sph ? 1.0f : fmaf(dx, dx, dy * dy);
+    const float b = fmaf(wx, dx, fmaf(wy, dy, wz * ez));
+    const float c = fmaf(wx, wx, fmaf(wy, wy, wz * wz)) - r * r;
     /* roots of a t^2 - 2 b t + c = 0 */
     const float disc = fmaf(b, b, -a * c);
-    if (!(disc >= 0.0f)) return;
-    const float sq = sqrtf(disc);
-    float t;
-    if (interior) {
-      /* far root (b + sq)/a, written without cancellation */
-      t = (b >= 0.0f) ? __fdividef(b + sq, a) : __fdividef(-c, sq - b);
-    } else {
-      /* near root (b - sq)/a = c / (b + sq), valid when approaching */
-      if (!(b > 0.0f)) return;
-      t = __fdividef(c, b + sq);
-      if (!(t >= -eps)) return;
-    }
-    if (!closer(t, s, tr, sb)) return;
-    if (type == REC_CYL) {
+    if ((interior || B.w != last_geom) && a > 0.0f && disc >= 0.0f) {
+      const float sq = sqrtf(disc);
+      /* from inside the far root (b + sq)/a, written without cancellation;
+         from outside the near root (b - sq)/a = c / (b + sq), valid when
+         approaching */
+      const bool bp = b >= 0.0f;
+      const float num = interior ? (bp ? b + sq : -c) : c;
+      const float den = interior ? (bp ? a : sq - b) : b + sq;
+      const float t = __fdividef(num, den);
       const float hz = fmaf(t, dz, pz);
-      if (hz < 0.0f || hz > zmax) return;
+      const bool ok = (interior || (b > 0.0f && t >= -eps)) && closer(t, s, tr, sb) &&
+                      (type != REC_CYL || !(hz < 0.0f || hz > zmax));
+      tr = ok ? t : tr;
+      sb = ok ? s : sb;
     }
-    tr = t;
-    sb = s;
   }
 }
 
@@ -385,18 +376,19 @@ __device__ __forceinline__ void scan_grain(const G_t& G, int grain, float px, fl
 __device__ __forceinline__ void slab_exit(float px, float py, float pz, float dx, float dy,
                                           float dz, float X, float Y, float Z, float& tb,
                                           int& sb) {
-  tb = 3.0e38f;
-  sb = -1;
-  if (dx > 0.0f) { tb = __fdividef(X - px, dx); sb = 1; }
-  else if (dx < 0.0f) { tb = __fdividef(-px, dx); sb = 0; }
-  if (dy != 0.0f) {
-    const float t = __fdividef((dy > 0.0f ? Y : 0.0f) - py, dy);
-    if (t < tb) { tb = t; sb = dy > 0.0f ? 3 : 2; }
-  }
-  if (dz != 0.0f) {
-    const float t = __fdividef((dz > 0.0f ? Z : 0.0f) - pz, dz);
-    if (t < tb) { tb = t; sb = dz > 0.0f ? 5 : 4; }
-  }
+  /* selects, no branches: the lanes of a warp go different ways */
+  const float tx = __fdividef(dx > 0.0f ? X - px : -px, dx);
+  const float ty = __fdividef((dy > 0.0f ? Y : 0.0f) - py, dy);
+  const float tz = __fdividef((dz > 0.0f ? Z : 0.0f) - pz, dz);
+  const bool hx = dx > 0.0f || dx < 0.0f;
+  tb = hx ? tx : 3.0e38f;
+  sb = hx ? (dx > 0.0f ? 1 : 0) : -1;
+  const bool hy = dy != 0.0f && ty < tb;
+  tb = hy ? ty : tb;
+  sb = hy ? (dy > 0.0f ? 3 : 2) : sb;
+  const bool hz = dz != 0.0f && tz < tb;
+  tb = hz ? tz : tb;
+  sb = hz ? (dz > 0.0f ? 5 : 4) : sb;
   tb = fmaxf(tb, 0.0f);
 }
 
@@ -487,21 +479,27 @@ __device__ __noinline__ float safety_bvh(const G_t& G, int root, float px, float
 
 /* Lower bound of the distance from p to every box face and to every
    candidate surface of the grain, less 4 eps.  A grain with a BVH is
-   searched only within `cap` (the radius the safe ball needs). */
+   searched only within `cap` (the radius the safe ball needs).  dgrain
+   receives the bound over the candidate surfaces alone (the grain ball: a
+   flight inside it needs the box-face test only); for a BVH grain it is
+   searched no farther than the full bound, so it costs no extra nodes. */
 template <bool EXT, class G_t>
 __device__ __forceinline__ float safety(const G_t& G, int grain, float px, float py, float pz,
-                                        float X, float Y, float Z, float eps, float cap) {
-  float d = fminf(fminf(fminf(px, X - px), fminf(py, Y - py)), fminf(pz, Z - pz));
+                                        float X, float Y, float Z, float eps, float cap,
+                                        float& dgrain) {
+  const float dbox = fminf(fminf(fminf(px, X - px), fminf(py, Y - py)), fminf(pz, Z - pz));
+  float dc = 3.0e38f;
   if (grain > 0) {
     const int root = EXT ? G.bvh_root(grain) : -1;
     if (root < 0) {
       const int kb = G.cand_begin(grain), ke = G.cand_begin(grain + 1);
-      for (int k = kb; k < ke; ++k) d = fminf(d, surface_lb<EXT>(G, G.cand(k), px, py, pz));
+      for (int k = kb; k < ke; ++k) dc = fminf(dc, surface_lb<EXT>(G, G.cand(k), px, py, pz));
     } else {
-      d = safety_bvh<EXT>(G, root, px, py, pz, fminf(d, cap));
+      dc = safety_bvh<EXT>(G, root, px, py, pz, fminf(dbox, cap));
     }
   }
-  return d - 4.0f * eps;
+  dgrain = dc - 4.0f * eps;
+  return fminf(dbox, dc) - 4.0f * eps;
 }
 
 /* Trace replay: position after flight f of the sample in replay-list slot t
@@ -607,9 +605,14 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   float flmax = r.fast_lambda_max;
   /* adjoint replay: per-block accumulators */
   __shared__ double adj_sh[MODE == MODE_ADJOINT ? kAdjSmemDoubles : 1];
-  /* cooperative rounds: one row of 32 (free path, direction) per warp */
-  __shared__ float4 coop_rows[(BATCH || MODE == MODE_TRACE) ? 1 : kBlock / 32][32];
-  float4* const wrow = coop_rows[(BATCH || MODE == MODE_TRACE) ? 0 : (threadIdx.x >> 5)];
+  /* cooperative rounds: per warp one row of 32 (free path, direction) and
+     one of 32 flight start points */
+  __shared__ float4 coop_rows[(BATCH || MODE == MODE_TRACE) ? 1 : kBlock / 32][2][32];
+  float4* const wrow = coop_rows[(BATCH || MODE == MODE_TRACE) ? 0 : (threadIdx.x >> 5)][0];
+  float4* const qrow = coop_rows[(BATCH || MODE == MODE_TRACE) ? 0 : (threadIdx.x >> 5)][1];
+  /* ... and five rows where the lanes' own phonons wait during the rounds */
+  __shared__ float4 coop_park[(BATCH || MODE == MODE_TRACE) ? 1 : kBlock / 32][5][32];
+  float4 (*const park)[32] = coop_park[(BATCH || MODE == MODE_TRACE) ? 0 : (threadIdx.x >> 5)];
   const int adj_stride = r.nsurf + 1;
   const bool adj_in_smem = (MODE == MODE_ADJOINT) && kAdjBatches * adj_stride <= kAdjSmemDoubles;
   if (MODE == MODE_ADJOINT && adj_in_smem) {
@@ -629,8 +632,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   /* lane state */
   bool alive = false;
   float px = 0, py = 0, pz = 0, dx = 1, dy = 0, dz = 0, fp = 0, lam = 0, omr = 0;
-  /* safe ball: no surface closer than sqrt(br2) to (bx, by, bz) */
-  float bx = 0, by = 0, bz = 0, br2 = 0;
+  /* safe ball: no surface closer than sqrt(br2) to (bx, by, bz); grain
+     ball: no candidate surface of the grain closer than sqrt(gr2) to the
+     same centre (box faces excepted), kept until the phonon changes grain */
+  float bx = 0, by = 0, bz = 0, br2 = 0, gr2 = 0;
   int grain = 0, last_geom = -1, task = 0;
   uint32_t slo = 0, shi = 0, flight = 0;
   unsigned long long my_flights = 0, my_samples = 0, my_capped = 0, my_lost = 0, my_max = 0;
@@ -748,6 +753,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           }
           last_geom = -1;
           br2 = 0.0f;
+          gr2 = 0.0f;
           flight = 0;
           alive = true;
           my_samples += 1;
@@ -791,22 +797,33 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           sparse ? elig : (elig & __ballot_sync(FULL, r.long_flights > 0 && flight >= r.long_flights));
       const int max_rounds = sparse ? kCoopRounds : kCoopRoundsBusy;
       if (todo0) {
+        /* every lane's own phonon waits in the warp's park rows while the
+           warp runs the rounds, so its registers serve the rounds; each
+           cooperative phonon is read from its lane's slot (broadcast loads)
+           and written back there by its lane */
+        park[0][lane] = make_float4(px, py, pz, dx);
+        park[1][lane] = make_float4(dy, dz, fp, lam);
+        park[2][lane] = make_float4(bx, by, bz, br2);
+        park[3][lane] = make_float4(__int_as_float(grain), __int_as_float(last_geom),
+                                    __int_as_float(task), omr);
+        park[4][lane] = make_float4(__uint_as_float(slo), __uint_as_float(shi),
+                                    __uint_as_float(flight), gr2);
+        __syncwarp();
         unsigned todo = todo0;
         while (todo) {
           const int L = __ffs(todo) - 1;
           todo &= todo - 1;
-          float cpx = __shfl_sync(FULL, px, L), cpy = __shfl_sync(FULL, py, L);
-          float cpz = __shfl_sync(FULL, pz, L);
-          float cdx = __shfl_sync(FULL, dx, L), cdy = __shfl_sync(FULL, dy, L);
-          float cdz = __shfl_sync(FULL, dz, L), cfp = __shfl_sync(FULL, fp, L);
-          const float clam = __shfl_sync(FULL, lam, L);
-          uint32_t cfl = __shfl_sync(FULL, flight, L);
-          const uint32_t cslo = __shfl_sync(FULL, slo, L), cshi = __shfl_sync(FULL, shi, L);
-          const int cgrain = __shfl_sync(FULL, grain, L);
-          int clast = __shfl_sync(FULL, last_geom, L);
+          const float4 s0 = park[0][L], s1 = park[1][L], s2 = park[2][L], s3 = park[3][L];
+          const float4 s4 = park[4][L];
+          float cpx = s0.x, cpy = s0.y, cpz = s0.z;
+          float cdx = s0.w, cdy = s1.x, cdz = s1.y, cfp = s1.z;
+          const float clam = s1.w;
+          uint32_t cfl = __float_as_uint(s4.z);
+          const uint32_t cslo = __float_as_uint(s4.x), cshi = __float_as_uint(s4.y);
+          const int cgrain = __float_as_int(s3.x);
+          int clast = __float_as_int(s3.y);
           /* the phonon's safe ball: flights ending inside it skip the test */
-          float cbx = __shfl_sync(FULL, bx, L), cby = __shfl_sync(FULL, by, L);
-          float cbz = __shfl_sync(FULL, bz, L), cbr2 = __shfl_sync(FULL, br2, L);
+          float cbx = s2.x, cby = s2.y, cbz = s2.z, cbr2 = s2.w, cgr2 = s4.w;
           float clen = 0.0f;
           unsigned cnpp = 0, ctaken = 0, crounds = 0;
           int stop = 0;  /* 0 round limit, 1 surface hit, 2 lost or capped */
@@ -825,24 +842,41 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             const float nf = -clam * __logf(u23f(R.z));
             /* flight `lane` starts with the state the previous flight drew:
                the warp's row of shared memory holds (free path, direction)
-               of every flight of the round, so the start points are summed
-               from broadcast loads issued ahead of the fma chain */
+               of flights 1..31 of the round.  The start point of flight j
+               is the chain p, fma(fp_0, d_0, p), ... after j steps, the same
+               for every lane: the warp runs the chain once (flight 0's step
+               from registers, the others from broadcast loads issued eight
+               at a time ahead of their fmas), stores every step to a second
+               row, and each lane reads its own start point back */
             if (lane < 31) wrow[lane + 1] = make_float4(nf, nx, ny, nz);
-            if (lane == 0) wrow[0] = make_float4(cfp, cdx, cdy, cdz);
             __syncwarp();
-            const float4 mine = wrow[lane];
+            const float4 mine = lane == 0 ? make_float4(cfp, cdx, cdy, cdz) : wrow[lane];
             const float sfp = mine.x, sdx = mine.y, sdy = mine.z, sdz = mine.w;
-            float qx = cpx, qy = cpy, qz = cpz;
+            {
+              float ax = fmaf(cfp, cdx, cpx), ay = fmaf(cfp, cdy, cpy), az = fmaf(cfp, cdz, cpz);
+              qrow[1] = make_float4(ax, ay, az, 0.0f);
 #pragma unroll
-            for (int i = 0; i < 31; ++i) {
-              const float4 v = wrow[i];
-              if (i < lane) {
-                qx = fmaf(v.x, v.y, qx);
-                qy = fmaf(v.x, v.z, qy);
-                qz = fmaf(v.x, v.w, qz);
+              for (int b = 1; b < 31; b += 8) {
+                float4 v[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k)
+                  if (b + k < 31) v[k] = wrow[b + k];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                  if (b + k < 31) {
+                    ax = fmaf(v[k].x, v[k].y, ax);
+                    ay = fmaf(v[k].x, v[k].z, ay);
+                    az = fmaf(v[k].x, v[k].w, az);
+                    qrow[b + k + 1] = make_float4(ax, ay, az, 0.0f);
+                  }
+                }
               }
             }
-            __syncwarp();  /* the next round rewrites the row */
+            __syncwarp();
+            const float4 qs = qrow[lane];
+            const float qx = lane == 0 ? cpx : qs.x, qy = lane == 0 ? cpy : qs.y;
+            const float qz = lane == 0 ? cpz : qs.z;
+            __syncwarp();  /* the next round rewrites both rows */
             const bool inbox = qx >= -eps && qx <= X + eps && qy >= -eps && qy <= Y + eps &&
                                qz >= -eps && qz <= Z + eps;
             const bool capd = (unsigned long long)cfl + (unsigned)lane >= r.max_flights;
@@ -852,13 +886,16 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             const float ex = fmaf(sfp, sdx, qx) - cbx, ey = fmaf(sfp, sdy, qy) - cby;
             const float ez = fmaf(sfp, sdz, qz) - cbz;
             const float sx = qx - cbx, sy = qy - cby, sz = qz - cbz;
-            const bool in_ball = fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < cbr2 &&
-                                 fmaf(sx, sx, fmaf(sy, sy, sz * sz)) < cbr2;
+            const float de2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+            const float ds2 = fmaf(sx, sx, fmaf(sy, sy, sz * sz));
+            const bool in_ball = de2 < cbr2 && ds2 < cbr2;
+            /* in the grain ball only the box faces can be hit */
+            const bool in_gball = de2 < cgr2 && ds2 < cgr2;
             float tb = 3.0e38f;
             int sb = -1;
             if (!in_ball) {
               slab_exit(qx, qy, qz, sdx, sdy, sdz, X, Y, Z, tb, sb);
-              if (cgrain > 0)
+              if (cgrain > 0 && !in_gball)
                 scan_grain<EXT>(G, cgrain, qx, qy, qz, sdx, sdy, sdz, lane == 0 ? clast : -1, eps,
                                 Z, tb, sb, my_box_tests, my_surf_tests);
             }
@@ -897,18 +934,22 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             cfl += 32u;
             /* a new ball where the walk left the old one */
             if (!__shfl_sync(FULL, in_ball, 31) && r.fast_steps > 0) {
-              const float d = safety<EXT>(G, cgrain, cpx, cpy, cpz, X, Y, Z, eps, kBallCapMfp * clam);
+              float dg;
+              const float d =
+                  safety<EXT>(G, cgrain, cpx, cpy, cpz, X, Y, Z, eps, kBallCapMfp * clam, dg);
               cbx = cpx; cby = cpy; cbz = cpz;
               cbr2 = d > 0.0f ? d * d : 0.0f;
+              cgr2 = dg > 0.0f ? dg * dg : 0.0f;
             }
             clast = -1;
           }
           if (lane == L) {
-            px = cpx; py = cpy; pz = cpz;
-            dx = cdx; dy = cdy; dz = cdz; fp = cfp;
-            bx = cbx; by = cby; bz = cbz; br2 = cbr2;
-            flight = cfl;
-            last_geom = clast;
+            park[0][lane] = make_float4(cpx, cpy, cpz, cdx);
+            park[1][lane] = make_float4(cdy, cdz, cfp, clam);
+            park[2][lane] = make_float4(cbx, cby, cbz, cbr2);
+            park[3][lane] = make_float4(__int_as_float(cgrain), __int_as_float(clast),
+                                        s3.z, s3.w);
+            park[4][lane] = make_float4(s4.x, s4.y, __uint_as_float(cfl), cgr2);
             if (MODE == MODE_ADJOINT) {
               adj_len += clen;
               adj_npp += cnpp;
@@ -926,6 +967,17 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             my_coop_flights += ctaken;
           }
         }
+        /* every lane takes its phonon back (each slot was last written by its
+           own lane) */
+        const float4 s0 = park[0][lane], s1 = park[1][lane], s2 = park[2][lane];
+        const float4 s3 = park[3][lane], s4 = park[4][lane];
+        px = s0.x; py = s0.y; pz = s0.z; dx = s0.w;
+        dy = s1.x; dz = s1.y; fp = s1.z; lam = s1.w;
+        bx = s2.x; by = s2.y; bz = s2.z; br2 = s2.w;
+        grain = __float_as_int(s3.x); last_geom = __float_as_int(s3.y);
+        task = __float_as_int(s3.z); omr = s3.w;
+        slo = __float_as_uint(s4.x); shi = __float_as_uint(s4.y); flight = __float_as_uint(s4.z);
+        gr2 = s4.w;
       }
     }
 
@@ -997,7 +1049,12 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           ++my_full;
           R = philox10(flight, c1, slo, shi, key);
           slab_exit(px, py, pz, dx, dy, dz, X, Y, Z, tb, sb);
-          if (grain > 0)
+          const float ex = fmaf(fp, dx, px) - bx, ey = fmaf(fp, dy, py) - by;
+          const float ez = fmaf(fp, dz, pz) - bz;
+          const float sx = px - bx, sy = py - by, sz = pz - bz;
+          const bool in_gball = fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < gr2 &&
+                                fmaf(sx, sx, fmaf(sy, sy, sz * sz)) < gr2;
+          if (grain > 0 && !in_gball)
             scan_grain<EXT>(G, grain, px, py, pz, dx, dy, dz, last_geom, eps, Z, tb, sb, my_box_tests,
                        my_surf_tests);
           go = true;
@@ -1024,9 +1081,14 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             last_geom = -1;
             br2 = 0.0f;
             if (MODE != MODE_TRACE && r.fast_steps > 0 && lam < flmax) {
-              const float d = safety<EXT>(G, grain, px, py, pz, X, Y, Z, eps, kBallCapMfp * lam);
+              float dg;
+              const float d = safety<EXT>(G, grain, px, py, pz, X, Y, Z, eps, kBallCapMfp * lam, dg);
               ++my_balls;
-              if (d > 0.0f) { bx = px; by = py; bz = pz; br2 = d * d; }
+              if (dg > 0.0f) {
+                bx = px; by = py; bz = pz;
+                br2 = d > 0.0f ? d * d : 0.0f;
+                gr2 = dg * dg;
+              }
             }
           } else {
             br2 = 0.0f;
@@ -1134,7 +1196,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
                 if (u3 <= thr) { sg = -sg; transmitted = true; }
                 dx = sg * vx; dy = sg * vy; dz = sg * vz;
               }
-              if (transmitted) grain = meta >> 8;
+              if (transmitted) {
+                grain = meta >> 8;
+                gr2 = 0.0f;
+              }
               last_geom = B.w;
             }
             if (end_side < 0 && fp < 1.0e-10f) {

@@ -194,7 +194,10 @@ def test_cooperative_tail_takes_the_same_trajectories(name, cap):
     past 16 flights with long_flights = 16) and the one-lane path
     (tune_flags bit 1) give identical per-task counts, lost counts and
     flight totals: a flight advances the position with the same rounding on
-    every path, so the trajectory depends only on its Philox counter."""
+    every path, so the trajectory depends only on its Philox counter.  With
+    the fast path off (tune_flags bit 0) no safe ball or grain ball is ever
+    computed and every flight takes the full test, so the variants without
+    it also show that the tests the balls skip could not have hit."""
     m = geometries()[name]
     spec = synth.spectrum(12, seed=5, mfp_lo=1e-9, mfp_hi=3e-8)
     gb = A.GeomBuf(m)
@@ -202,13 +205,13 @@ def test_cooperative_tail_takes_the_same_trajectories(name, cap):
     out = {}
     for key, opts in (("lane", dict(tune_flags=2)), ("coop", dict(coop_lanes=32)),
                       ("tail", dict()), ("coop_nofast", dict(coop_lanes=32, tune_flags=1)),
-                      ("long", dict(coop_lanes=1, long_flights=16))):
+                      ("long", dict(coop_lanes=1, long_flights=16)), ("lane_nofast", dict(tune_flags=3))):
         with A.Handle(gb.view, spec, max_flights=cap, **opts) as h:
             k = h.kappa(run, want_counts=True)
             out[key] = (k["counts"], k["lost"], h.stats())
     base_counts, base_lost, base_st = out["lane"]
     assert base_st["coop_rounds"] == 0
-    for key in ("coop", "tail", "coop_nofast", "long"):
+    for key in ("coop", "tail", "coop_nofast", "long", "lane_nofast"):
         counts, lost, st = out[key]
         np.testing.assert_array_equal(counts, base_counts, err_msg=key)
         assert lost == base_lost, key
