@@ -190,12 +190,14 @@ typedef struct ptg_options {
   int64_t chunk;            /* samples per work-queue chunk (0 = tuned)         */
   int32_t tune_flags;       /* persistent kernel variants (autotuner):          */
                             /*   bit 0: no safe-distance p-p fast path          */
-                            /*   bit 1: no warp-cooperative tail                */
+                            /*   bit 1: no tail phase (one lane per phonon to   */
+                            /*          the end)                                */
   int32_t fast_steps;       /* fast p-p flights per iteration (0 = tuned)       */
-  int32_t coop_lanes;       /* a warp with at most this many live phonons       */
-                            /* advances them with all 32 lanes (0 = tuned)      */
-  int32_t long_flights;     /* a phonon past this many flights is advanced by   */
-                            /* its whole warp even in a busy warp (<= 0: never) */
+  int32_t coop_lanes;       /* once the work queue is dry, a warp with at most  */
+                            /* this many live phonons hands its diffusive ones  */
+                            /* to the tail phase, a second kernel that gives    */
+                            /* each a warp of 32 cooperating lanes (0 = 32)     */
+  int32_t long_flights;     /* unused; kept so the struct layout stays          */
 } ptg_options;
 
 /*
@@ -455,7 +457,7 @@ int ptg_write_trace(ptg_handle* h, const ptg_run* run, int32_t particle_trace, c
  * bvh_leaf rebuilds the device geometry.  ptg_autotune times ptg_kappa with
  * `run` in FP32 (best of `reps` calls per trial) while it varies, one at a
  * time, bvh_leaf (when a grain has a BVH), block_size, blocks_per_sm,
- * coop_lanes, long_flights, fast_steps, regen_threshold and chunk; it leaves the fastest
+ * coop_lanes, fast_steps, regen_threshold and chunk; it leaves the fastest
  * options on the handle and in *best, with their kernel time in *best_ms.
  * Trajectories depend only on their Philox counters, so no option changes a
  * result.  The call runs about 20 trials of the given run: tune on a run

@@ -74,6 +74,8 @@ struct ptg_handle {
   size_t blob_bytes = 0;
   /* work buffers */
   DevBuf task, chunk, counts, lost, stats, queue;
+  /* FP32 tail phase: phonons the drain phase hands over */
+  DevBuf tail;
   /* reduction */
   DevBuf red_coef, red_K, red_W, red_mfp, red_bin, red_grid, red_tc, red_kv, red_bw, red_bv,
       red_emfp, red_trans, red_result;
@@ -87,7 +89,7 @@ struct ptg_handle {
     DevBuf* all[] = {&blob, &task, &chunk, &counts, &lost, &stats, &queue, &red_coef, &red_K,
                      &red_W, &red_mfp, &red_bin, &red_grid, &red_tc, &red_kv, &red_bw, &red_bv,
                      &red_emfp, &red_trans, &red_result, &adj_list, &adj_w, &adj_acc,
-                     &tr_off, &tr_npos, &tr_end, &tr_pos};
+                     &tr_off, &tr_npos, &tr_end, &tr_pos, &tail};
     for (DevBuf* b : all) b->release();
     for (cudaEvent_t e : ev) if (e) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);
@@ -527,13 +529,9 @@ int run_transport(ptg_handle* h, const Transport& T) {
     r.fast_steps = (h->opt.tune_flags & 1) ? 0 : (h->opt.fast_steps > 0 ? h->opt.fast_steps : 16);
     const double lmin = std::min(h->geom.box[0], std::min(h->geom.box[1], h->geom.box[2]));
     r.fast_lambda_max = (float)(0.1 * lmin);
-    /* tune_flags bit 1 turns the cooperative tail off; 0 selects 8 lanes */
-    r.coop_lanes = (h->opt.tune_flags & 2) ? 0 : (h->opt.coop_lanes > 0 ? std::min(h->opt.coop_lanes, 32) : 8);
-    /* busy-warp promotion only when asked for (it slows the warps that
-       carry a promoted phonon more than it shortens the tail on the
-       thin-film workload) */
-    r.long_flights = (r.coop_lanes == 0 || h->opt.long_flights <= 0) ? 0u
-                                                                     : (uint32_t)h->opt.long_flights;
+    /* tune_flags bit 1 turns the tail phase off; 0 selects 32 lanes (every
+       diffusive phonon still alive when a warp finds the queue dry) */
+    r.coop_lanes = (h->opt.tune_flags & 2) ? 0 : (h->opt.coop_lanes > 0 ? std::min(h->opt.coop_lanes, 32) : 32);
     r.counts = h->counts.as<unsigned long long>();
     r.lost = h->lost.as<unsigned long long>();
     r.stats = h->stats.as<unsigned long long>();
@@ -557,14 +555,31 @@ int run_transport(ptg_handle* h, const Transport& T) {
     if (h->opt.blocks_per_sm > 0 && h->opt.blocks_per_sm < bps) bps = h->opt.blocks_per_sm;
     if (bps < 1) bps = 1;
     const int grid = h->num_sms * bps;
+    /* a lane hands over at most one phonon (no refill once the queue is
+       dry), so the drain grid's lanes bound the tail list */
+    const bool tail = r.coop_lanes > 0 && T.mode != ptg::MODE_TRACE;
+    if (tail) {
+      CU(h->tail.ensure(sizeof(float4) * 6 * (size_t)grid * block));
+      r.tail = h->tail.as<float4>();
+      r.tail_cap = grid * block;
+    }
+    int tgrid = 0;
+    if (tail) {
+      int tbps = 0;
+      CU(ptg::tail_occupancy(block, smem, &tbps, T.mode, h->g32.has_ext != 0));
+      tgrid = h->num_sms * (tbps < 1 ? 1 : tbps);
+    }
     CU(cudaEventRecord(h->ev[0], h->stream));
     const bool work = (T.mode == ptg::MODE_ADJOINT || T.mode == ptg::MODE_TRACE) ? T.alist_n > 0
                                                                                    : r.nchunk > 0;
-    if (work) CU(ptg::launch_persistent_fp32(h->g32, r, grid, block, smem, h->stream, T.mode));
+    if (work) {
+      CU(ptg::launch_persistent_fp32(h->g32, r, grid, block, smem, h->stream, T.mode));
+      if (tail) CU(ptg::launch_tail_fp32(h->g32, r, tgrid, block, smem, h->stream, T.mode));
+    }
     CU(cudaEventRecord(h->ev[1], h->stream));
     h->last.grid = grid;
     h->last.block = block;
-    h->last.launches = 1;
+    h->last.launches = work ? (tail ? 2 : 1) : 0;
   }
   return PTG_OK;
 }

@@ -130,17 +130,20 @@ struct RunF32 {
   int32_t regen_threshold;
   int32_t fast_steps;         /* max safe-distance p-p flights per iteration (0: off) */
   float fast_lambda_max;      /* tasks with a smaller MFP use the fast path           */
-  int32_t coop_lanes;         /* warps with at most this many live lanes advance them
-                                 cooperatively, 32 flights a round (0: off)       */
-  uint32_t long_flights;      /* a phonon past this many flights goes cooperative
-                                 even in a busy warp (0: never)                    */
+  int32_t coop_lanes;         /* once the queue is dry, a warp with at most this many
+                                 live phonons moves its diffusive ones to the tail
+                                 list, where each gets a warp of its own that
+                                 advances it 32 flights a round (0: off)          */
+  float4* tail;               /* tail list: 6 float4 per phonon                    */
+  int32_t tail_cap;           /* its capacity in phonons                           */
   unsigned long long* counts;
   unsigned long long* lost;
   /* flights, lost, capped, samples, max trajectory flights,
      t_start (min), t_drain (min), t_end (max) in globaltimer ns,
      flights taken with the intersection test, safe balls built */
   unsigned long long* stats;
-  int* queue;                 /* [0] next chunk, [1] error flags */
+  int* queue;                 /* [0] next chunk, [1] error flags, [2] phonons put
+                                 in the tail list, [3] next tail-list phonon */
   /* adjoint support */
   unsigned long long* tlist;  /* mode 1: sample ids of transmitted phonons         */
   unsigned long long tlist_cap;
@@ -170,6 +173,12 @@ enum { MODE_FORWARD = 0, MODE_LIST = 1, MODE_ADJOINT = 2, MODE_TRACE = 3 };
 
 cudaError_t launch_persistent_fp32(const GeoF32& g, const RunF32& r, int grid, int block,
                                    size_t smem, cudaStream_t st, int mode = MODE_FORWARD);
+/* The tail phase after it (forward, list and adjoint modes): the phonons
+   the drain phase left in r.tail, one per warp. */
+cudaError_t launch_tail_fp32(const GeoF32& g, const RunF32& r, int grid, int block, size_t smem,
+                             cudaStream_t st, int mode = MODE_FORWARD);
+cudaError_t tail_occupancy(int block, size_t smem, int* blocks_per_sm, int mode = MODE_FORWARD,
+                           bool bvh = false);
 /* Batched launch over several geometries (forward mode, geometry in global memory). */
 cudaError_t launch_persistent_batch(const RunF32& r, int grid, int block, cudaStream_t st,
                                     bool bvh);

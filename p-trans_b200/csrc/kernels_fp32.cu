@@ -578,19 +578,28 @@ constexpr int kAdjSmemDoubles = 2048;
 /* rounds of 32 flights one cooperative visit may take before the phonon's
    lane returns to the refill / tally step */
 constexpr int kCoopRounds = 8;
-/* rounds per visit of a long phonon in a warp whose other lanes are busy */
-constexpr int kCoopRoundsBusy = 4;
+
+/* Kernel phases.  PH_DRAIN pulls (task, particle range) chunks from the
+   work queue, one phonon per lane; once the queue is dry a warp holding at
+   most coop_lanes live phonons moves its diffusive ones (MFP below the
+   fast-path limit) to the tail list and finishes the others.  PH_TAIL runs
+   after it: every warp takes one phonon of the tail list at a time into
+   lane 0 and advances it with cooperative rounds, so the longest
+   trajectories get a warp each instead of sharing one. */
+enum { PH_DRAIN = 0, PH_TAIL = 1 };
+/* float4 per phonon in the tail list */
+constexpr int kTailUnits = 6;
 
 /* safe-ball radius searched in a grain with a BVH, in units of the MFP: a
    walk needs about (radius / MFP)^2 flights to leave the ball */
 constexpr float kBallCapMfp = 32.0f;
 
-template <bool SMEM, int MODE, bool BATCH, bool EXT>
+template <bool SMEM, int MODE, bool BATCH, bool EXT, int PH>
 __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   typename std::conditional<BATCH, GeoBatch, Geo<SMEM>>::type G;
   G.lay = gp.lay;
   G.base = gp.blob;
-  if (threadIdx.x == 0) atomicMin(r.stats + 5, globaltimer());
+  if (PH == PH_DRAIN && threadIdx.x == 0) atomicMin(r.stats + 5, globaltimer());
   if (SMEM) {
     /* on a timeout the block records the error and leaves: the host reports it */
     if (!stage_blob(gp.blob, sblob, gp.lay.total, r.queue + 1)) return;
@@ -607,12 +616,14 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   __shared__ double adj_sh[MODE == MODE_ADJOINT ? kAdjSmemDoubles : 1];
   /* cooperative rounds: per warp one row of 32 (free path, direction) and
      one of 32 flight start points */
-  __shared__ float4 coop_rows[(BATCH || MODE == MODE_TRACE) ? 1 : kBlock / 32][2][32];
-  float4* const wrow = coop_rows[(BATCH || MODE == MODE_TRACE) ? 0 : (threadIdx.x >> 5)][0];
-  float4* const qrow = coop_rows[(BATCH || MODE == MODE_TRACE) ? 0 : (threadIdx.x >> 5)][1];
+  __shared__ float4 coop_rows[PH == PH_TAIL ? kBlock / 32 : 1][2][32];
+  float4* const wrow = coop_rows[PH == PH_TAIL ? (threadIdx.x >> 5) : 0][0];
+  float4* const qrow = coop_rows[PH == PH_TAIL ? (threadIdx.x >> 5) : 0][1];
   /* ... and five rows where the lanes' own phonons wait during the rounds */
-  __shared__ float4 coop_park[(BATCH || MODE == MODE_TRACE) ? 1 : kBlock / 32][5][32];
-  float4 (*const park)[32] = coop_park[(BATCH || MODE == MODE_TRACE) ? 0 : (threadIdx.x >> 5)];
+  __shared__ float4 coop_park[PH == PH_TAIL ? kBlock / 32 : 1][5][32];
+  float4 (*const park)[32] = coop_park[PH == PH_TAIL ? (threadIdx.x >> 5) : 0];
+  /* tail phase: phonons the drain left (the count is final at launch) */
+  const int ntail = PH == PH_TAIL ? min(r.queue[2], r.tail_cap) : 0;
   const int adj_stride = r.nsurf + 1;
   const bool adj_in_smem = (MODE == MODE_ADJOINT) && kAdjBatches * adj_stride <= kAdjSmemDoubles;
   if (MODE == MODE_ADJOINT && adj_in_smem) {
@@ -644,9 +655,34 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   unsigned my_box_tests = 0, my_surf_tests = 0;  /* BVH node boxes, surfaces tested */
 
   while (true) {
+    /* ---- tail phase: lane 0 takes the next phonon of the tail list ----- */
+    if (PH == PH_TAIL && !queue_done && !__shfl_sync(FULL, alive, 0)) {
+      int c = 0;
+      if (lane == 0) c = atomicAdd(r.queue + 3, 1);
+      c = __shfl_sync(FULL, c, 0);
+      if (c >= ntail) {
+        queue_done = true;
+      } else if (lane == 0) {
+        const float4* e = r.tail + (size_t)kTailUnits * c;
+        const float4 e0 = e[0], e1 = e[1], e2 = e[2], e3 = e[3], e4 = e[4];
+        px = e0.x; py = e0.y; pz = e0.z; dx = e0.w;
+        dy = e1.x; dz = e1.y; fp = e1.z; lam = e1.w;
+        bx = e2.x; by = e2.y; bz = e2.z; br2 = e2.w;
+        grain = __float_as_int(e3.x); last_geom = __float_as_int(e3.y);
+        task = __float_as_int(e3.z); omr = e3.w;
+        slo = __float_as_uint(e4.x); shi = __float_as_uint(e4.y);
+        flight = __float_as_uint(e4.z); gr2 = e4.w;
+        if (MODE == MODE_ADJOINT) {
+          const float4 e5 = e[5];
+          adj_w = e5.x; adj_len = e5.y;
+          adj_npp = __float_as_uint(e5.z); adj_b = __float_as_int(e5.w);
+        }
+        alive = true;
+      }
+    }
     /* ---- refill idle lanes from the warp's chunk ---------------------- */
     unsigned idle = __ballot_sync(FULL, !alive);
-    if (!queue_done && idle &&
+    if (PH == PH_DRAIN && !queue_done && idle &&
         (__popc(idle) >= r.regen_threshold || idle == FULL)) {
       while (idle && !queue_done) {
         if (ch_left == 0) {
@@ -768,6 +804,33 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
       if (queue_done) break;
       continue;
     }
+    /* ---- drain phase, queue dry: diffusive phonons go to the tail list */
+    if (PH == PH_DRAIN && !BATCH && MODE != MODE_TRACE && queue_done && r.coop_lanes > 0 &&
+        __popc(__ballot_sync(FULL, alive)) <= r.coop_lanes) {
+      const unsigned mv = __ballot_sync(FULL, alive && lam < flmax);
+      if (mv) {
+        const int first = __ffs(mv) - 1;
+        int base = 0;
+        if (lane == first) base = atomicAdd(r.queue + 2, __popc(mv));
+        base = __shfl_sync(FULL, base, first);
+        const int slot = base + __popc(mv & lanemask_lt());
+        /* past the list's capacity a phonon stays here */
+        if (((mv >> lane) & 1u) && slot < r.tail_cap) {
+          float4* e = r.tail + (size_t)kTailUnits * slot;
+          e[0] = make_float4(px, py, pz, dx);
+          e[1] = make_float4(dy, dz, fp, lam);
+          e[2] = make_float4(bx, by, bz, br2);
+          e[3] = make_float4(__int_as_float(grain), __int_as_float(last_geom),
+                             __int_as_float(task), omr);
+          e[4] = make_float4(__uint_as_float(slo), __uint_as_float(shi), __uint_as_float(flight),
+                             gr2);
+          if (MODE == MODE_ADJOINT)
+            e[5] = make_float4(adj_w, adj_len, __uint_as_float(adj_npp), __int_as_float(adj_b));
+          alive = false;
+        }
+        if (!__any_sync(FULL, alive)) break;
+      }
+    }
 
     int end_side = -1;  /* -1 still running, 0 lost, 1 x-, 2 x+ */
 
@@ -788,14 +851,9 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
     uint4 preR = make_uint4(0u, 0u, 0u, 0u);
     float pre_tb = 0.0f;
     int pre_sb = -1;
-    if (!BATCH && MODE != MODE_TRACE && r.coop_lanes > 0) {
-      const unsigned elig = __ballot_sync(FULL, alive && lam < flmax);
-      const bool sparse = __popc(__ballot_sync(FULL, alive)) <= r.coop_lanes;
-      /* in a busy warp only phonons past long_flights flights go cooperative,
-         for fewer rounds, so the warp's other lanes keep moving */
-      const unsigned todo0 =
-          sparse ? elig : (elig & __ballot_sync(FULL, r.long_flights > 0 && flight >= r.long_flights));
-      const int max_rounds = sparse ? kCoopRounds : kCoopRoundsBusy;
+    if (PH == PH_TAIL) {
+      const unsigned todo0 = __ballot_sync(FULL, alive && lam < flmax);
+      const int max_rounds = kCoopRounds;
       if (todo0) {
         /* every lane's own phonon waits in the warp's park rows while the
            warp runs the rounds, so its registers serve the rounds; each
@@ -1299,34 +1357,36 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
 
 }  // namespace
 
-template <int MODE, bool EXT>
+template <int MODE, bool EXT, int PH>
 cudaError_t occupancy_mode(int block, size_t smem, int* bps) {
   if (smem > 0)
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_persistent<true, MODE, false, EXT>,
-                                                         block, smem);
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, k_persistent<false, MODE, false, EXT>,
-                                                       block, 0);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        bps, k_persistent<true, MODE, false, EXT, PH>, block, smem);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      bps, k_persistent<false, MODE, false, EXT, PH>, block, 0);
 }
 
-template <int MODE, bool EXT>
+template <int MODE, bool EXT, int PH>
 cudaError_t launch_mode(const GeoF32& g, const RunF32& r, int grid, int block, size_t smem,
                         cudaStream_t st) {
   if (g.stage_smem && smem > 0) {
     if (smem > 48 * 1024) {
-      cudaError_t e = cudaFuncSetAttribute(k_persistent<true, MODE, false, EXT>,
+      cudaError_t e = cudaFuncSetAttribute(k_persistent<true, MODE, false, EXT, PH>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
       if (e != cudaSuccess) return e;
     }
-    k_persistent<true, MODE, false, EXT><<<grid, block, smem, st>>>(g, r);
+    k_persistent<true, MODE, false, EXT, PH><<<grid, block, smem, st>>>(g, r);
   } else {
-    k_persistent<false, MODE, false, EXT><<<grid, block, 0, st>>>(g, r);
+    k_persistent<false, MODE, false, EXT, PH><<<grid, block, 0, st>>>(g, r);
   }
   return cudaGetLastError();
 }
 
 cudaError_t persistent_batch_occupancy(int block, int* bps, bool bvh) {
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      bps, bvh ? k_persistent<false, MODE_FORWARD, true, true> : k_persistent<false, MODE_FORWARD, true, false>,
+      bps,
+      bvh ? k_persistent<false, MODE_FORWARD, true, true, PH_DRAIN>
+          : k_persistent<false, MODE_FORWARD, true, false, PH_DRAIN>,
       block, 0);
 }
 
@@ -1334,37 +1394,58 @@ cudaError_t launch_persistent_batch(const RunF32& r, int grid, int block, cudaSt
   if (block != kBlock) return cudaErrorInvalidConfiguration;
   GeoF32 g;
   memset(&g, 0, sizeof(g));
-  if (bvh) k_persistent<false, MODE_FORWARD, true, true><<<grid, block, 0, st>>>(g, r);
-  else k_persistent<false, MODE_FORWARD, true, false><<<grid, block, 0, st>>>(g, r);
+  if (bvh) k_persistent<false, MODE_FORWARD, true, true, PH_DRAIN><<<grid, block, 0, st>>>(g, r);
+  else k_persistent<false, MODE_FORWARD, true, false, PH_DRAIN><<<grid, block, 0, st>>>(g, r);
   return cudaGetLastError();
 }
 
-template <bool EXT>
+/* The tail phase exists for the modes with cooperative rounds (forward,
+   list, adjoint replay); a trace replay runs every flight on one lane. */
+template <bool EXT, int PH>
 cudaError_t occupancy_bvh(int block, size_t smem, int* bps, int mode) {
-  if (mode == MODE_LIST) return occupancy_mode<MODE_LIST, EXT>(block, smem, bps);
-  if (mode == MODE_ADJOINT) return occupancy_mode<MODE_ADJOINT, EXT>(block, smem, bps);
-  if (mode == MODE_TRACE) return occupancy_mode<MODE_TRACE, EXT>(block, smem, bps);
-  return occupancy_mode<MODE_FORWARD, EXT>(block, smem, bps);
+  if (mode == MODE_LIST) return occupancy_mode<MODE_LIST, EXT, PH>(block, smem, bps);
+  if (mode == MODE_ADJOINT) return occupancy_mode<MODE_ADJOINT, EXT, PH>(block, smem, bps);
+  if (mode == MODE_TRACE) {
+    if (PH == PH_TAIL) return cudaErrorInvalidValue;
+    return occupancy_mode<MODE_TRACE, EXT, PH_DRAIN>(block, smem, bps);
+  }
+  return occupancy_mode<MODE_FORWARD, EXT, PH>(block, smem, bps);
 }
 
 cudaError_t persistent_occupancy(int block, size_t smem, int* bps, int mode, bool bvh) {
-  return bvh ? occupancy_bvh<true>(block, smem, bps, mode) : occupancy_bvh<false>(block, smem, bps, mode);
+  return bvh ? occupancy_bvh<true, PH_DRAIN>(block, smem, bps, mode)
+             : occupancy_bvh<false, PH_DRAIN>(block, smem, bps, mode);
 }
 
-template <bool EXT>
+cudaError_t tail_occupancy(int block, size_t smem, int* bps, int mode, bool bvh) {
+  return bvh ? occupancy_bvh<true, PH_TAIL>(block, smem, bps, mode)
+             : occupancy_bvh<false, PH_TAIL>(block, smem, bps, mode);
+}
+
+template <bool EXT, int PH>
 cudaError_t launch_bvh(const GeoF32& g, const RunF32& r, int grid, int block, size_t smem,
                        cudaStream_t st, int mode) {
-  if (mode == MODE_LIST) return launch_mode<MODE_LIST, EXT>(g, r, grid, block, smem, st);
-  if (mode == MODE_ADJOINT) return launch_mode<MODE_ADJOINT, EXT>(g, r, grid, block, smem, st);
-  if (mode == MODE_TRACE) return launch_mode<MODE_TRACE, EXT>(g, r, grid, block, smem, st);
-  return launch_mode<MODE_FORWARD, EXT>(g, r, grid, block, smem, st);
+  if (mode == MODE_LIST) return launch_mode<MODE_LIST, EXT, PH>(g, r, grid, block, smem, st);
+  if (mode == MODE_ADJOINT) return launch_mode<MODE_ADJOINT, EXT, PH>(g, r, grid, block, smem, st);
+  if (mode == MODE_TRACE) {
+    if (PH == PH_TAIL) return cudaErrorInvalidValue;
+    return launch_mode<MODE_TRACE, EXT, PH_DRAIN>(g, r, grid, block, smem, st);
+  }
+  return launch_mode<MODE_FORWARD, EXT, PH>(g, r, grid, block, smem, st);
 }
 
 cudaError_t launch_persistent_fp32(const GeoF32& g, const RunF32& r, int grid, int block,
                                    size_t smem, cudaStream_t st, int mode) {
   if (block > kBlock || block % 32) return cudaErrorInvalidConfiguration;
-  return g.has_ext ? launch_bvh<true>(g, r, grid, block, smem, st, mode)
-                   : launch_bvh<false>(g, r, grid, block, smem, st, mode);
+  return g.has_ext ? launch_bvh<true, PH_DRAIN>(g, r, grid, block, smem, st, mode)
+                   : launch_bvh<false, PH_DRAIN>(g, r, grid, block, smem, st, mode);
+}
+
+cudaError_t launch_tail_fp32(const GeoF32& g, const RunF32& r, int grid, int block, size_t smem,
+                             cudaStream_t st, int mode) {
+  if (block > kBlock || block % 32) return cudaErrorInvalidConfiguration;
+  return g.has_ext ? launch_bvh<true, PH_TAIL>(g, r, grid, block, smem, st, mode)
+                   : launch_bvh<false, PH_TAIL>(g, r, grid, block, smem, st, mode);
 }
 
 }  // namespace ptg

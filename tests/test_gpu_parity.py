@@ -190,8 +190,9 @@ def test_rank_partition_is_exact_fp32():
                                   "nanowire_mixed", "capped"])
 @pytest.mark.parametrize("cap", [0, 40])
 def test_cooperative_tail_takes_the_same_trajectories(name, cap):
-    """Warp-cooperative rounds (every warp with coop_lanes = 32; only phonons
-    past 16 flights with long_flights = 16) and the one-lane path
+    """The tail phase (a warp of cooperating lanes per diffusive phonon once
+    the queue is dry: handed over at once with coop_lanes = 32, or when a
+    warp holds at most 8 or 1 live phonons) and the one-lane path to the end
     (tune_flags bit 1) give identical per-task counts, lost counts and
     flight totals: a flight advances the position with the same rounding on
     every path, so the trajectory depends only on its Philox counter.  With
@@ -203,22 +204,22 @@ def test_cooperative_tail_takes_the_same_trajectories(name, cap):
     gb = A.GeomBuf(m)
     run = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=5, np_=257, seed=21, precision=A.PREC_FP32)
     out = {}
-    for key, opts in (("lane", dict(tune_flags=2)), ("coop", dict(coop_lanes=32)),
-                      ("tail", dict()), ("coop_nofast", dict(coop_lanes=32, tune_flags=1)),
-                      ("long", dict(coop_lanes=1, long_flights=16)), ("lane_nofast", dict(tune_flags=3))):
+    for key, opts in (("lane", dict(tune_flags=2)), ("coop8", dict(coop_lanes=8)),
+                      ("tail", dict()), ("coop_nofast", dict(tune_flags=1)),
+                      ("coop1", dict(coop_lanes=1)), ("lane_nofast", dict(tune_flags=3))):
         with A.Handle(gb.view, spec, max_flights=cap, **opts) as h:
             k = h.kappa(run, want_counts=True)
             out[key] = (k["counts"], k["lost"], h.stats())
     base_counts, base_lost, base_st = out["lane"]
     assert base_st["coop_rounds"] == 0
-    for key in ("coop", "tail", "coop_nofast", "long", "lane_nofast"):
+    for key in ("coop8", "tail", "coop_nofast", "coop1", "lane_nofast"):
         counts, lost, st = out[key]
         np.testing.assert_array_equal(counts, base_counts, err_msg=key)
         assert lost == base_lost, key
         assert st["flights"] == base_st["flights"], key
         assert st["max_traj_flights"] == base_st["max_traj_flights"], key
-    assert out["coop"][2]["coop_rounds"] > 0 and out["coop"][2]["coop_flights"] > 0
-    assert out["long"][2]["coop_rounds"] > 0
+    for key in ("tail", "coop8", "coop1"):
+        assert out[key][2]["coop_rounds"] > 0 and out[key][2]["coop_flights"] > 0, key
     if cap:
         assert base_lost > 0
 
