@@ -35,11 +35,13 @@
  *     together so that four independent chains fill the issue slots of a
  *     warp that is alone on its scheduler (the tail of a run); tallies are
  *     integer, aggregated per warp by task (match_any) before one atomic;
- *   - warp-cooperative tail: a warp left with few live phonons advances each
- *     of them 32 flights per round, one flight per lane, with the flights'
- *     start points summed in flight order; every path (fast, full,
- *     cooperative) moves the position with the same fma, so a trajectory is
- *     the same whichever path takes its flights.
+ *   - two phases: the drain phase runs the work queue one lane per phonon
+ *     and, once the queue is dry, hands its diffusive phonons to a tail list;
+ *     the tail phase (a second launch of the same kernel) gives each of them
+ *     a warp that advances it 32 flights per round, one flight per lane, with
+ *     the flights' start points summed in flight order; every path (fast,
+ *     full, cooperative) moves the position with the same fma, so a
+ *     trajectory is the same whichever path takes its flights.
  */
 #include <cuda_runtime.h>
 #include <math.h>
@@ -393,7 +395,10 @@ __device__ __forceinline__ void slab_exit(float px, float py, float pz, float dx
 }
 
 /* Lower bound of the distance from p to one candidate surface (planes bound
-   polygons from below, the infinite cylinder bounds the clipped one). */
+   polygons from below, the infinite cylinder bounds the clipped one).  The
+   square roots are the hardware approximation: its relative error (< 2^-22
+   of a distance below the box diagonal) is far inside the 4 eps the callers
+   take off, so the bound stays a bound. */
 template <bool EXT, class G_t>
 __device__ __forceinline__ float surface_lb(const G_t& G, int s, float px, float py, float pz) {
   const float4 A = G.hotA(s);
@@ -406,24 +411,25 @@ __device__ __forceinline__ float surface_lb(const G_t& G, int s, float px, float
     const float wx = px - A.x, wy = py - A.y, wz = pz - A.z;
     const float sa = fmaf(wx, E.x, fmaf(wy, E.y, wz * E.z));
     const float ux = fmaf(-sa, E.x, wx), uy = fmaf(-sa, E.y, wy), uz = fmaf(-sa, E.z, wz);
-    const float er = sqrtf(fmaf(ux, ux, fmaf(uy, uy, uz * uz))) - A.w;
+    const float er = sqrt_approx(fmaf(ux, ux, fmaf(uy, uy, uz * uz))) - A.w;
     const float ea = fabsf(sa) - E.w;
     return (er <= 0.0f && ea <= 0.0f) ? fminf(-er, -ea) : fmaxf(er, ea);
   }
   if (type == REC_SPHERE) {
     const float wx = px - A.x, wy = py - A.y, wz = pz - A.z;
-    return fabsf(sqrtf(fmaf(wx, wx, fmaf(wy, wy, wz * wz))) - A.w);
+    return fabsf(sqrt_approx(fmaf(wx, wx, fmaf(wy, wy, wz * wz))) - A.w);
   }
   const float wx = px - A.x, wy = py - A.y;
-  return fabsf(sqrtf(fmaf(wx, wx, wy * wy)) - A.z);
+  return fabsf(sqrt_approx(fmaf(wx, wx, wy * wy)) - A.z);
 }
 
-/* Distance from p to a node box (0 inside). */
+/* Distance from p to a node box (0 inside; approximate square root, as in
+   surface_lb). */
 __device__ __forceinline__ float box_dist(float4 lo, float4 hi, float px, float py, float pz) {
   const float ex = fmaxf(fmaxf(lo.x - px, px - hi.x), 0.0f);
   const float ey = fmaxf(fmaxf(lo.y - py, py - hi.y), 0.0f);
   const float ez = fmaxf(fmaxf(lo.z - pz, pz - hi.z), 0.0f);
-  return sqrtf(fmaf(ex, ex, fmaf(ey, ey, ez * ez)));
+  return sqrt_approx(fmaf(ex, ex, fmaf(ey, ey, ez * ez)));
 }
 
 /* BVH range query for the safe ball: the smallest lower bound of the
@@ -577,7 +583,7 @@ constexpr int kAdjSmemDoubles = 2048;
 
 /* rounds of 32 flights one cooperative visit may take before the phonon's
    lane returns to the refill / tally step */
-constexpr int kCoopRounds = 8;
+constexpr int kCoopRounds = 32;
 
 /* Kernel phases.  PH_DRAIN pulls (task, particle range) chunks from the
    work queue, one phonon per lane; once the queue is dry a warp holding at
@@ -614,11 +620,9 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   float flmax = r.fast_lambda_max;
   /* adjoint replay: per-block accumulators */
   __shared__ double adj_sh[MODE == MODE_ADJOINT ? kAdjSmemDoubles : 1];
-  /* cooperative rounds: per warp one row of 32 (free path, direction) and
-     one of 32 flight start points */
-  __shared__ float4 coop_rows[PH == PH_TAIL ? kBlock / 32 : 1][2][32];
-  float4* const wrow = coop_rows[PH == PH_TAIL ? (threadIdx.x >> 5) : 0][0];
-  float4* const qrow = coop_rows[PH == PH_TAIL ? (threadIdx.x >> 5) : 0][1];
+  /* cooperative rounds: per warp one row of 32 (free path, direction) */
+  __shared__ float4 coop_rows[PH == PH_TAIL ? kBlock / 32 : 1][32];
+  float4* const wrow = coop_rows[PH == PH_TAIL ? (threadIdx.x >> 5) : 0];
   /* ... and five rows where the lanes' own phonons wait during the rounds */
   __shared__ float4 coop_park[PH == PH_TAIL ? kBlock / 32 : 1][5][32];
   float4 (*const park)[32] = coop_park[PH == PH_TAIL ? (threadIdx.x >> 5) : 0];
@@ -834,17 +838,16 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
 
     int end_side = -1;  /* -1 still running, 0 lost, 1 x-, 2 x+ */
 
-    /* ---- warp-cooperative flights for the last few live lanes ----------
-       Once a warp holds at most coop_lanes live phonons (the tail of a run,
-       when only the longest diffusive trajectories are left), its 32 lanes
-       advance one phonon at a time, 32 flights per round: lane j draws the
-       Philox block of flight f+1+j, the start point of every flight is the
-       serial sum of the earlier flights (in their order, with the rounding
-       of the one-lane path), and each lane runs the full intersection test
-       of its own flight.  The first flight that hits a surface, leaves the
-       box or reaches the cap ends the round; the flights before it are p-p
-       events.  The hit flight's Philox block and nearest surface are handed
-       to the phonon's lane, which processes the event below. */
+    /* ---- tail phase: warp-cooperative flights for lane 0's phonon -------
+       The warp's 32 lanes advance the phonon 32 flights per round: lane j
+       draws the Philox block of flight f+1+j, the start point of every
+       flight is the serial sum of the earlier flights (in their order, with
+       the rounding of the one-lane path), and each lane runs the full
+       intersection test of its own flight unless the flight stays in the
+       safe ball.  The first flight that hits a surface, leaves the box or
+       reaches the cap ends the round; the flights before it are p-p events.
+       The hit flight's Philox block and nearest surface are handed to the
+       phonon's lane, which processes the event below. */
     bool coop = false;       /* this lane was advanced cooperatively          */
     bool pre = false;        /* ... up to a surface hit: preR / pre_tb / pre_sb */
     bool skip_full = false;  /* ... up to the round limit: no event this pass  */
@@ -902,17 +905,17 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
                the warp's row of shared memory holds (free path, direction)
                of flights 1..31 of the round.  The start point of flight j
                is the chain p, fma(fp_0, d_0, p), ... after j steps, the same
-               for every lane: the warp runs the chain once (flight 0's step
+               for every lane: each lane runs the whole chain (flight 0's step
                from registers, the others from broadcast loads issued eight
-               at a time ahead of their fmas), stores every step to a second
-               row, and each lane reads its own start point back */
+               at a time ahead of their fmas) and keeps step j with a select */
             if (lane < 31) wrow[lane + 1] = make_float4(nf, nx, ny, nz);
             __syncwarp();
             const float4 mine = lane == 0 ? make_float4(cfp, cdx, cdy, cdz) : wrow[lane];
             const float sfp = mine.x, sdx = mine.y, sdy = mine.z, sdz = mine.w;
+            float qx = cpx, qy = cpy, qz = cpz;
             {
               float ax = fmaf(cfp, cdx, cpx), ay = fmaf(cfp, cdy, cpy), az = fmaf(cfp, cdz, cpz);
-              qrow[1] = make_float4(ax, ay, az, 0.0f);
+              qx = lane == 1 ? ax : qx; qy = lane == 1 ? ay : qy; qz = lane == 1 ? az : qz;
 #pragma unroll
               for (int b = 1; b < 31; b += 8) {
                 float4 v[8];
@@ -925,16 +928,13 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
                     ax = fmaf(v[k].x, v[k].y, ax);
                     ay = fmaf(v[k].x, v[k].z, ay);
                     az = fmaf(v[k].x, v[k].w, az);
-                    qrow[b + k + 1] = make_float4(ax, ay, az, 0.0f);
+                    const bool me = lane == b + k + 1;
+                    qx = me ? ax : qx; qy = me ? ay : qy; qz = me ? az : qz;
                   }
                 }
               }
             }
-            __syncwarp();
-            const float4 qs = qrow[lane];
-            const float qx = lane == 0 ? cpx : qs.x, qy = lane == 0 ? cpy : qs.y;
-            const float qz = lane == 0 ? cpz : qs.z;
-            __syncwarp();  /* the next round rewrites both rows */
+            __syncwarp();  /* the next round rewrites the row */
             const bool inbox = qx >= -eps && qx <= X + eps && qy >= -eps && qy <= Y + eps &&
                                qz >= -eps && qz <= Z + eps;
             const bool capd = (unsigned long long)cfl + (unsigned)lane >= r.max_flights;
