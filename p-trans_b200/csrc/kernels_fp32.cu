@@ -1357,11 +1357,23 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
 
 }  // namespace
 
+/* Static shared memory (the adjoint accumulators, the cooperative rows) plus
+   the staged blob can pass the 48 KB a launch gets without opting in, so
+   every launch with a staged blob opts in to its dynamic size. */
+template <int MODE, bool EXT, int PH>
+cudaError_t allow_dynamic_smem(size_t smem) {
+  return cudaFuncSetAttribute(k_persistent<true, MODE, false, EXT, PH>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
 template <int MODE, bool EXT, int PH>
 cudaError_t occupancy_mode(int block, size_t smem, int* bps) {
-  if (smem > 0)
+  if (smem > 0) {
+    cudaError_t e = allow_dynamic_smem<MODE, EXT, PH>(smem);
+    if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
         bps, k_persistent<true, MODE, false, EXT, PH>, block, smem);
+  }
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
       bps, k_persistent<false, MODE, false, EXT, PH>, block, 0);
 }
@@ -1370,11 +1382,8 @@ template <int MODE, bool EXT, int PH>
 cudaError_t launch_mode(const GeoF32& g, const RunF32& r, int grid, int block, size_t smem,
                         cudaStream_t st) {
   if (g.stage_smem && smem > 0) {
-    if (smem > 48 * 1024) {
-      cudaError_t e = cudaFuncSetAttribute(k_persistent<true, MODE, false, EXT, PH>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-    }
+    cudaError_t e = allow_dynamic_smem<MODE, EXT, PH>(smem);
+    if (e != cudaSuccess) return e;
     k_persistent<true, MODE, false, EXT, PH><<<grid, block, smem, st>>>(g, r);
   } else {
     k_persistent<false, MODE, false, EXT, PH><<<grid, block, 0, st>>>(g, r);

@@ -153,3 +153,22 @@ def test_adjoint_capped_cylinders_matches_finite_differences():
     mf, sf = _mean_se(fd)
     assert abs(ma - mf) < 3.5 * math.hypot(sa, sf), (ma, sa, mf, sf)
     assert abs(ma) > 3 * sa
+
+
+def test_adjoint_with_a_blob_past_the_default_shared_memory():
+    """A staged geometry blob of tens of KB plus the adjoint kernels' static
+    shared memory (accumulators, cooperative rows) passes the 48 KB a launch
+    gets without opting in: both passes still launch, replay every
+    transmitted sample and reproduce the forward kappa."""
+    model = synth.spheres_cylinders_box(n_spheres=150, n_cylinders=30, l=1000.0, seed=2,
+                                        r_sphere=(15.0, 40.0), r_cylinder=15.0, length=(60.0, 160.0))
+    spec = synth.spectrum(10, seed=3, mfp_lo=2e-9, mfp_hi=1e-6)
+    gb = A.GeomBuf(model)
+    run = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=5, np_=200, seed=4)
+    with A.Handle(gb.view, spec) as h:
+        a = h.adjoint(run)
+        k = h.kappa(run, want_counts=True)
+    assert a["replayed"] == int(k["counts"].sum()) > 0
+    assert a["mismatched"] == 0
+    assert a["kappa"] == pytest.approx(k["kappa"], rel=1e-12)
+    assert np.all(np.isfinite(a["dk_dp"][~np.isnan(a["dk_dp"])]))
