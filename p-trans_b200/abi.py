@@ -119,6 +119,8 @@ class PtgStats(C.Structure):
         ("full_flights", C.c_uint64), ("safe_balls", C.c_uint64),
         ("coop_rounds", C.c_uint64), ("coop_flights", C.c_uint64),
         ("box_tests", C.c_uint64), ("surface_tests", C.c_uint64),
+        ("drain_kernel_ms", C.c_double), ("tail_kernel_ms", C.c_double),
+        ("tail_phonons", C.c_uint64), ("tail_flights", C.c_uint64),
     ]
 
 

@@ -59,7 +59,9 @@ struct ptg_handle {
   int device = 0;
   int num_sms = 0;
   cudaStream_t stream = nullptr;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  /* 0/1 around the transport, 2/3 around the reduction, 4 between the
+     drain and tail kernels */
+  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   ptg_options opt;
   ptg::GeomSoA geom;
   ptg::SpecSoA spec;
@@ -84,6 +86,8 @@ struct ptg_handle {
   /* trace replay: position offsets, counts, exit sides, positions */
   DevBuf tr_off, tr_npos, tr_end, tr_pos;
   unsigned long long list_n = 0, mismatch = 0;
+  bool fp32_split = false;  /* the last transport was the FP32 drain (+ tail) */
+  int tail_cap = 0;          /* its tail-list capacity (0: no tail phase)       */
   ~ptg_handle() {
     for (DevBuf* b : owned) { b->release(); delete b; }
     DevBuf* all[] = {&blob, &task, &chunk, &counts, &lost, &stats, &queue, &red_coef, &red_K,
@@ -431,11 +435,11 @@ int run_transport(ptg_handle* h, const Transport& T) {
   CU(cudaSetDevice(h->device));
   CU(h->counts.ensure(sizeof(unsigned long long) * ntask));
   CU(h->lost.ensure(sizeof(unsigned long long) * ntask));
-  CU(h->stats.ensure(sizeof(unsigned long long) * 16));
+  CU(h->stats.ensure(sizeof(unsigned long long) * ptg::kStatSlots));
   CU(h->queue.ensure(sizeof(int) * 4));
   CU(cudaMemsetAsync(h->counts.p, 0, sizeof(unsigned long long) * ntask, h->stream));
   CU(cudaMemsetAsync(h->lost.p, 0, sizeof(unsigned long long) * ntask, h->stream));
-  CU(cudaMemsetAsync(h->stats.p, 0, sizeof(unsigned long long) * 16, h->stream));
+  CU(cudaMemsetAsync(h->stats.p, 0, sizeof(unsigned long long) * ptg::kStatSlots, h->stream));
   /* stats[5], stats[6] collect minima of the global timer */
   CU(cudaMemsetAsync(h->stats.as<unsigned long long>() + 5, 0xFF, sizeof(unsigned long long) * 2,
                      h->stream));
@@ -477,6 +481,7 @@ int run_transport(ptg_handle* h, const Transport& T) {
     h->last.grid = grid;
     h->last.block = block;
     h->last.launches = 1;
+    h->fp32_split = false;
   } else {
     std::vector<float4> t32(ntask);
     std::vector<int64_t> order;
@@ -574,18 +579,21 @@ int run_transport(ptg_handle* h, const Transport& T) {
                                                                                    : r.nchunk > 0;
     if (work) {
       CU(ptg::launch_persistent_fp32(h->g32, r, grid, block, smem, h->stream, T.mode));
+      CU(cudaEventRecord(h->ev[4], h->stream));
       if (tail) CU(ptg::launch_tail_fp32(h->g32, r, tgrid, block, smem, h->stream, T.mode));
     }
     CU(cudaEventRecord(h->ev[1], h->stream));
     h->last.grid = grid;
     h->last.block = block;
     h->last.launches = work ? (tail ? 2 : 1) : 0;
+    h->fp32_split = work;
+    h->tail_cap = tail ? r.tail_cap : 0;
   }
   return PTG_OK;
 }
 
 int finish_stats(ptg_handle* h) {
-  unsigned long long st[16];
+  unsigned long long st[ptg::kStatSlots];
   int qerr[4];
   CU(cudaMemcpyAsync(st, h->stats.p, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
   CU(cudaMemcpyAsync(qerr, h->queue.p, sizeof(qerr), cudaMemcpyDeviceToHost, h->stream));
@@ -605,6 +613,16 @@ int finish_stats(ptg_handle* h) {
   h->last.coop_flights = st[13];
   h->last.box_tests = st[14];
   h->last.surface_tests = st[15];
+  h->last.drain_kernel_ms = h->last.tail_kernel_ms = 0.0;
+  h->last.tail_phonons = h->last.tail_flights = 0;
+  if (h->fp32_split) {
+    float dms = 0.f;
+    CU(cudaEventElapsedTime(&dms, h->ev[0], h->ev[4]));
+    h->last.drain_kernel_ms = dms;
+    h->last.tail_kernel_ms = ms - dms;
+    h->last.tail_phonons = (uint64_t)std::max(0, std::min(qerr[2], h->tail_cap));
+    h->last.tail_flights = st[17] >= st[16] ? st[17] - st[16] : 0;
+  }
   h->list_n = st[10];
   h->mismatch = st[11];
   if (st[5] != ~0ull && st[7] >= st[5]) {

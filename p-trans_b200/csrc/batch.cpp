@@ -197,7 +197,7 @@ extern "C" int ptg_batch_create(const ptg_batch_item* items, int32_t nitems,
   BCU(b->chunks.alloc(sizeof(int4) * (chunks.size() + 1)));
   BCU(b->counts.alloc(sizeof(unsigned long long) * ntot));
   BCU(b->lost.alloc(sizeof(unsigned long long) * ntot));
-  BCU(b->stats.alloc(sizeof(unsigned long long) * 16));
+  BCU(b->stats.alloc(sizeof(unsigned long long) * ptg::kStatSlots));
   BCU(b->queue.alloc(sizeof(int) * 4));
   BCU(b->coef.alloc(sizeof(double) * coef.size()));
   BCU(b->K.alloc(sizeof(double) * nm));
@@ -292,7 +292,8 @@ extern "C" int ptg_batch_create(const ptg_batch_item* items, int32_t nitems,
   BCU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
   cudaError_t ce = cudaMemsetAsync(b->counts.p, 0, sizeof(unsigned long long) * ntot, b->stream);
   if (ce == cudaSuccess) ce = cudaMemsetAsync(b->lost.p, 0, sizeof(unsigned long long) * ntot, b->stream);
-  if (ce == cudaSuccess) ce = cudaMemsetAsync(dstats, 0, sizeof(unsigned long long) * 16, b->stream);
+  if (ce == cudaSuccess)
+    ce = cudaMemsetAsync(dstats, 0, sizeof(unsigned long long) * ptg::kStatSlots, b->stream);
   if (ce == cudaSuccess) ce = cudaMemsetAsync(dstats + 5, 0xFF, sizeof(unsigned long long) * 2, b->stream);
   if (ce == cudaSuccess) ce = cudaMemsetAsync(b->queue.p, 0, sizeof(int) * 4, b->stream);
   if (ce == cudaSuccess && r.nchunk > 0) ce = ptg::launch_persistent_batch(r, b->launch_grid, 256, b->stream, b->bvh);

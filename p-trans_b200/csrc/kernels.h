@@ -163,6 +163,14 @@ struct RunF32 {
   const int* task_geo;
 };
 
+/* u64 statistics slots of a transport launch: 0 flights, 1 lost, 2 capped,
+   3 samples, 4 longest trajectory, 5-7 globaltimer start / queue dry / end,
+   8 full-test flights, 9 safe balls, 10 listed samples, 11 replay
+   mismatches, 12 cooperative rounds, 13 cooperative flights, 14 BVH boxes,
+   15 surfaces tested, 16 flights of phonons handed to the tail phase before
+   the hand-over, 17 flights of phonons that ended in the tail phase. */
+constexpr int kStatSlots = 24;
+
 /* Replays are split in this many interleaved batches (sample % kAdjBatches)
    whose spread gives the standard error of the adjoint estimates. */
 constexpr int kAdjBatches = 8;

@@ -830,6 +830,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
                              gr2);
           if (MODE == MODE_ADJOINT)
             e[5] = make_float4(adj_w, adj_len, __uint_as_float(adj_npp), __int_as_float(adj_b));
+          atomicAdd(r.stats + 16, (unsigned long long)flight);
           alive = false;
         }
         if (!__any_sync(FULL, alive)) break;
@@ -1336,6 +1337,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   }
   if (lane == 0) {
     if (v0) atomicAdd(r.stats + 0, v0);
+    if (PH == PH_TAIL && v0) atomicAdd(r.stats + 17, v0);
     if (v1) atomicAdd(r.stats + 1, v1);
     if (v2) atomicAdd(r.stats + 2, v2);
     if (v3) atomicAdd(r.stats + 3, v3);

@@ -39,7 +39,8 @@ constexpr int64_t kMaxChunks = PTG_NOALLOC_MAX_CHUNKS;
 constexpr int kMaxAngles = 64;
 
 /* layout of the scratch array, byte offsets (all 256-byte aligned) */
-constexpr size_t kOffStats = 0;                                /* u64[16]       */
+constexpr size_t kOffStats = 0;                                /* u64[kStatSlots] */
+static_assert(ptg::kStatSlots * 8 <= 256, "stats region");
 constexpr size_t kOffQueue = 256;                              /* int[4]        */
 constexpr size_t kOffCounts = 512;                             /* u64[tasks]    */
 constexpr size_t kOffLost = kOffCounts + 8 * kMaxTasks;        /* u64[tasks]    */
@@ -136,7 +137,7 @@ extern "C" int ptg_transmission_noalloc(ptg_handle* h, double mfp_nm, int32_t na
   unsigned long long* counts = reinterpret_cast<unsigned long long*>(base + kOffCounts);
   unsigned long long* lost = reinterpret_cast<unsigned long long*>(base + kOffLost);
   /* clear what the kernel accumulates into; the tables are rewritten */
-  if (cudaMemsetAsync(stats, 0, 16 * sizeof(unsigned long long), s) != cudaSuccess ||
+  if (cudaMemsetAsync(stats, 0, ptg::kStatSlots * sizeof(unsigned long long), s) != cudaSuccess ||
       cudaMemsetAsync(stats + 5, 0xFF, 2 * sizeof(unsigned long long), s) != cudaSuccess ||
       cudaMemsetAsync(queue, 0, 4 * sizeof(int), s) != cudaSuccess ||
       cudaMemsetAsync(counts, 0, sizeof(unsigned long long) * ntask, s) != cudaSuccess ||
