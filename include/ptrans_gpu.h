@@ -180,7 +180,7 @@ typedef struct ptg_options {
   int32_t device;           /* CUDA device ordinal                              */
   int32_t block_size;       /* persistent kernel threads per block (0 = tuned)  */
   int32_t blocks_per_sm;    /* persistent kernel residency (0 = occupancy)      */
-  int32_t regen_threshold;  /* idle lanes before a warp refills (0 = 1)         */
+  int32_t regen_threshold;  /* idle lanes before a warp refills (0 = 2)         */
   int32_t ref_quirks;       /* 1: a lost phonon also counts as transmitted      */
                             /*    (src/RTMCphon.f90:1701 then :1833)            */
   int32_t bvh_leaf;         /* BVH leaf size (0 = tuned, < 0 = no BVH): grains  */
@@ -192,7 +192,9 @@ typedef struct ptg_options {
                             /*   bit 0: no safe-distance p-p fast path          */
                             /*   bit 1: no tail phase (one lane per phonon to   */
                             /*          the end)                                */
-  int32_t fast_steps;       /* fast p-p flights per iteration (0 = tuned)       */
+  int32_t fast_steps;       /* fast p-p flights per iteration before a warp     */
+                            /* goes on only while half its lanes still can      */
+                            /* (at most 4x; 0 = 8)                              */
   int32_t coop_lanes;       /* once the work queue is dry, a warp with at most  */
                             /* this many live phonons hands its diffusive ones  */
                             /* to the tail phase, a second kernel that gives    */

@@ -244,9 +244,9 @@ extern "C" int ptg_batch_create(const ptg_batch_item* items, int32_t nitems,
   const int64_t maxf = o.max_flights > 0 ? o.max_flights : 10000000LL;
   r.max_flights = (uint32_t)std::min<int64_t>(maxf, 4294967295LL);
   r.ref_quirks = o.ref_quirks;
-  const int rt = o.regen_threshold;
-  r.regen_threshold = rt < 1 ? 1 : (rt > 32 ? 32 : rt);
-  r.fast_steps = (o.tune_flags & 1) ? 0 : (o.fast_steps > 0 ? o.fast_steps : 16);
+  const int rt = o.regen_threshold > 0 ? o.regen_threshold : ptg::kDefaultRegen;
+  r.regen_threshold = rt > 32 ? 32 : rt;
+  r.fast_steps = (o.tune_flags & 1) ? 0 : (o.fast_steps > 0 ? o.fast_steps : ptg::kDefaultFastSteps);
   r.counts = b->counts.as<unsigned long long>();
   r.lost = b->lost.as<unsigned long long>();
   r.stats = b->stats.as<unsigned long long>();

@@ -171,6 +171,12 @@ struct RunF32 {
    the hand-over, 17 flights of phonons that ended in the tail phase. */
 constexpr int kStatSlots = 24;
 
+/* Scheduling defaults of the persistent kernel (ptg_options 0 = these):
+   idle lanes before a warp refills, fast-path flights per lane and
+   iteration. */
+constexpr int kDefaultRegen = 2;
+constexpr int kDefaultFastSteps = 8;
+
 /* Replays are split in this many interleaved batches (sample % kAdjBatches)
    whose spread gives the standard error of the adjoint estimates. */
 constexpr int kAdjBatches = 8;

@@ -1040,15 +1040,28 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
       }
     }
 
-    if (alive) {
+    bool paused = false;  /* stopped by the step limit while still in its ball */
+    {
       /* ---- safe-ball p-p flights: the segment to the next p-p point stays
          inside the safe ball (convex), so no surface is crossed.  Four
          flights at a time: their Philox blocks, new directions and free
          paths do not depend on the phonon state and are computed together;
-         only the position / ball test chain is serial. ---- */
-      int k = 0;
-      bool fast_more = MODE != MODE_TRACE && br2 > 0.0f && !coop;
-      while (fast_more && k < r.fast_steps && flight + 4u <= r.max_flights) {
+         only the position / ball test chain is serial.  Every lane takes
+         part in the loop control (the ballots): past fast_steps flights the
+         warp goes on only while at least half of its live lanes are still in
+         their balls, and never past 4 x fast_steps, so a few lanes deep in
+         large balls do not hold the others' full flights back. ---- */
+      bool fast_more = alive && MODE != MODE_TRACE && br2 > 0.0f && !coop;
+      const int nalive = __popc(__ballot_sync(FULL, alive));
+      for (int g = 0;; g += 4) {
+        const bool go = fast_more && flight + 4u <= r.max_flights;
+        const unsigned gm = __ballot_sync(FULL, go);
+        if (!gm) break;
+        if (g >= r.fast_steps && (g >= 4 * r.fast_steps || 2 * __popc(gm) < nalive)) {
+          paused = go;
+          break;
+        }
+        if (!go) continue;
         uint4 B[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) B[j] = philox10(flight + 1u + j, c1, slo, shi, key);
@@ -1078,16 +1091,17 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             adj_npp += acc ? 1u : 0u;
           }
           flight += acc ? 1u : 0u;
-          k += acc ? 1 : 0;
           px = acc ? qx : px; py = acc ? qy : py; pz = acc ? qz : pz;
           dx = acc ? nx[j] : dx; dy = acc ? ny[j] : dy; dz = acc ? nz[j] : dz;
           fp = acc ? nf[j] : fp;
           fast_more = acc;
         }
       }
-      /* a lane that used up its fast steps waits for the next iteration;
-         any other lane takes one flight with the full test now */
-      if (!(fast_more && k >= r.fast_steps) && !skip_full) {
+    }
+    if (alive) {
+      /* a lane paused in its ball waits for the next iteration; any other
+         lane takes one flight with the full test now */
+      if (!paused && !skip_full) {
         /* ---- one free flight with the intersection test (already run by
            the cooperative round when it handed over a hit) -------------- */
         bool go = false;

@@ -162,9 +162,9 @@ extern "C" int ptg_transmission_noalloc(ptg_handle* h, double mfp_nm, int32_t na
   const int64_t maxf = v.opt.max_flights > 0 ? v.opt.max_flights : 10000000LL;
   r.max_flights = (uint32_t)(maxf < 4294967295LL ? maxf : 4294967295LL);
   r.ref_quirks = v.opt.ref_quirks;
-  const int rt = v.opt.regen_threshold;
-  r.regen_threshold = rt < 1 ? 1 : (rt > 32 ? 32 : rt);
-  r.fast_steps = (v.opt.tune_flags & 1) ? 0 : (v.opt.fast_steps > 0 ? v.opt.fast_steps : 16);
+  const int rt = v.opt.regen_threshold > 0 ? v.opt.regen_threshold : ptg::kDefaultRegen;
+  r.regen_threshold = rt > 32 ? 32 : rt;
+  r.fast_steps = (v.opt.tune_flags & 1) ? 0 : (v.opt.fast_steps > 0 ? v.opt.fast_steps : ptg::kDefaultFastSteps);
   const double lmin = fmin(v.geom->box[0], fmin(v.geom->box[1], v.geom->box[2]));
   r.fast_lambda_max = (float)(0.1 * lmin);
   r.counts = counts;

@@ -17,7 +17,7 @@
  *   block_size      128 256
  *   blocks_per_sm   1 2
  *   coop_lanes      4 8 16 32
- *   fast_steps      8 16 32
+ *   fast_steps      4 8 16
  *   regen_threshold 1 2 4 8
  *   chunk           32 64 128
  */
@@ -68,7 +68,7 @@ extern "C" int ptg_autotune(ptg_handle* h, const ptg_run* run, int32_t reps, ptg
   params.push_back({&ptg_options::block_size, nullptr, {128, 256}});
   params.push_back({&ptg_options::blocks_per_sm, nullptr, {1, 2}});
   params.push_back({&ptg_options::coop_lanes, nullptr, {4, 8, 16, 32}});
-  params.push_back({&ptg_options::fast_steps, nullptr, {8, 16, 32}});
+  params.push_back({&ptg_options::fast_steps, nullptr, {4, 8, 16}});
   params.push_back({&ptg_options::regen_threshold, nullptr, {1, 2, 4, 8}});
   params.push_back({nullptr, &ptg_options::chunk, {32, 64, 128}});
 
