@@ -833,7 +833,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           atomicAdd(r.stats + 16, (unsigned long long)flight);
           alive = false;
         }
-        if (!__any_sync(FULL, alive)) break;
+        if (!__any_sync(FULL, alive)) {
+          if (queue_done) break;
+          continue;
+        }
       }
     }
 
