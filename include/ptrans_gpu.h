@@ -481,9 +481,10 @@ int ptg_autotune(ptg_handle* h, const ptg_run* run, int32_t reps, ptg_options* b
  * front by another framework, or a service that must keep a fixed
  * footprint).  It computes what ptg_transmission computes with
  * PTG_PREC_FP32 (same counts, so the same transmit array) but allocates no
- * device or host memory: the kernel's scratch (work-queue counter,
- * statistics, tallies, task and chunk tables) lives in one static device
- * array of fixed size that every GPU loading the library keeps until exit,
+ * device or host memory: the kernels' scratch (work-queue counter,
+ * statistics, tallies, task and chunk tables, a 65536-phonon tail-phase
+ * list) lives in one static device array of fixed size (about 8 MB) that
+ * every GPU loading the library keeps until exit,
  * and the caller's transmit array receives the counts before they are
  * divided by np in place.  Limits: nbranch*nkpoint*(nangle-1) <=
  * PTG_NOALLOC_MAX_TASKS, nangle <= 64; larger runs return PTG_ERR_INVALID.

@@ -436,14 +436,14 @@ int run_transport(ptg_handle* h, const Transport& T) {
   CU(h->counts.ensure(sizeof(unsigned long long) * ntask));
   CU(h->lost.ensure(sizeof(unsigned long long) * ntask));
   CU(h->stats.ensure(sizeof(unsigned long long) * ptg::kStatSlots));
-  CU(h->queue.ensure(sizeof(int) * 4));
+  CU(h->queue.ensure(sizeof(int) * 8));
   CU(cudaMemsetAsync(h->counts.p, 0, sizeof(unsigned long long) * ntask, h->stream));
   CU(cudaMemsetAsync(h->lost.p, 0, sizeof(unsigned long long) * ntask, h->stream));
   CU(cudaMemsetAsync(h->stats.p, 0, sizeof(unsigned long long) * ptg::kStatSlots, h->stream));
   /* stats[5], stats[6] collect minima of the global timer */
   CU(cudaMemsetAsync(h->stats.as<unsigned long long>() + 5, 0xFF, sizeof(unsigned long long) * 2,
                      h->stream));
-  CU(cudaMemsetAsync(h->queue.p, 0, sizeof(int) * 4, h->stream));
+  CU(cudaMemsetAsync(h->queue.p, 0, sizeof(int) * 8, h->stream));
   const int64_t maxf = h->opt.max_flights > 0 ? h->opt.max_flights : 10000000LL;
   memset(&h->last, 0, sizeof(h->last));
   if (T.precision == PTG_PREC_FP64) {
@@ -598,7 +598,7 @@ int run_transport(ptg_handle* h, const Transport& T) {
 
 int finish_stats(ptg_handle* h) {
   unsigned long long st[ptg::kStatSlots];
-  int qerr[4];
+  int qerr[8];
   CU(cudaMemcpyAsync(st, h->stats.p, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
   CU(cudaMemcpyAsync(qerr, h->queue.p, sizeof(qerr), cudaMemcpyDeviceToHost, h->stream));
   CU(cudaStreamSynchronize(h->stream));
@@ -624,7 +624,8 @@ int finish_stats(ptg_handle* h) {
     CU(cudaEventElapsedTime(&dms, h->ev[0], h->ev[4]));
     h->last.drain_kernel_ms = dms;
     h->last.tail_kernel_ms = ms - dms;
-    h->last.tail_phonons = (uint64_t)std::max(0, std::min(qerr[2], h->tail_cap));
+    h->last.tail_phonons =
+        (uint64_t)std::max(0, std::min(qerr[2], h->tail_cap) + std::min(qerr[4], h->tail_cap));
     h->last.tail_flights = st[17] >= st[16] ? st[17] - st[16] : 0;
   }
   h->list_n = st[10];

@@ -142,8 +142,9 @@ struct RunF32 {
      t_start (min), t_drain (min), t_end (max) in globaltimer ns,
      flights taken with the intersection test, safe balls built */
   unsigned long long* stats;
-  int* queue;                 /* [0] next chunk, [1] error flags, [2] phonons put
-                                 in the tail list, [3] next tail-list phonon */
+  int* queue;                 /* [0] next chunk, [1] error flags, [2] / [4] phonons
+                                 put at the front / back of the tail list, [3]
+                                 next tail-list phonon (8 ints) */
   /* adjoint support */
   unsigned long long* tlist;  /* mode 1: sample ids of transmitted phonons         */
   unsigned long long tlist_cap;

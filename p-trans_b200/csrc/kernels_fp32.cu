@@ -595,6 +595,11 @@ constexpr int kCoopRounds = 32;
 enum { PH_DRAIN = 0, PH_TAIL = 1 };
 /* float4 per phonon in the tail list */
 constexpr int kTailUnits = 6;
+/* A phonon handed over past this many flights goes to the front of the tail
+   list, which the tail phase takes first, the others to the back: a phonon
+   that has lasted long is the likeliest to last longer, and the tail ends
+   when its longest trajectory does. */
+constexpr uint32_t kTailLong = 8192;
 
 /* safe-ball radius searched in a grain with a BVH, in units of the MFP: a
    walk needs about (radius / MFP)^2 flights to leave the ball */
@@ -626,8 +631,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   /* ... and five rows where the lanes' own phonons wait during the rounds */
   __shared__ float4 coop_park[PH == PH_TAIL ? kBlock / 32 : 1][5][32];
   float4 (*const park)[32] = coop_park[PH == PH_TAIL ? (threadIdx.x >> 5) : 0];
-  /* tail phase: phonons the drain left (the count is final at launch) */
-  const int ntail = PH == PH_TAIL ? min(r.queue[2], r.tail_cap) : 0;
+  /* tail phase: phonons the drain left (the counts are final at launch),
+     long ones from the front of the list, the others from the back */
+  const int nlong = PH == PH_TAIL ? min(r.queue[2], r.tail_cap) : 0;
+  const int ntail = PH == PH_TAIL ? nlong + min(r.queue[4], r.tail_cap - nlong) : 0;
   const int adj_stride = r.nsurf + 1;
   const bool adj_in_smem = (MODE == MODE_ADJOINT) && kAdjBatches * adj_stride <= kAdjSmemDoubles;
   if (MODE == MODE_ADJOINT && adj_in_smem) {
@@ -667,7 +674,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
       if (c >= ntail) {
         queue_done = true;
       } else if (lane == 0) {
-        const float4* e = r.tail + (size_t)kTailUnits * c;
+        const int slot = c < nlong ? c : r.tail_cap - 1 - (c - nlong);
+        const float4* e = r.tail + (size_t)kTailUnits * slot;
         const float4 e0 = e[0], e1 = e[1], e2 = e[2], e3 = e[3], e4 = e[4];
         px = e0.x; py = e0.y; pz = e0.z; dx = e0.w;
         dy = e1.x; dz = e1.y; fp = e1.z; lam = e1.w;
@@ -813,13 +821,22 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
         __popc(__ballot_sync(FULL, alive)) <= r.coop_lanes) {
       const unsigned mv = __ballot_sync(FULL, alive && lam < flmax);
       if (mv) {
-        const int first = __ffs(mv) - 1;
-        int base = 0;
-        if (lane == first) base = atomicAdd(r.queue + 2, __popc(mv));
-        base = __shfl_sync(FULL, base, first);
-        const int slot = base + __popc(mv & lanemask_lt());
+        /* long phonons fill the list from the front, the others from the
+           back; a lane hands over at most one phonon, so the two never meet
+           in a list with a slot per lane */
+        const unsigned ml = mv & __ballot_sync(FULL, flight >= kTailLong);
+        const unsigned ms = mv & ~ml;
+        const int fl = ml ? __ffs(ml) - 1 : 0, fs = ms ? __ffs(ms) - 1 : 0;
+        int bl = 0, bs = 0;
+        if (ml && lane == fl) bl = atomicAdd(r.queue + 2, __popc(ml));
+        if (ms && lane == fs) bs = atomicAdd(r.queue + 4, __popc(ms));
+        bl = __shfl_sync(FULL, bl, fl);
+        bs = __shfl_sync(FULL, bs, fs);
+        const bool lng = (ml >> lane) & 1u;
+        const int idx = lng ? bl + __popc(ml & lanemask_lt()) : bs + __popc(ms & lanemask_lt());
+        const int slot = lng ? idx : r.tail_cap - 1 - idx;
         /* past the list's capacity a phonon stays here */
-        if (((mv >> lane) & 1u) && slot < r.tail_cap) {
+        if (((mv >> lane) & 1u) && idx < r.tail_cap && slot >= 0 && slot < r.tail_cap) {
           float4* e = r.tail + (size_t)kTailUnits * slot;
           e[0] = make_float4(px, py, pz, dx);
           e[1] = make_float4(dy, dz, fp, lam);

@@ -8,9 +8,10 @@
  * (a fixed budget carved out at start-up), or a long-running service that
  * must not grow or fragment its footprint between requests.  For them the
  * kernel's scratch memory (work-queue counter, statistics, per-task tallies,
- * task and chunk tables) lives in one fixed static device array,
- * g_noalloc_scratch, sized for PTG_NOALLOC_MAX_TASKS tasks and
- * PTG_NOALLOC_MAX_CHUNKS work chunks.  Every GPU that loads the library holds
+ * task and chunk tables, the tail-phase list) lives in one fixed static
+ * device array, g_noalloc_scratch, sized for PTG_NOALLOC_MAX_TASKS tasks,
+ * PTG_NOALLOC_MAX_CHUNKS work chunks and kMaxTail handed-over phonons (a
+ * phonon past that capacity stays in the drain phase).  Every GPU that loads the library holds
  * the array until the process exits.
  *
  * Rules of use:
@@ -27,6 +28,7 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "kernels.h"
@@ -37,17 +39,19 @@ namespace {
 constexpr int64_t kMaxTasks = PTG_NOALLOC_MAX_TASKS;
 constexpr int64_t kMaxChunks = PTG_NOALLOC_MAX_CHUNKS;
 constexpr int kMaxAngles = 64;
+constexpr int kMaxTail = 65536;   /* tail-list phonons, 96 B each */
 
 /* layout of the scratch array, byte offsets (all 256-byte aligned) */
 constexpr size_t kOffStats = 0;                                /* u64[kStatSlots] */
 static_assert(ptg::kStatSlots * 8 <= 256, "stats region");
-constexpr size_t kOffQueue = 256;                              /* int[4]        */
+constexpr size_t kOffQueue = 256;                              /* int[8]        */
 constexpr size_t kOffCounts = 512;                             /* u64[tasks]    */
 constexpr size_t kOffLost = kOffCounts + 8 * kMaxTasks;        /* u64[tasks]    */
 constexpr size_t kOffTasks = kOffLost + 8 * kMaxTasks;         /* float4[tasks] */
 constexpr size_t kOffOmega = kOffTasks + 16 * kMaxTasks;       /* double[tasks] */
 constexpr size_t kOffChunks = kOffOmega + 8 * kMaxTasks;       /* int4[chunks]  */
-constexpr size_t kScratchBytes = kOffChunks + 16 * kMaxChunks;
+constexpr size_t kOffTail = kOffChunks + 16 * kMaxChunks;     /* float4[6 * tail] */
+constexpr size_t kScratchBytes = kOffTail + 96 * (size_t)kMaxTail;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
@@ -139,7 +143,7 @@ extern "C" int ptg_transmission_noalloc(ptg_handle* h, double mfp_nm, int32_t na
   /* clear what the kernel accumulates into; the tables are rewritten */
   if (cudaMemsetAsync(stats, 0, ptg::kStatSlots * sizeof(unsigned long long), s) != cudaSuccess ||
       cudaMemsetAsync(stats + 5, 0xFF, 2 * sizeof(unsigned long long), s) != cudaSuccess ||
-      cudaMemsetAsync(queue, 0, 4 * sizeof(int), s) != cudaSuccess ||
+      cudaMemsetAsync(queue, 0, 8 * sizeof(int), s) != cudaSuccess ||
       cudaMemsetAsync(counts, 0, sizeof(unsigned long long) * ntask, s) != cudaSuccess ||
       cudaMemsetAsync(lost, 0, sizeof(unsigned long long) * ntask, s) != cudaSuccess ||
       cudaMemcpyAsync(base + kOffOmega, v.spec->omega.data(), sizeof(double) * nmode,
@@ -171,6 +175,8 @@ extern "C" int ptg_transmission_noalloc(ptg_handle* h, double mfp_nm, int32_t na
   r.lost = lost;
   r.stats = stats;
   r.queue = queue;
+  /* the tail phase as in ptg_transmission (tune_flags bit 1 turns it off) */
+  r.coop_lanes = (v.opt.tune_flags & 2) ? 0 : (v.opt.coop_lanes > 0 ? std::min(v.opt.coop_lanes, 32) : 32);
   const int block = 256;
   const size_t smem = v.g32.stage_smem ? v.blob_bytes : 0;
   int bps = 0;
@@ -179,9 +185,22 @@ extern "C" int ptg_transmission_noalloc(ptg_handle* h, double mfp_nm, int32_t na
     return PTG_ERR_CUDA;
   if (v.opt.blocks_per_sm > 0 && v.opt.blocks_per_sm < bps) bps = v.opt.blocks_per_sm;
   if (bps < 1) bps = 1;
-  if (r.nchunk > 0 &&
-      ptg::launch_persistent_fp32(v.g32, r, v.num_sms * bps, block, smem, s) != cudaSuccess)
-    return PTG_ERR_CUDA;
+  const int grid = v.num_sms * bps;
+  int tgrid = 0;
+  if (r.coop_lanes > 0) {
+    r.tail = reinterpret_cast<float4*>(base + kOffTail);
+    r.tail_cap = std::min(kMaxTail, grid * block);
+    int tbps = 0;
+    if (ptg::tail_occupancy(block, smem, &tbps, ptg::MODE_FORWARD, v.g32.has_ext != 0) != cudaSuccess)
+      return PTG_ERR_CUDA;
+    tgrid = v.num_sms * (tbps < 1 ? 1 : tbps);
+  }
+  if (r.nchunk > 0) {
+    if (ptg::launch_persistent_fp32(v.g32, r, grid, block, smem, s) != cudaSuccess)
+      return PTG_ERR_CUDA;
+    if (tgrid > 0 && ptg::launch_tail_fp32(v.g32, r, tgrid, block, smem, s) != cudaSuccess)
+      return PTG_ERR_CUDA;
+  }
   /* the counts land in the caller's transmit array (ntask <= its length),
      then become count / np in place; the last angle is zero */
   int qerr[4] = {0, 0, 0, 0};
