@@ -584,6 +584,8 @@ constexpr int kAdjSmemDoubles = 2048;
 /* rounds of 32 flights one cooperative visit may take before the phonon's
    lane returns to the refill / tally step */
 constexpr int kCoopRounds = 32;
+/* floats between the rows of a warp's cooperative-round block */
+constexpr int kRowStride = 36;
 
 /* Kernel phases.  PH_DRAIN pulls (task, particle range) chunks from the
    work queue, one phonon per lane; once the queue is dry a warp holding at
@@ -625,9 +627,12 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   float flmax = r.fast_lambda_max;
   /* adjoint replay: per-block accumulators */
   __shared__ double adj_sh[MODE == MODE_ADJOINT ? kAdjSmemDoubles : 1];
-  /* cooperative rounds: per warp one row of 32 (free path, direction) */
-  __shared__ float4 coop_rows[PH == PH_TAIL ? kBlock / 32 : 1][32];
-  float4* const wrow = coop_rows[PH == PH_TAIL ? (threadIdx.x >> 5) : 0];
+  /* cooperative rounds: per warp the rows of the round's 32 free paths and
+     directions (fp, dx, dy, dz) and of the start points summed from them
+     (x, y, z), 36 floats apart so three lanes reading three rows hit
+     different banks */
+  __shared__ __align__(16) float coop_rowf[PH == PH_TAIL ? kBlock / 32 : 1][kRowStride * 7];
+  float* const crow = coop_rowf[PH == PH_TAIL ? (threadIdx.x >> 5) : 0];
   /* ... and five rows where the lanes' own phonons wait during the rounds */
   __shared__ float4 coop_park[PH == PH_TAIL ? kBlock / 32 : 1][5][32];
   float4 (*const park)[32] = coop_park[PH == PH_TAIL ? (threadIdx.x >> 5) : 0];
@@ -923,39 +928,55 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             const float nx = ct, ny = st * cp, nz = st * sp;
             const float nf = -clam * __logf(u23f(R.z));
             /* flight `lane` starts with the state the previous flight drew:
-               the warp's row of shared memory holds (free path, direction)
-               of flights 1..31 of the round.  The start point of flight j
-               is the chain p, fma(fp_0, d_0, p), ... after j steps, the same
-               for every lane: each lane runs the whole chain (flight 0's step
-               from registers, the others from broadcast loads issued eight
-               at a time ahead of their fmas) and keeps step j with a select */
-            if (lane < 31) wrow[lane + 1] = make_float4(nf, nx, ny, nz);
+               the rows hold the (free path, direction) of the round's 32
+               flights.  The start point of flight j is the chain p,
+               fma(fp_0, d_0, p), ... after j steps, the same for every lane,
+               so lane c < 3 runs coordinate c's chain alone (two 4-wide
+               loads, four fmas and one 4-wide store of the chain per four
+               flights) and every lane then reads its own start point */
+            float* const frow = crow;
+            if (lane < 31) {
+              frow[lane + 1] = nf;
+              frow[kRowStride + lane + 1] = nx;
+              frow[2 * kRowStride + lane + 1] = ny;
+              frow[3 * kRowStride + lane + 1] = nz;
+            }
+            if (lane == 0) {
+              frow[0] = cfp;
+              frow[kRowStride] = cdx;
+              frow[2 * kRowStride] = cdy;
+              frow[3 * kRowStride] = cdz;
+            }
             __syncwarp();
-            const float4 mine = lane == 0 ? make_float4(cfp, cdx, cdy, cdz) : wrow[lane];
-            const float sfp = mine.x, sdx = mine.y, sdy = mine.z, sdz = mine.w;
-            float qx = cpx, qy = cpy, qz = cpz;
+            const float sfp = frow[lane], sdx = frow[kRowStride + lane];
+            const float sdy = frow[2 * kRowStride + lane], sdz = frow[3 * kRowStride + lane];
             {
-              float ax = fmaf(cfp, cdx, cpx), ay = fmaf(cfp, cdy, cpy), az = fmaf(cfp, cdz, cpz);
-              qx = lane == 1 ? ax : qx; qy = lane == 1 ? ay : qy; qz = lane == 1 ? az : qz;
+              const int cc = lane < 3 ? lane : 2;
+              const float* const drow = frow + kRowStride * (cc + 1);
+              float* const qrow = frow + kRowStride * (cc + 4);
+              float a = cc == 0 ? cpx : (cc == 1 ? cpy : cpz);
 #pragma unroll
-              for (int b = 1; b < 31; b += 8) {
-                float4 v[8];
-#pragma unroll
-                for (int k = 0; k < 8; ++k)
-                  if (b + k < 31) v[k] = wrow[b + k];
-#pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                  if (b + k < 31) {
-                    ax = fmaf(v[k].x, v[k].y, ax);
-                    ay = fmaf(v[k].x, v[k].z, ay);
-                    az = fmaf(v[k].x, v[k].w, az);
-                    const bool me = lane == b + k + 1;
-                    qx = me ? ax : qx; qy = me ? ay : qy; qz = me ? az : qz;
-                  }
-                }
+              for (int b = 0; b < 32; b += 4) {
+                const float4 f = *reinterpret_cast<const float4*>(frow + b);
+                const float4 d = *reinterpret_cast<const float4*>(drow + b);
+                float4 q;
+                a = fmaf(f.x, d.x, a);
+                q.x = a;
+                a = fmaf(f.y, d.y, a);
+                q.y = a;
+                a = fmaf(f.z, d.z, a);
+                q.z = a;
+                a = fmaf(f.w, d.w, a);
+                q.w = a;
+                if (lane < 3) *reinterpret_cast<float4*>(qrow + b) = q;
               }
             }
-            __syncwarp();  /* the next round rewrites the row */
+            __syncwarp();
+            const int jq = lane > 0 ? lane - 1 : 0;
+            const float qx = lane == 0 ? cpx : frow[4 * kRowStride + jq];
+            const float qy = lane == 0 ? cpy : frow[5 * kRowStride + jq];
+            const float qz = lane == 0 ? cpz : frow[6 * kRowStride + jq];
+            __syncwarp();  /* the next round rewrites the rows */
             const bool inbox = qx >= -eps && qx <= X + eps && qy >= -eps && qy <= Y + eps &&
                                qz >= -eps && qz <= Z + eps;
             const bool capd = (unsigned long long)cfl + (unsigned)lane >= r.max_flights;
