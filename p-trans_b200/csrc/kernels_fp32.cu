@@ -586,6 +586,10 @@ constexpr int kAdjSmemDoubles = 2048;
 constexpr int kCoopRounds = 32;
 /* floats between the rows of a warp's cooperative-round block */
 constexpr int kRowStride = 36;
+/* flights a round tests from its first flight outside the safe ball, in a
+   kernel built for BVH grains (every such flight walks the tree and the round
+   waits for the slowest walk); the round ends after them */
+constexpr int kTestWindow = 4;
 
 /* Kernel phases.  PH_DRAIN pulls (task, particle range) chunks from the
    work queue, one phonon per lane; once the queue is dry a warp holding at
@@ -991,17 +995,20 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             const bool in_ball = de2 < cbr2 && ds2 < cbr2;
             /* in the grain ball only the box faces can be hit */
             const bool in_gball = de2 < cgr2 && ds2 < cgr2;
+            const unsigned outm = __ballot_sync(FULL, !in_ball);
+            const int jw = (EXT && outm) ? min(32, __ffs(outm) - 1 + kTestWindow) : 32;
             float tb = 3.0e38f;
             int sb = -1;
-            if (!in_ball) {
+            if (!in_ball && lane < jw) {
               slab_exit(qx, qy, qz, sdx, sdy, sdz, X, Y, Z, tb, sb);
               if (cgrain > 0 && !in_gball)
                 scan_grain<EXT>(G, cgrain, qx, qy, qz, sdx, sdy, sdz, lane == 0 ? clast : -1, eps,
                                 Z, tb, sb, my_box_tests, my_surf_tests);
             }
             const bool brk = !inbox || capd;
-            const unsigned sm = __ballot_sync(FULL, brk || (!in_ball && !(sfp < tb)));
-            const int j = sm ? __ffs(sm) - 1 : 32;
+            const unsigned sm =
+                __ballot_sync(FULL, lane < jw && (brk || (!in_ball && !(sfp < tb))));
+            const int j = sm ? __ffs(sm) - 1 : jw;
             if (MODE == MODE_ADJOINT) {
               float l = lane < j ? sfp : 0.0f;
               for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(FULL, l, o);
@@ -1009,7 +1016,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
               cnpp += (unsigned)j;
             }
             ctaken += (unsigned)j;
-            if (j < 32) {
+            if (sm) {
               cpx = __shfl_sync(FULL, qx, j); cpy = __shfl_sync(FULL, qy, j);
               cpz = __shfl_sync(FULL, qz, j);
               cdx = __shfl_sync(FULL, sdx, j); cdy = __shfl_sync(FULL, sdy, j);
@@ -1025,15 +1032,24 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
               }
               break;
             }
-            /* all 32 flights end in p-p events: the state after the last */
-            cpx = __shfl_sync(FULL, fmaf(sfp, sdx, qx), 31);
-            cpy = __shfl_sync(FULL, fmaf(sfp, sdy, qy), 31);
-            cpz = __shfl_sync(FULL, fmaf(sfp, sdz, qz), 31);
-            cdx = __shfl_sync(FULL, nx, 31); cdy = __shfl_sync(FULL, ny, 31);
-            cdz = __shfl_sync(FULL, nz, 31); cfp = __shfl_sync(FULL, nf, 31);
-            cfl += 32u;
+            if (j < 32) {
+              /* the window's flights all end in p-p events: the state at the
+                 start of flight j */
+              cpx = __shfl_sync(FULL, qx, j); cpy = __shfl_sync(FULL, qy, j);
+              cpz = __shfl_sync(FULL, qz, j);
+              cdx = __shfl_sync(FULL, sdx, j); cdy = __shfl_sync(FULL, sdy, j);
+              cdz = __shfl_sync(FULL, sdz, j); cfp = __shfl_sync(FULL, sfp, j);
+            } else {
+              /* all 32 flights end in p-p events: the state after the last */
+              cpx = __shfl_sync(FULL, fmaf(sfp, sdx, qx), 31);
+              cpy = __shfl_sync(FULL, fmaf(sfp, sdy, qy), 31);
+              cpz = __shfl_sync(FULL, fmaf(sfp, sdz, qz), 31);
+              cdx = __shfl_sync(FULL, nx, 31); cdy = __shfl_sync(FULL, ny, 31);
+              cdz = __shfl_sync(FULL, nz, 31); cfp = __shfl_sync(FULL, nf, 31);
+            }
+            cfl += (uint32_t)j;
             /* a new ball where the walk left the old one */
-            if (!__shfl_sync(FULL, in_ball, 31) && r.fast_steps > 0) {
+            if (!__shfl_sync(FULL, in_ball, j - 1) && r.fast_steps > 0) {
               float dg;
               const float d =
                   safety<EXT>(G, cgrain, cpx, cpy, cpz, X, Y, Z, eps, kBallCapMfp * clam, dg);
