@@ -29,19 +29,25 @@
  *     counted and still draws its own Philox block, so the trajectory is the
  *     one the full test gives.  A diffusive walk leaves the ball only after
  *     about (d/MFP)^2 flights, which shortens the serial chain of the longest
- *     trajectories that bound the kernel's run time;
+ *     trajectories that bound the kernel's run time.  A warp takes fast
+ *     flights in groups of four, past fast_steps only while half its live
+ *     lanes are still in their balls, so lanes that need a full flight are
+ *     not held back.  With the ball the lane keeps a second radius about the
+ *     same centre, over the grain's candidate surfaces alone (the grain
+ *     ball): a flight inside it needs only the box-face test;
  *   - one Philox4x32-10 block per free flight supplies the four uniforms of
  *     any event; on the fast path the blocks of four flights are computed
- *     together so that four independent chains fill the issue slots of a
- *     warp that is alone on its scheduler (the tail of a run); tallies are
- *     integer, aggregated per warp by task (match_any) before one atomic;
+ *     together so that four independent chains fill the issue slots; tallies
+ *     are integer, aggregated per warp by task (match_any) before one atomic;
  *   - two phases: the drain phase runs the work queue one lane per phonon
  *     and, once the queue is dry, hands its diffusive phonons to a tail list;
  *     the tail phase (a second launch of the same kernel) gives each of them
  *     a warp that advances it 32 flights per round, one flight per lane, with
- *     the flights' start points summed in flight order; every path (fast,
- *     full, cooperative) moves the position with the same fma, so a
- *     trajectory is the same whichever path takes its flights.
+ *     the flights' start points summed in flight order (in grains with a BVH
+ *     a round tests at most kTestWindow flights from its first one outside
+ *     the safe ball); every path (fast, full, cooperative) moves the position
+ *     with the same fma, so a trajectory is the same whichever path takes its
+ *     flights.
  */
 #include <cuda_runtime.h>
 #include <math.h>
