@@ -145,26 +145,122 @@ def dram_traffic(phase="drain"):
     return None, None
 
 
-def cpu_baseline(pkg, model, spec, target_s=10.0):
-    """The oracle (OpenMP, all host threads) on a bounded sample of the workload:
-    every (mode, angle) task with fewer particles."""
+ORACLE_SEED = 777   # the oracle's seed: independent of the GPU run's 12345
+
+
+def cpu_leg(args):
+    """The cpu_baseline leg in a process of its own (bench.py --cpu-leg): the
+    oracle (OpenMP, all host threads) on the workload with this run's
+    particles per task, or fewer when that would take more than about 20 s.
+    torch is never imported here: next to torch's OpenMP runtime the oracle
+    ran about three times slower.  Prints one JSON line: the rate, the
+    sample, and the oracle's kappa and per-bin transmission with their
+    standard errors (the FP64 side of the parity object)."""
+    pkg = load_pkg()
+    model, spec, _ = workload(pkg, np_per_task=args.np, mfp_lo=args.mfp_lo)
     if ROOT not in sys.path:
         sys.path.insert(0, ROOT)
     from oracle import oracle as O
     o = O.Oracle(model=model, spectrum=spec)
     n = 2
-    run = make_run(pkg, spec, n, 0, 1, 0)
+    run = make_run(pkg, spec, n, 0, 1, 0, seed=ORACLE_SEED)
     _, _, r = o.counts(run)
-    rate = r["flights"] / max(r["seconds"], 1e-6)
+    probe_rate = r["flights"] / max(r["seconds"], 1e-6)
     per_particle = r["seconds"] / n
-    n = max(2, min(500, int(target_s / max(per_particle, 1e-9))))
-    run = make_run(pkg, spec, n, 0, 1, 0)
-    _, _, r = o.counts(run)
-    return {"value": r["flights"] / r["seconds"], "unit": UNIT, "cores": int(r["threads"]),
-            "kind": "port", "seconds": r["seconds"], "flights": int(r["flights"]),
-            "sample": (f"all 20000 (mode, angle) tasks with {n} particles each " +
-                       ("(the whole workload)" if n >= 500 else "instead of 500") +
-                       f", {r['samples']} trajectories, same geometry, spectrum and seed")}
+    n = max(2, min(args.np, int(args.cpu_target_s / max(per_particle, 1e-9))))
+    run = make_run(pkg, spec, n, 0, 1, 0, seed=ORACLE_SEED)
+    cnt, _, r = o.counts(run)
+    k = o.kappa(run, cnt)
+    ntask = spec.nmode * 10
+    print(json.dumps({
+        "value": r["flights"] / r["seconds"], "unit": UNIT, "cores": int(r["threads"]), "kind": "port",
+        "seconds": r["seconds"], "flights": int(r["flights"]), "probe_rate": probe_rate,
+        "particles_per_task": n,
+        "sample": (f"all {ntask} (mode, angle) tasks with {n} particles each " +
+                   ("(the whole workload)" if n >= args.np else f"instead of {args.np}") +
+                   f", {r['samples']} trajectories, same geometry and spectrum, seed {ORACLE_SEED}"),
+        "kappa": k["kappa"], "kappa_stderr": k["kappa_stderr"],
+        "bin_T": [float(x) for x in k["bin_T"]], "bin_T_stderr": [float(x) for x in k["bin_T_stderr"]]}))
+    return 0
+
+
+def cpu_baseline(args):
+    """Runs the cpu_baseline leg (cpu_leg) as a child process with every host
+    thread and returns its JSON record."""
+    import subprocess
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    cmd = [sys.executable, os.path.abspath(__file__), "--cpu-leg", "--np", str(args.np),
+           "--mfp-lo", repr(args.mfp_lo), "--cpu-target-s", repr(args.cpu_target_s)]
+    p = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=900)
+    if p.returncode != 0:
+        raise RuntimeError(f"cpu_baseline leg failed ({p.returncode}): {p.stderr[-2000:]}")
+    return json.loads(p.stdout.strip().splitlines()[-1])
+
+
+def parity(out, leg):
+    """The FP32 GPU result against the FP64 oracle on the same workload
+    (independent seeds): kappa and the per-bin transmission, with z-scores
+    over the combined standard errors."""
+    kg, sg = out["kappa"], out["kappa_stderr"]
+    ko, so = leg["kappa"], leg["kappa_stderr"]
+    se = math.hypot(sg, so)
+    bg, bo = np.asarray(out["bin_T"], float), np.asarray(leg["bin_T"], float)
+    eg, eo = np.asarray(out["bin_T_stderr"], float), np.asarray(leg["bin_T_stderr"], float)
+    seb = np.hypot(eg, eo)
+    live = seb > 0
+    zb = np.zeros_like(bg)
+    zb[live] = (bg[live] - bo[live]) / seb[live]
+    d = bg - bo
+    return {"reference": "FP64 CPU oracle (the cpu_baseline run)", "gpu_kappa": kg, "gpu_kappa_stderr": sg,
+            "oracle_kappa": ko, "oracle_kappa_stderr": so, "z_kappa": (kg - ko) / se if se > 0 else None,
+            "kappa_rel_diff": (kg - ko) / ko if ko else None,
+            "kappa_rel_combined_stderr": se / ko if ko else None,
+            "bins": int(bg.size), "bins_compared": int(live.sum()),
+            "max_abs_z_bin": float(np.max(np.abs(zb))) if live.any() else None,
+            "max_abs_bin_diff": float(np.max(np.abs(d))), "rms_bin_diff": float(np.sqrt(np.mean(d * d))),
+            "bin_diff": [float(x) for x in d]}
+
+
+def spawn_ranks(n, script, argv, timeout_s=3600, extra_env=None):
+    """Runs `script argv` as n processes on this node, one per GPU, with the
+    environment torchrun gives a rank (RANK, LOCAL_RANK, WORLD_SIZE,
+    MASTER_ADDR = 127.0.0.1, a free MASTER_PORT).  Their output is passed
+    through (rank 0 prints the result line); returns the largest exit code.
+    A rank that fails ends the others."""
+    import socket
+    import subprocess
+    sk = socket.socket()
+    sk.bind(("127.0.0.1", 0))
+    port = sk.getsockname()[1]
+    sk.close()
+    procs = []
+    for r in range(n):
+        env = dict(os.environ, RANK=str(r), LOCAL_RANK=str(r), WORLD_SIZE=str(n), LOCAL_WORLD_SIZE=str(n),
+                   MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        env.update(extra_env or {})
+        procs.append(subprocess.Popen([sys.executable, script] + list(argv), env=env))
+    rc = 0
+    t0 = time.time()
+    pending = list(procs)
+    while pending:
+        for pr in list(pending):
+            code = pr.poll()
+            if code is None:
+                continue
+            pending.remove(pr)
+            rc = max(rc, abs(code))
+            if code != 0:
+                for other in pending:
+                    other.kill()
+        if time.time() - t0 > timeout_s:
+            for pr in pending:
+                pr.kill()
+            rc = max(rc, 124)
+        time.sleep(0.05)
+    for pr in procs:
+        pr.wait()
+    return rc
 
 
 def run_reference(args):
@@ -406,7 +502,12 @@ def main():
                          "the adjoint; c5: 256-film batched screening; voronoi / mesh: the C4 structures")
     ap.add_argument("--fp64-subset", type=int, default=16,
                     help="c5: films timed one by one with the plain FP64 kernel")
+    ap.add_argument("--cpu-leg", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--cpu-target-s", type=float, default=20.0,
+                    help="seconds of CPU work the cpu_baseline leg is sized to")
     args = ap.parse_args()
+    if args.cpu_leg:
+        return cpu_leg(args)
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "c5":
@@ -416,9 +517,15 @@ def main():
     if args.workload == "c3":
         return run_c3(args)
 
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # not launched by torchrun: start the ranks here, one per GPU
+        return spawn_ranks(args.gpus, os.path.abspath(__file__), sys.argv[1:])
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus:
+        print(f"bench: WORLD_SIZE {world} differs from --gpus {args.gpus}", file=sys.stderr)
+        return 2
     import torch
     torch.cuda.set_device(local)
     dist = None
@@ -565,7 +672,10 @@ def main():
             "clocks": clocks,
         }
         if world == 1 and not args.no_cpu:
-            result["cpu_baseline"] = cpu_baseline(pkg, model, spec)
+            leg = cpu_baseline(args)
+            result["cpu_baseline"] = {k: leg[k] for k in ("value", "unit", "cores", "kind", "sample",
+                                                          "seconds", "flights", "probe_rate")}
+            result["parity"] = parity(out, leg)
     h.close()
     del flush
     if dist is not None:

@@ -192,6 +192,10 @@ typedef struct ptg_options {
                             /*   bit 0: no safe-distance p-p fast path          */
                             /*   bit 1: no tail phase (one lane per phonon to   */
                             /*          the end)                                */
+                            /*   bit 2: test only: the shared-memory staging    */
+                            /*          copy is not issued, so its bounded wait */
+                            /*          runs out and the call returns           */
+                            /*          PTG_ERR_TIMEOUT                         */
   int32_t fast_steps;       /* fast p-p flights per iteration before a warp     */
                             /* goes on only while half its lanes still can      */
                             /* (at most 4x; 0 = 8)                              */
@@ -199,7 +203,7 @@ typedef struct ptg_options {
                             /* this many live phonons hands its diffusive ones  */
                             /* to the tail phase, a second kernel that gives    */
                             /* each a warp of 32 cooperating lanes (0 = 32)     */
-  int32_t long_flights;     /* unused; kept so the struct layout stays          */
+  int32_t reserved;         /* reserved, must be 0                              */
 } ptg_options;
 
 /*
@@ -269,6 +273,8 @@ typedef struct ptg_stats {
                             /*   (0 when the tail phase is off)                 */
   uint64_t tail_phonons;    /* FP32: phonons the drain phase handed over        */
   uint64_t tail_flights;    /* FP32: free flights taken in the tail phase       */
+  uint64_t tail_refused;    /* FP32: hand-overs refused because the tail list   */
+                            /*   was full (those phonons stayed in the drain)   */
 } ptg_stats;
 
 typedef struct ptg_handle ptg_handle;
@@ -427,6 +433,30 @@ typedef struct ptg_batch_out {
 int ptg_batch_create(const ptg_batch_item* items, int32_t nitems, const ptg_spectrum* spec,
                      const ptg_run* run, const ptg_options* opt, ptg_batch** out);
 int ptg_batch_run(ptg_batch* b, ptg_batch_out* out);
+/*
+ * Per-geometry adjoint of a batch (no counterpart in the reference): what
+ * ptg_adjoint gives for each geometry's own run, from two batched launches
+ * over all geometries - a forward pass that lists the samples leaving
+ * through x+ as (global task, particle) ids, then, after the host has
+ * assembled every geometry's kappa and d kappa / d T_task, one replay of
+ * all listed samples from their Philox counters that accumulates each
+ * sample's score into its geometry's slice.  dk_dp and dk_dp_stderr hold
+ * the geometries' surface records one after the other (geometry g starts at
+ * the sum of the earlier geometries' nsurf); NaN where p is 0 or 1.
+ */
+typedef struct ptg_batch_adjoint_out {
+  double* kappa;            /* [nitems]                                      */
+  double* kappa_stderr;     /* [nitems]                                      */
+  double* dk_dp;            /* [sum of nsurf]                                */
+  double* dk_dp_stderr;     /* [sum of nsurf]                                */
+  double* dk_dscale;        /* [nitems]                                      */
+  double* dk_dscale_stderr; /* [nitems]                                      */
+  uint64_t flights;         /* forward + replay free flights                 */
+  uint64_t replayed;        /* transmitted samples re-generated              */
+  uint64_t mismatched;      /* replays that did not transmit again (0)       */
+  double kernel_ms;         /* device time of the two launches               */
+} ptg_batch_adjoint_out;
+int ptg_batch_adjoint(ptg_batch* b, ptg_batch_adjoint_out* out);
 void ptg_batch_destroy(ptg_batch* b);
 
 /* Statistics of the last transport call on h. */
@@ -480,13 +510,16 @@ int ptg_autotune(ptg_handle* h, const ptg_run* run, int32_t reps, ptg_options* b
  * hosts that cannot allocate memory while they run (device memory reserved up
  * front by another framework, or a service that must keep a fixed
  * footprint).  It computes what ptg_transmission computes with
- * PTG_PREC_FP32 (same counts, so the same transmit array) but allocates no
- * device or host memory: the kernels' scratch (work-queue counter,
- * statistics, tallies, task and chunk tables, a 65536-phonon tail-phase
- * list) lives in one static device array of fixed size (about 8 MB) that
- * every GPU loading the library keeps until exit,
- * and the caller's transmit array receives the counts before they are
- * divided by np in place.  Limits: nbranch*nkpoint*(nangle-1) <=
+ * PTG_PREC_FP32 (same counts, so the same transmit array; the same
+ * lost-phonon limit; the same ptg_last_stats record, kernel times aside) but
+ * allocates no device or host memory: the kernels' scratch (work-queue
+ * counter, statistics, tallies, task and chunk tables, a 65536-phonon
+ * tail-phase list; hand-overs past its capacity stay in the drain phase and
+ * are counted in ptg_stats.tail_refused) lives in one static device array of
+ * fixed size (about 8 MB) that every GPU loading the library keeps until
+ * exit, and the caller's transmit array receives the counts before they are
+ * divided by np in place (on PTG_ERR_TIMEOUT or PTG_ERR_CUDA after the
+ * launch it is zeroed).  Limits: nbranch*nkpoint*(nangle-1) <=
  * PTG_NOALLOC_MAX_TASKS, nangle <= 64; larger runs return PTG_ERR_INVALID.
  * The first call on a device looks up the array's address (make it before
  * any stream capture).  All calls share the array: calls whose GPU work

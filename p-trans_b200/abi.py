@@ -1,7 +1,7 @@
 """ctypes binding of include/ptrans_gpu.h (libptrans_b200.so).
 
 This is the Python host mirror of the drop-in seam: the same entry points a
-Fortran host binds with ISO_C_BINDING, with the
+Fortran host binds with ISO_C_BINDING (p-trans_b200/fortran/ptrans_gpu.f90), with the
 reference's argument meaning (``RayTrace``'s parameters, ``TransmissionFunction``
 filling ``transmit(nbranch,nkpoint,nangle)``, src/RTMCphon.f90:1544-1604) and
 its error behaviour (a non-zero status raises ``PtgError``).
@@ -86,7 +86,7 @@ class PtgOptions(C.Structure):
         ("regen_threshold", C.c_int32), ("ref_quirks", C.c_int32), ("bvh_leaf", C.c_int32),
         ("max_flights", C.c_int64), ("lost_limit", C.c_double), ("chunk", C.c_int64),
         ("tune_flags", C.c_int32), ("fast_steps", C.c_int32), ("coop_lanes", C.c_int32),
-        ("long_flights", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 
@@ -121,6 +121,7 @@ class PtgStats(C.Structure):
         ("box_tests", C.c_uint64), ("surface_tests", C.c_uint64),
         ("drain_kernel_ms", C.c_double), ("tail_kernel_ms", C.c_double),
         ("tail_phonons", C.c_uint64), ("tail_flights", C.c_uint64),
+        ("tail_refused", C.c_uint64),
     ]
 
 
@@ -141,6 +142,12 @@ class PtgBatchOut(C.Structure):
     _fields_ = [("kappa", F64P), ("kappa_stderr", F64P), ("bin_T", F64P), ("bin_T_stderr", F64P),
                 ("counts", U64P), ("flights", C.c_uint64), ("lost", C.c_uint64),
                 ("samples", C.c_uint64), ("graph_ms", C.c_double)]
+
+
+class PtgBatchAdjointOut(C.Structure):
+    _fields_ = [("kappa", F64P), ("kappa_stderr", F64P), ("dk_dp", F64P), ("dk_dp_stderr", F64P),
+                ("dk_dscale", F64P), ("dk_dscale_stderr", F64P), ("flights", C.c_uint64),
+                ("replayed", C.c_uint64), ("mismatched", C.c_uint64), ("kernel_ms", C.c_double)]
 
 
 class PtgError(RuntimeError):
@@ -200,6 +207,7 @@ SIGNATURES = {
     "ptg_batch_create": (C.c_int, [C.POINTER(PtgBatchItem), C.c_int32, C.POINTER(PtgSpectrum),
                                    C.POINTER(PtgRun), C.POINTER(PtgOptions), C.POINTER(C.c_void_p)]),
     "ptg_batch_run": (C.c_int, [C.c_void_p, C.POINTER(PtgBatchOut)]),
+    "ptg_batch_adjoint": (C.c_int, [C.c_void_p, C.POINTER(PtgBatchAdjointOut)]),
     "ptg_batch_destroy": (None, [C.c_void_p]),
     "ptg_transmission_noalloc": (C.c_int, [C.c_void_p, C.c_double, C.c_int32, C.c_int64, C.c_int32,
                                            C.c_int32, C.c_uint64, F64P]),
@@ -670,6 +678,27 @@ class Batch:
                 "bin_T_stderr": be[: self.n * self.nbins].reshape(self.n, self.nbins),
                 "counts": None if cn is None else cn.reshape(self.n, self.ntask),
                 "flights": out.flights, "lost": out.lost, "samples": out.samples, "graph_ms": out.graph_ms}
+
+    def adjoint(self) -> dict:
+        """ptg_batch_adjoint: every geometry's kappa, d kappa / d p of its
+        surface records (a list of arrays, one per geometry) and d kappa / d
+        scale, from one batched listing pass and one batched replay."""
+        ns = [int(g.nsurf) for g in self._geoms]
+        tot = max(1, sum(ns))
+        k, ke = np.zeros(self.n), np.zeros(self.n)
+        dp, dpe = np.zeros(tot), np.zeros(tot)
+        ds, dse = np.zeros(self.n), np.zeros(self.n)
+        out = PtgBatchAdjointOut()
+        out.kappa, out.kappa_stderr = _ptr(k, C.c_double), _ptr(ke, C.c_double)
+        out.dk_dp, out.dk_dp_stderr = _ptr(dp, C.c_double), _ptr(dpe, C.c_double)
+        out.dk_dscale, out.dk_dscale_stderr = _ptr(ds, C.c_double), _ptr(dse, C.c_double)
+        _check(self.lib.ptg_batch_adjoint(self.h, C.byref(out)), "ptg_batch_adjoint")
+        off = np.concatenate([[0], np.cumsum(ns)])
+        return {"kappa": k, "kappa_stderr": ke,
+                "dk_dp": [dp[off[g]:off[g + 1]] for g in range(self.n)],
+                "dk_dp_stderr": [dpe[off[g]:off[g + 1]] for g in range(self.n)],
+                "dk_dscale": ds, "dk_dscale_stderr": dse, "flights": out.flights,
+                "replayed": out.replayed, "mismatched": out.mismatched, "kernel_ms": out.kernel_ms}
 
     def close(self):
         if getattr(self, "h", None):

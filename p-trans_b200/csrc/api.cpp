@@ -541,6 +541,7 @@ int run_transport(ptg_handle* h, const Transport& T) {
     /* tune_flags bit 1 turns the tail phase off; 0 selects 32 lanes (every
        diffusive phonon still alive when a warp finds the queue dry) */
     r.coop_lanes = (h->opt.tune_flags & 2) ? 0 : (h->opt.coop_lanes > 0 ? std::min(h->opt.coop_lanes, 32) : 32);
+    r.stage_test = (h->opt.tune_flags & 4) ? 1 : 0;
     r.counts = h->counts.as<unsigned long long>();
     r.lost = h->lost.as<unsigned long long>();
     r.stats = h->stats.as<unsigned long long>();
@@ -618,14 +619,13 @@ int finish_stats(ptg_handle* h) {
   h->last.box_tests = st[14];
   h->last.surface_tests = st[15];
   h->last.drain_kernel_ms = h->last.tail_kernel_ms = 0.0;
-  h->last.tail_phonons = h->last.tail_flights = 0;
+  h->last.tail_phonons = h->last.tail_flights = h->last.tail_refused = 0;
   if (h->fp32_split) {
     float dms = 0.f;
     CU(cudaEventElapsedTime(&dms, h->ev[0], h->ev[4]));
     h->last.drain_kernel_ms = dms;
     h->last.tail_kernel_ms = ms - dms;
-    h->last.tail_phonons =
-        (uint64_t)std::max(0, std::min(qerr[2], h->tail_cap) + std::min(qerr[4], h->tail_cap));
+    ptg::tail_counts(qerr, h->tail_cap, &h->last.tail_phonons, &h->last.tail_refused);
     h->last.tail_flights = st[17] >= st[16] ? st[17] - st[16] : 0;
   }
   h->list_n = st[10];
@@ -793,6 +793,7 @@ int handle_noalloc_view(ptg_handle* h, NoallocView* v) {
   v->opt = h->opt;
   v->spec = &h->spec;
   v->geom = &h->geom;
+  v->last = &h->last;
   return PTG_OK;
 }
 
@@ -825,6 +826,7 @@ int ptg_create(const ptg_geometry* geom, const ptg_spectrum* spec, const ptg_opt
   memset(&h->opt, 0, sizeof(h->opt));
   if (opt) h->opt = *opt;
   memset(&h->last, 0, sizeof(h->last));
+  if (h->opt.reserved != 0) { delete h; return PTG_ERR_INVALID; }
   std::string why;
   int st = ptg::copy_geometry(geom, &h->geom, &why);
   if (st == PTG_OK) st = ptg::copy_spectrum(spec, &h->spec, &why);
@@ -883,6 +885,7 @@ int ptg_set_options(ptg_handle* h, const ptg_options* opt) {
     h->last_error = "block_size must be 0 or a multiple of 32 up to 256";
     return PTG_ERR_INVALID;
   }
+  if (opt->reserved != 0) { h->last_error = "ptg_options.reserved must be 0"; return PTG_ERR_INVALID; }
   const bool rebuild = opt->bvh_leaf != h->opt.bvh_leaf;
   const ptg_options old = h->opt;
   h->opt = *opt;

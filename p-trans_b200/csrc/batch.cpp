@@ -52,6 +52,17 @@ struct ptg_batch {
   unsigned long long* host_stats = nullptr;   /* pinned */
   int launch_grid = 0;
   bool bvh = false;   /* a BVH or capped cylinders: the kernel built for them */
+  /* what the per-geometry adjoint needs besides the forward's tables */
+  ptg::SpecSoA spec;
+  ptg_run run;
+  std::vector<double> mfp_grid;               /* run.mfp_grid_nm points here */
+  ptg::RunF32 r;                              /* the forward's kernel arguments */
+  std::vector<int> nsurf, adj_base;
+  std::vector<std::vector<double>> specularity;
+  std::vector<double> box_x;
+  std::vector<int64_t> np;
+  Dev adj_list, adj_w, adj_acc;
+  size_t adj_list_cap = 0, adj_acc_n = 0;
   ~ptg_batch() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
@@ -146,6 +157,15 @@ extern "C" int ptg_batch_create(const ptg_batch_item* items, int32_t nitems,
     e.k1 = (uint32_t)(it.seed >> 32);
     e.c1 = ((uint32_t)it.stream) << 8;
     e.task_base = (int)(g * ntg);
+    e.nsurf = G.nsurf();
+    e.adj_base = (int)b->adj_acc_n;
+    b->adj_base.push_back(e.adj_base);
+    b->nsurf.push_back(e.nsurf);
+    b->specularity.push_back(G.specularity);
+    b->box_x.push_back(G.box[0]);
+    b->np.push_back(it.np);
+    b->adj_acc_n += (size_t)ptg::kAdjBatches * (size_t)(e.nsurf + 1);
+    if (b->adj_acc_n > 2147483647ull) { delete b; return PTG_ERR_UNSUPPORTED; }
     np_geo[g] = (double)it.np;
     double dS;
     ptg::simpson_weights(run->nangle, G.box[0], &coef, &dS);
@@ -198,7 +218,7 @@ extern "C" int ptg_batch_create(const ptg_batch_item* items, int32_t nitems,
   BCU(b->counts.alloc(sizeof(unsigned long long) * ntot));
   BCU(b->lost.alloc(sizeof(unsigned long long) * ntot));
   BCU(b->stats.alloc(sizeof(unsigned long long) * ptg::kStatSlots));
-  BCU(b->queue.alloc(sizeof(int) * 4));
+  BCU(b->queue.alloc(sizeof(int) * 8));
   BCU(b->coef.alloc(sizeof(double) * coef.size()));
   BCU(b->K.alloc(sizeof(double) * nm));
   BCU(b->W.alloc(sizeof(double) * nm));
@@ -278,6 +298,11 @@ extern "C" int ptg_batch_create(const ptg_batch_item* items, int32_t nitems,
   rb.np_geo = b->np_geo.as<const double>();
   rb.dS_geo = b->dS_geo.as<const double>();
   rb.tnorm_geo = b->tnorm_geo.as<const double>();
+  b->r = r;
+  b->spec = S;
+  b->run = *run;
+  if (run->kind_mfp == PTG_MFP_GRID) b->mfp_grid.assign(run->mfp_grid_nm, run->mfp_grid_nm + ns);
+  b->run.mfp_grid_nm = b->mfp_grid.empty() ? nullptr : b->mfp_grid.data();
   int bps = 0;
   BCU(ptg::persistent_batch_occupancy(256, &bps, b->bvh));
   if (o.blocks_per_sm > 0 && o.blocks_per_sm < bps) bps = o.blocks_per_sm;
@@ -295,7 +320,7 @@ extern "C" int ptg_batch_create(const ptg_batch_item* items, int32_t nitems,
   if (ce == cudaSuccess)
     ce = cudaMemsetAsync(dstats, 0, sizeof(unsigned long long) * ptg::kStatSlots, b->stream);
   if (ce == cudaSuccess) ce = cudaMemsetAsync(dstats + 5, 0xFF, sizeof(unsigned long long) * 2, b->stream);
-  if (ce == cudaSuccess) ce = cudaMemsetAsync(b->queue.p, 0, sizeof(int) * 4, b->stream);
+  if (ce == cudaSuccess) ce = cudaMemsetAsync(b->queue.p, 0, sizeof(int) * 8, b->stream);
   if (ce == cudaSuccess && r.nchunk > 0) ce = ptg::launch_persistent_batch(r, b->launch_grid, 256, b->stream, b->bvh);
   if (ce == cudaSuccess) ce = ptg::launch_kappa_reduce_batch(rb, b->stream);
   if (ce == cudaSuccess)
@@ -342,6 +367,138 @@ extern "C" int ptg_batch_run(ptg_batch* b, ptg_batch_out* out) {
   out->lost = b->host_stats[1];
   out->samples = b->host_stats[3];
   out->graph_ms = ms;
+  return PTG_OK;
+}
+
+/* One batched transport launch outside the graph (list or adjoint mode):
+   clears the tallies, statistics and queue, launches, waits; *ms receives
+   its device time and st its statistics. */
+static int batch_launch(ptg_batch* b, const ptg::RunF32& r, int mode, unsigned long long* st,
+                        float* ms) {
+  const size_t ntot = (size_t)b->ngeo * (size_t)b->ntask_per_geo;
+  unsigned long long* dstats = b->stats.as<unsigned long long>();
+  int bps = 0;
+  if (ptg::persistent_batch_occupancy(256, &bps, b->bvh, mode) != cudaSuccess) return PTG_ERR_CUDA;
+  if (bps < 1) bps = 1;
+  if (cudaMemsetAsync(b->counts.p, 0, sizeof(unsigned long long) * ntot, b->stream) != cudaSuccess ||
+      cudaMemsetAsync(b->lost.p, 0, sizeof(unsigned long long) * ntot, b->stream) != cudaSuccess ||
+      cudaMemsetAsync(dstats, 0, sizeof(unsigned long long) * ptg::kStatSlots, b->stream) != cudaSuccess ||
+      cudaMemsetAsync(dstats + 5, 0xFF, sizeof(unsigned long long) * 2, b->stream) != cudaSuccess ||
+      cudaMemsetAsync(b->queue.p, 0, sizeof(int) * 8, b->stream) != cudaSuccess ||
+      cudaEventRecord(b->ev0, b->stream) != cudaSuccess)
+    return PTG_ERR_CUDA;
+  const bool work = mode == ptg::MODE_ADJOINT ? r.alist_n > 0 : r.nchunk > 0;
+  if (work && ptg::launch_persistent_batch(r, b->num_sms * bps, 256, b->stream, b->bvh, mode) != cudaSuccess)
+    return PTG_ERR_CUDA;
+  if (cudaEventRecord(b->ev1, b->stream) != cudaSuccess ||
+      cudaMemcpyAsync(st, dstats, sizeof(unsigned long long) * ptg::kStatSlots, cudaMemcpyDeviceToHost,
+                      b->stream) != cudaSuccess ||
+      cudaStreamSynchronize(b->stream) != cudaSuccess)
+    return PTG_ERR_CUDA;
+  *ms = 0.f;
+  cudaEventElapsedTime(ms, b->ev0, b->ev1);
+  return PTG_OK;
+}
+
+extern "C" int ptg_batch_adjoint(ptg_batch* b, ptg_batch_adjoint_out* out) {
+  if (!b || !out) return PTG_ERR_INVALID;
+  if (cudaSetDevice(b->device) != cudaSuccess) return PTG_ERR_CUDA;
+  const int64_t ntg = b->ntask_per_geo;
+  const size_t ntot = (size_t)b->ngeo * (size_t)ntg;
+  /* 1. forward pass over all geometries that lists the transmitted samples */
+  unsigned long long total = 0;
+  for (int g = 0; g < b->ngeo; ++g) {
+    const int64_t npl = b->np[g] > b->run.rank
+                            ? (b->np[g] - b->run.rank + b->run.nranks - 1) / b->run.nranks : 0;
+    total += (unsigned long long)ntg * (unsigned long long)npl;
+  }
+  const unsigned long long cap = std::min<unsigned long long>(total, 1ull << 26);
+  if (b->adj_list_cap < cap || !b->adj_list.p) {
+    if (b->adj_list.p) { cudaFree(b->adj_list.p); b->adj_list.p = nullptr; }
+    if (b->adj_list.alloc(sizeof(unsigned long long) * (cap ? cap : 1)) != cudaSuccess) return PTG_ERR_NOMEM;
+    b->adj_list_cap = cap;
+  }
+  if (!b->adj_w.p && b->adj_w.alloc(sizeof(float) * ntot) != cudaSuccess) return PTG_ERR_NOMEM;
+  if (!b->adj_acc.p && b->adj_acc.alloc(sizeof(double) * b->adj_acc_n) != cudaSuccess) return PTG_ERR_NOMEM;
+  ptg::RunF32 r = b->r;
+  r.tlist = b->adj_list.as<unsigned long long>();
+  r.tlist_cap = cap;
+  unsigned long long st[ptg::kStatSlots];
+  float fwd_ms = 0.f, rep_ms = 0.f;
+  int rc = batch_launch(b, r, ptg::MODE_LIST, st, &fwd_ms);
+  if (rc != PTG_OK) return rc;
+  const unsigned long long nlist = st[10];
+  if (nlist > cap) return PTG_ERR_UNSUPPORTED;
+  const uint64_t fwd_flights = st[0];
+  std::vector<uint64_t> counts(ntot);
+  if (cudaMemcpy(counts.data(), b->counts.p, sizeof(uint64_t) * ntot, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return PTG_ERR_CUDA;
+  /* 2. every geometry's kappa and d kappa / d T_task on the host */
+  std::vector<float> wsample(ntot);
+  std::vector<double> dks_an(b->ngeo, 0.0), wtask;
+  for (int g = 0; g < b->ngeo; ++g) {
+    ptg_run rg = b->run;
+    rg.np = b->np[g];
+    ptg_kappa_out ko;
+    memset(&ko, 0, sizeof(ko));
+    rc = ptg::assemble_host(b->spec, &rg, b->box_x[g], counts.data() + (size_t)g * ntg, &ko, &wtask,
+                            &dks_an[g]);
+    if (rc != PTG_OK) return rc;
+    if (out->kappa) out->kappa[g] = ko.kappa;
+    if (out->kappa_stderr) out->kappa_stderr[g] = ko.kappa_stderr;
+    for (int64_t t = 0; t < ntg; ++t)
+      wsample[(size_t)g * ntg + t] = (float)(wtask[t] / (double)b->np[g]);
+  }
+  if (cudaMemcpyAsync(b->adj_w.p, wsample.data(), sizeof(float) * ntot, cudaMemcpyHostToDevice,
+                      b->stream) != cudaSuccess ||
+      cudaMemsetAsync(b->adj_acc.p, 0, sizeof(double) * b->adj_acc_n, b->stream) != cudaSuccess)
+    return PTG_ERR_CUDA;
+  /* 3. replay of every listed sample, scores into its geometry's slice */
+  r = b->r;
+  r.alist = b->adj_list.as<const unsigned long long>();
+  r.alist_n = (long long)nlist;
+  r.wsample = b->adj_w.as<const float>();
+  r.adj = b->adj_acc.as<double>();
+  rc = batch_launch(b, r, ptg::MODE_ADJOINT, st, &rep_ms);
+  if (rc != PTG_OK) return rc;
+  std::vector<double> acc(b->adj_acc_n);
+  if (cudaMemcpy(acc.data(), b->adj_acc.p, sizeof(double) * b->adj_acc_n, cudaMemcpyDeviceToHost) !=
+      cudaSuccess)
+    return PTG_ERR_CUDA;
+  /* 4. batch sums and standard errors per geometry */
+  const int B = ptg::kAdjBatches;
+  size_t rec = 0;
+  for (int g = 0; g < b->ngeo; ++g) {
+    const int ns = b->nsurf[g];
+    const double* a = acc.data() + b->adj_base[g];
+    auto reduce = [&](int col, double* total_v, double* se) {
+      double sum = 0.0, sq = 0.0;
+      for (int k = 0; k < B; ++k) sum += a[(size_t)k * (ns + 1) + col];
+      const double mb = sum / B;
+      for (int k = 0; k < B; ++k) {
+        const double d = a[(size_t)k * (ns + 1) + col] - mb;
+        sq += d * d;
+      }
+      *total_v = sum;
+      *se = sqrt((double)B * sq / (B - 1));
+    };
+    for (int k = 0; k < ns; ++k, ++rec) {
+      double v, e;
+      reduce(k, &v, &e);
+      const double p = b->specularity[g][k];
+      const bool interior = p > 0.0 && p < 1.0;
+      if (out->dk_dp) out->dk_dp[rec] = interior ? v : NAN;
+      if (out->dk_dp_stderr) out->dk_dp_stderr[rec] = interior ? e : NAN;
+    }
+    double vs, es;
+    reduce(ns, &vs, &es);
+    if (out->dk_dscale) out->dk_dscale[g] = (b->run.kind_mfp == PTG_MFP_PER_MODE ? vs : 0.0) + dks_an[g];
+    if (out->dk_dscale_stderr) out->dk_dscale_stderr[g] = b->run.kind_mfp == PTG_MFP_PER_MODE ? es : 0.0;
+  }
+  out->flights = fwd_flights + st[0];
+  out->replayed = nlist;
+  out->mismatched = st[11];
+  out->kernel_ms = (double)fwd_ms + (double)rep_ms;
   return PTG_OK;
 }
 

@@ -115,6 +115,8 @@ struct GeoEntry {
   long long np;                /* particles per task of this geometry        */
   unsigned k0, k1, c1;         /* Philox key and stream word                 */
   int task_base;               /* first global task of this geometry         */
+  int nsurf;                   /* its surfaces (adjoint replay)               */
+  int adj_base;                /* its adjoint accumulators' first element    */
 };
 
 /* Per task (FP32): lambda (inf = ballistic, <= 0 skipped), cos, sin, omega/max_omega */
@@ -136,6 +138,9 @@ struct RunF32 {
                                  advances it 32 flights a round (0: off)          */
   float4* tail;               /* tail list: 6 float4 per phonon                    */
   int32_t tail_cap;           /* its capacity in phonons                           */
+  int32_t stage_test;         /* test only: set up the shared-memory staging
+                                 barrier without issuing the copy, so its
+                                 bounded wait runs out (PTG_ERR_TIMEOUT)          */
   unsigned long long* counts;
   unsigned long long* lost;
   /* flights, lost, capped, samples, max trajectory flights,
@@ -144,7 +149,8 @@ struct RunF32 {
   unsigned long long* stats;
   int* queue;                 /* [0] next chunk, [1] error flags, [2] / [4] phonons
                                  put at the front / back of the tail list, [3]
-                                 next tail-list phonon (8 ints) */
+                                 next tail-list phonon, [5] tail-list requests
+                                 (8 ints) */
   /* adjoint support */
   unsigned long long* tlist;  /* mode 1: sample ids of transmitted phonons         */
   unsigned long long tlist_cap;
@@ -194,10 +200,13 @@ cudaError_t launch_tail_fp32(const GeoF32& g, const RunF32& r, int grid, int blo
                              cudaStream_t st, int mode = MODE_FORWARD);
 cudaError_t tail_occupancy(int block, size_t smem, int* blocks_per_sm, int mode = MODE_FORWARD,
                            bool bvh = false);
-/* Batched launch over several geometries (forward mode, geometry in global memory). */
+/* Batched launch over several geometries (geometry in global memory):
+   forward, list (ids of transmitted samples as (global task << 32) |
+   particle) or adjoint replay of such a list. */
 cudaError_t launch_persistent_batch(const RunF32& r, int grid, int block, cudaStream_t st,
-                                    bool bvh);
-cudaError_t persistent_batch_occupancy(int block, int* blocks_per_sm, bool bvh);
+                                    bool bvh, int mode = MODE_FORWARD);
+cudaError_t persistent_batch_occupancy(int block, int* blocks_per_sm, bool bvh,
+                                       int mode = MODE_FORWARD);
 /* Residency of the persistent kernel for a block size and shared memory. */
 cudaError_t persistent_occupancy(int block, size_t smem, int* blocks_per_sm,
                                  int mode = MODE_FORWARD, bool bvh = false);

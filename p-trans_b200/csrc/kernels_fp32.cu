@@ -547,10 +547,36 @@ __device__ __forceinline__ void warp_add_by_task(bool pred, int task, unsigned l
   }
 }
 
+/* Bound of one wait on the staging barrier, in global-timer nanoseconds:
+   the copy (at most 96 KB) takes microseconds. */
+constexpr unsigned long long kStageWaitNs = 200000000ull;
+
+/* Polls phase 0 of a shared-memory mbarrier until it completes or the global
+   timer passes the deadline; returns 1 when it completed. */
+__device__ unsigned wait_phase0(unsigned bar_a, unsigned long long deadline) {
+  unsigned done = 0;
+  for (int it = 0; it < (1 << 26) && !done; ++it) {
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(bar_a)
+        : "memory");
+    if (!done && globaltimer() > deadline) break;
+  }
+  return done;
+}
+
 /* Copies the geometry blob into shared memory with one bulk asynchronous
-   copy completed on an mbarrier.  The wait is bounded; on timeout the block
-   records an error and falls back to the global copy. */
-__device__ bool stage_blob(const float4* gblob, float4* sblob, int units, int* err) {
+   copy completed on an mbarrier.  The wait is bounded (kStageWaitNs).  On a
+   timeout the block sets bit 0 of *err, waits once more, with the same bound,
+   for the copy it issued (so that none of its writes can land in shared
+   memory after the block has left), and returns false: the block then takes
+   no work (the others drain the work queue) and the host returns
+   PTG_ERR_TIMEOUT.  issue_copy = false (a test-only option) sets the barrier
+   up without issuing the copy, so that the wait runs out with nothing in
+   flight. */
+__device__ bool stage_blob(const float4* gblob, float4* sblob, int units, int* err,
+                           bool issue_copy) {
   __shared__ alignas(8) unsigned long long bar;
   const unsigned bar_a = (unsigned)__cvta_generic_to_shared(&bar);
   const unsigned dst_a = (unsigned)__cvta_generic_to_shared(sblob);
@@ -564,22 +590,22 @@ __device__ bool stage_blob(const float4* gblob, float4* sblob, int units, int* e
   if (threadIdx.x == 0) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(bytes)
                  : "memory");
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            dst_a),
-        "l"(gblob), "r"(bytes), "r"(bar_a)
-        : "memory");
+    if (issue_copy)
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+              dst_a),
+          "l"(gblob), "r"(bytes), "r"(bar_a)
+          : "memory");
   }
-  unsigned done = 0;
-  for (int it = 0; it < (1 << 20) && !done; ++it) {
-    asm volatile(
-        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
-        : "=r"(done)
-        : "r"(bar_a)
-        : "memory");
-  }
+  const unsigned done = wait_phase0(bar_a, globaltimer() + kStageWaitNs);
   const int ok = __syncthreads_and((int)done);
-  if (!ok && threadIdx.x == 0) atomicOr(err, 1);
+  if (!ok) {
+    if (threadIdx.x == 0) {
+      atomicOr(err, 1);
+      if (issue_copy) wait_phase0(bar_a, globaltimer() + kStageWaitNs);
+    }
+    __syncthreads();
+  }
   return ok != 0;
 }
 
@@ -624,8 +650,9 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   G.base = gp.blob;
   if (PH == PH_DRAIN && threadIdx.x == 0) atomicMin(r.stats + 5, globaltimer());
   if (SMEM) {
-    /* on a timeout the block records the error and leaves: the host reports it */
-    if (!stage_blob(gp.blob, sblob, gp.lay.total, r.queue + 1)) return;
+    /* on a timeout the block records the error and takes no work: the host
+       reports it */
+    if (!stage_blob(gp.blob, sblob, gp.lay.total, r.queue + 1, r.stage_test == 0)) return;
   }
   const int lane = threadIdx.x & 31;
   /* geometry and run scalars: kernel-wide, or per lane in a batched launch */
@@ -650,10 +677,13 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
      long ones from the front of the list, the others from the back */
   const int nlong = PH == PH_TAIL ? min(r.queue[2], r.tail_cap) : 0;
   const int ntail = PH == PH_TAIL ? nlong + min(r.queue[4], r.tail_cap - nlong) : 0;
-  const int adj_stride = r.nsurf + 1;
-  const bool adj_in_smem = (MODE == MODE_ADJOINT) && kAdjBatches * adj_stride <= kAdjSmemDoubles;
+  /* accumulators of the sample's geometry: [kAdjBatches][nsurf + 1] at
+     adj_off (a batched replay sets both per sample, in global memory) */
+  int adj_stride = r.nsurf + 1, adj_off = 0;
+  const bool adj_in_smem =
+      (MODE == MODE_ADJOINT) && !BATCH && kAdjBatches * (r.nsurf + 1) <= kAdjSmemDoubles;
   if (MODE == MODE_ADJOINT && adj_in_smem) {
-    for (int i = threadIdx.x; i < kAdjBatches * adj_stride; i += blockDim.x) adj_sh[i] = 0.0;
+    for (int i = threadIdx.x; i < kAdjBatches * (r.nsurf + 1); i += blockDim.x) adj_sh[i] = 0.0;
     __syncthreads();
   }
   float adj_w = 0.0f, adj_len = 0.0f;   /* weight of the sample, path length */
@@ -665,6 +695,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   /* warp-uniform chunk cursor */
   int ch_task = -1, ch_next = 0, ch_left = 0;
   bool queue_done = false;
+  bool tail_full = false;  /* the tail list refused this warp: stop asking */
 
   /* lane state */
   bool alive = false;
@@ -739,9 +770,20 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
         const int rank = __popc(idle & lanemask_lt());
         if (((idle >> lane) & 1u) && rank < take) {
           uint64_t sample;
+          const GeoEntry* ge = nullptr;  /* batched launch: the sample's geometry */
           if (MODE == MODE_ADJOINT) {
-            sample = r.alist[ch_next + rank];
-            task = (int)(sample / (uint64_t)r.np);
+            const unsigned long long id = r.alist[ch_next + rank];
+            if (BATCH) {
+              /* batched list entries are (global task << 32) | particle */
+              task = (int)(id >> 32);
+              ge = r.geos + __ldg(r.task_geo + task);
+              sample = (uint64_t)(task - ge->task_base) * (uint64_t)ge->np + (id & 0xffffffffull);
+              adj_stride = ge->nsurf + 1;
+              adj_off = ge->adj_base;
+            } else {
+              sample = id;
+              task = (int)(sample / (uint64_t)r.np);
+            }
             adj_w = r.wsample[task];
             adj_b = (int)(sample % kAdjBatches);
             adj_len = 0.0f;
@@ -753,21 +795,23 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           } else if (BATCH) {
             const int64_t p = (int64_t)r.rank + (int64_t)(ch_next + rank) * r.nranks;
             task = ch_task;
-            const GeoEntry* e = r.geos + __ldg(r.task_geo + task);
-            G.base = e->blob;
-            G.lay = e->lay;
-            X = e->box[0]; Y = e->box[1]; Z = e->box[2];
-            eps = e->eps;
-            key.k0 = e->k0; key.k1 = e->k1;
-            c1 = e->c1;
-            pmask = e->periodic_mask;
-            nmat = e->nmaterial;
-            flmax = e->fast_lambda_max;
-            sample = (uint64_t)(task - e->task_base) * (uint64_t)e->np + (uint64_t)p;
+            ge = r.geos + __ldg(r.task_geo + task);
+            sample = (uint64_t)(task - ge->task_base) * (uint64_t)ge->np + (uint64_t)p;
           } else {
             const int64_t p = (int64_t)r.rank + (int64_t)(ch_next + rank) * r.nranks;
             sample = (uint64_t)ch_task * (uint64_t)r.np + (uint64_t)p;
             task = ch_task;
+          }
+          if (BATCH && ge) {
+            G.base = ge->blob;
+            G.lay = ge->lay;
+            X = ge->box[0]; Y = ge->box[1]; Z = ge->box[2];
+            eps = ge->eps;
+            key.k0 = ge->k0; key.k1 = ge->k1;
+            c1 = ge->c1;
+            pmask = ge->periodic_mask;
+            nmat = ge->nmaterial;
+            flmax = ge->fast_lambda_max;
           }
           slo = (uint32_t)sample;
           shi = (uint32_t)(sample >> 32);
@@ -833,12 +877,21 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
     }
     /* ---- drain phase, queue dry: diffusive phonons go to the tail list */
     if (PH == PH_DRAIN && !BATCH && MODE != MODE_TRACE && queue_done && r.coop_lanes > 0 &&
-        __popc(__ballot_sync(FULL, alive)) <= r.coop_lanes) {
-      const unsigned mv = __ballot_sync(FULL, alive && lam < flmax);
-      if (mv) {
-        /* long phonons fill the list from the front, the others from the
-           back; a lane hands over at most one phonon, so the two never meet
-           in a list with a slot per lane */
+        !tail_full && __popc(__ballot_sync(FULL, alive)) <= r.coop_lanes) {
+      const unsigned mw = __ballot_sync(FULL, alive && lam < flmax);
+      if (mw) {
+        /* a slot is reserved from one counter of all requests (queue[5])
+           before the phonon picks its end of the list: the phonons admitted
+           number at most tail_cap, so the long ones, filling the list from
+           the front, and the others, filling it from the back, never meet
+           whatever the list's size; a phonon past the capacity stays here */
+        const int fw = __ffs(mw) - 1;
+        int bw = 0;
+        if (lane == fw) bw = atomicAdd(r.queue + 5, __popc(mw));
+        bw = __shfl_sync(FULL, bw, fw);
+        const unsigned mv =
+            mw & __ballot_sync(FULL, bw + __popc(mw & lanemask_lt()) < r.tail_cap);
+        if (mv != mw) tail_full = true;
         const unsigned ml = mv & __ballot_sync(FULL, flight >= kTailLong);
         const unsigned ms = mv & ~ml;
         const int fl = ml ? __ffs(ml) - 1 : 0, fs = ms ? __ffs(ms) - 1 : 0;
@@ -1301,7 +1354,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
                 if (pk > 0.0f && pk < 1.0f) {
                   const double sc = (u0 <= pk) ? 1.0 / (double)pk : -1.0 / (1.0 - (double)pk);
                   const double v = (double)adj_w * sc;
-                  const int idx = adj_b * adj_stride + sb;
+                  const int idx = adj_off + adj_b * adj_stride + sb;
                   if (adj_in_smem) atomicAdd(&adj_sh[idx], v);
                   else atomicAdd(&r.adj[idx], v);
                 }
@@ -1364,7 +1417,16 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
         if (lane == __ffs(m) - 1) base = atomicAdd(r.stats + 10, (unsigned long long)__popc(m));
         base = __shfl_sync(FULL, base, __ffs(m) - 1);
         const unsigned long long at = base + __popc(m & lanemask_lt());
-        if (put && at < r.tlist_cap) r.tlist[at] = ((unsigned long long)shi << 32) | slo;
+        if (put && at < r.tlist_cap) {
+          unsigned long long id = ((unsigned long long)shi << 32) | slo;
+          if (BATCH) {
+            /* (global task << 32) | particle: the replay finds the geometry */
+            const GeoEntry* e = r.geos + __ldg(r.task_geo + task);
+            id = ((unsigned long long)task << 32) |
+                 (id - (unsigned long long)(task - e->task_base) * (unsigned long long)e->np);
+          }
+          r.tlist[at] = id;
+        }
       }
     }
     if (MODE == MODE_TRACE && fin) {
@@ -1375,7 +1437,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
       if (end_side == 2) {
         /* d log P / d s of the exponential free paths at rate s / lambda */
         const double v = (double)adj_w * ((double)adj_npp - (double)adj_len / (double)lam);
-        const int idx = adj_b * adj_stride + r.nsurf;
+        const int idx = adj_off + adj_b * adj_stride + adj_stride - 1;
         if (!isinf(lam)) {
           if (adj_in_smem) atomicAdd(&adj_sh[idx], v);
           else atomicAdd(&r.adj[idx], v);
@@ -1429,7 +1491,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   }
   if (MODE == MODE_ADJOINT && adj_in_smem) {
     __syncthreads();
-    for (int i = threadIdx.x; i < kAdjBatches * adj_stride; i += blockDim.x)
+    for (int i = threadIdx.x; i < kAdjBatches * (r.nsurf + 1); i += blockDim.x)
       if (adj_sh[i] != 0.0) atomicAdd(&r.adj[i], adj_sh[i]);
   }
 }
@@ -1470,21 +1532,38 @@ cudaError_t launch_mode(const GeoF32& g, const RunF32& r, int grid, int block, s
   return cudaGetLastError();
 }
 
-cudaError_t persistent_batch_occupancy(int block, int* bps, bool bvh) {
+template <int MODE>
+cudaError_t batch_occupancy_mode(int block, int* bps, bool bvh) {
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
       bps,
-      bvh ? k_persistent<false, MODE_FORWARD, true, true, PH_DRAIN>
-          : k_persistent<false, MODE_FORWARD, true, false, PH_DRAIN>,
+      bvh ? k_persistent<false, MODE, true, true, PH_DRAIN>
+          : k_persistent<false, MODE, true, false, PH_DRAIN>,
       block, 0);
 }
 
-cudaError_t launch_persistent_batch(const RunF32& r, int grid, int block, cudaStream_t st, bool bvh) {
-  if (block != kBlock) return cudaErrorInvalidConfiguration;
+cudaError_t persistent_batch_occupancy(int block, int* bps, bool bvh, int mode) {
+  if (mode == MODE_LIST) return batch_occupancy_mode<MODE_LIST>(block, bps, bvh);
+  if (mode == MODE_ADJOINT) return batch_occupancy_mode<MODE_ADJOINT>(block, bps, bvh);
+  if (mode != MODE_FORWARD) return cudaErrorInvalidValue;
+  return batch_occupancy_mode<MODE_FORWARD>(block, bps, bvh);
+}
+
+template <int MODE>
+cudaError_t launch_batch_mode(const RunF32& r, int grid, int block, cudaStream_t st, bool bvh) {
   GeoF32 g;
   memset(&g, 0, sizeof(g));
-  if (bvh) k_persistent<false, MODE_FORWARD, true, true, PH_DRAIN><<<grid, block, 0, st>>>(g, r);
-  else k_persistent<false, MODE_FORWARD, true, false, PH_DRAIN><<<grid, block, 0, st>>>(g, r);
+  if (bvh) k_persistent<false, MODE, true, true, PH_DRAIN><<<grid, block, 0, st>>>(g, r);
+  else k_persistent<false, MODE, true, false, PH_DRAIN><<<grid, block, 0, st>>>(g, r);
   return cudaGetLastError();
+}
+
+cudaError_t launch_persistent_batch(const RunF32& r, int grid, int block, cudaStream_t st, bool bvh,
+                                    int mode) {
+  if (block != kBlock) return cudaErrorInvalidConfiguration;
+  if (mode == MODE_LIST) return launch_batch_mode<MODE_LIST>(r, grid, block, st, bvh);
+  if (mode == MODE_ADJOINT) return launch_batch_mode<MODE_ADJOINT>(r, grid, block, st, bvh);
+  if (mode != MODE_FORWARD) return cudaErrorInvalidValue;
+  return launch_batch_mode<MODE_FORWARD>(r, grid, block, st, bvh);
 }
 
 /* The tail phase exists for the modes with cooperative rounds (forward,

@@ -177,7 +177,11 @@ extern "C" int ptg_transmission_noalloc(ptg_handle* h, double mfp_nm, int32_t na
   r.queue = queue;
   /* the tail phase as in ptg_transmission (tune_flags bit 1 turns it off) */
   r.coop_lanes = (v.opt.tune_flags & 2) ? 0 : (v.opt.coop_lanes > 0 ? std::min(v.opt.coop_lanes, 32) : 32);
-  const int block = 256;
+  r.stage_test = (v.opt.tune_flags & 4) ? 1 : 0;
+  /* the block size rule of ptg_transmission: opt.block_size when it is a
+     multiple of 32 up to 256, else 256 */
+  const int bs = v.opt.block_size;
+  const int block = (bs >= 32 && bs <= 256 && bs % 32 == 0) ? bs : 256;
   const size_t smem = v.g32.stage_smem ? v.blob_bytes : 0;
   int bps = 0;
   if (ptg::persistent_occupancy(block, smem, &bps, ptg::MODE_FORWARD, v.g32.has_ext != 0) !=
@@ -188,6 +192,9 @@ extern "C" int ptg_transmission_noalloc(ptg_handle* h, double mfp_nm, int32_t na
   const int grid = v.num_sms * bps;
   int tgrid = 0;
   if (r.coop_lanes > 0) {
+    /* the drain kernel admits at most tail_cap hand-overs in total (one
+       counter of all requests), so a grid with more lanes than the list
+       holds keeps the extra phonons in the drain phase */
     r.tail = reinterpret_cast<float4*>(base + kOffTail);
     r.tail_cap = std::min(kMaxTail, grid * block);
     int tbps = 0;
@@ -202,19 +209,56 @@ extern "C" int ptg_transmission_noalloc(ptg_handle* h, double mfp_nm, int32_t na
       return PTG_ERR_CUDA;
   }
   /* the counts land in the caller's transmit array (ntask <= its length),
-     then become count / np in place; the last angle is zero */
-  int qerr[4] = {0, 0, 0, 0};
+     then become count / np in place; the last angle is zero.  Statistics and
+     queue counters come back into stack arrays. */
+  int qerr[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  unsigned long long sv[ptg::kStatSlots];
   if (cudaMemcpyAsync(transmit, counts, sizeof(unsigned long long) * ntask, cudaMemcpyDeviceToHost,
                       s) != cudaSuccess ||
       cudaMemcpyAsync(qerr, queue, sizeof(qerr), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-      cudaStreamSynchronize(s) != cudaSuccess)
+      cudaMemcpyAsync(sv, stats, sizeof(sv), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess) {
+    for (int64_t t = 0; t < nmode * nangle; ++t) transmit[t] = 0.0;
     return PTG_ERR_CUDA;
-  if (qerr[1] != 0) return PTG_ERR_TIMEOUT;
+  }
+  /* the handle's record of its last call, as ptg_transmission leaves it
+     (no kernel times: this entry records no events) */
+  ptg_stats* L = v.last;
+  memset(L, 0, sizeof(*L));
+  L->flights = sv[0];
+  L->lost = sv[1];
+  L->capped = sv[2];
+  L->samples = sv[3];
+  L->max_traj_flights = sv[4];
+  L->full_flights = sv[8];
+  L->safe_balls = sv[9];
+  L->coop_rounds = sv[12];
+  L->coop_flights = sv[13];
+  L->box_tests = sv[14];
+  L->surface_tests = sv[15];
+  L->launches = 1 + (r.nchunk > 0 ? (tgrid > 0 ? 2 : 1) : 0);
+  L->grid = grid;
+  L->block = block;
+  L->h2d_bytes = sizeof(double) * nmode;
+  L->d2h_bytes = sizeof(unsigned long long) * ntask + sizeof(qerr) + sizeof(sv);
+  if (tgrid > 0) {
+    ptg::tail_counts(qerr, r.tail_cap, &L->tail_phonons, &L->tail_refused);
+    L->tail_flights = sv[17] >= sv[16] ? sv[17] - sv[16] : 0;
+  }
+  if (qerr[1] != 0) {
+    /* a staging wait ran out: the counts are incomplete, return none */
+    for (int64_t t = 0; t < nmode * nangle; ++t) transmit[t] = 0.0;
+    return PTG_ERR_TIMEOUT;
+  }
   for (int64_t t = 0; t < ntask; ++t) {
     unsigned long long c;
     memcpy(&c, &transmit[t], sizeof(c));
     transmit[t] = (double)c / (double)np;
   }
   for (int64_t t = ntask; t < nmode * nangle; ++t) transmit[t] = 0.0;
+  /* the lost-phonon limit of ptg_transmission */
+  if (v.opt.lost_limit > 0.0 && L->samples > 0 &&
+      (double)L->lost > v.opt.lost_limit * (double)L->samples)
+    return PTG_ERR_LOST;
   return PTG_OK;
 }

@@ -82,8 +82,21 @@ struct NoallocView {
   ptg_options opt;
   const SpecSoA* spec;
   const GeomSoA* geom;
+  ptg_stats* last;   /* the handle's record of its last call (plain struct) */
 };
 int handle_noalloc_view(ptg_handle* h, NoallocView* v);
+
+/* Phonons handed to the tail list and hand-overs refused for lack of room,
+   from the drain kernel's queue counters (queue[2] long, queue[4] short,
+   queue[5] all requests) and the list's capacity. */
+inline void tail_counts(const int* queue, int cap, uint64_t* handed, uint64_t* refused) {
+  const int64_t lng = queue[2] < 0 ? 0 : queue[2], sht = queue[4] < 0 ? 0 : queue[4];
+  int64_t got = lng + sht;
+  if (got > cap) got = cap;
+  const int64_t req = queue[5] < 0 ? 0 : queue[5];
+  *handed = (uint64_t)got;
+  *refused = (uint64_t)(req > got ? req - got : 0);
+}
 
 /* FP32 geometry blob (host copy) of a built geometry; grains with more than
    kBvhMinCand candidates get a BVH with leaves of bvh_leaf surfaces

@@ -37,7 +37,7 @@ module ptrans_gpu
     integer(c_int64_t) :: max_flights = 0
     real(c_double) :: lost_limit = 0.0d0
     integer(c_int64_t) :: chunk = 0
-    integer(c_int32_t) :: tune_flags = 0, fast_steps = 0, coop_lanes = 0, long_flights = 0
+    integer(c_int32_t) :: tune_flags = 0, fast_steps = 0, coop_lanes = 0, reserved = 0
   end type ptg_options
 
   public :: ptg_create, ptg_destroy, ptg_transmission, ptg_strerror_f

@@ -146,6 +146,30 @@ def brick_box(l: float = 200.0, lo=(60.0, 60.0, 60.0), hi=(140.0, 140.0, 140.0),
         cellspec=(1.0, 1.0, p_wall, p_wall, p_wall, p_wall), tt_kind=kind, tt_trans=tt, tt_spec=ts)
 
 
+def with_interface(model: Model, kind: int, param: float, spec: float = 0.0,
+                   two_materials: bool = False) -> Model:
+    """The model with every internal interface of the given transmission kind
+    (the Nt table, src/RTMCphon.f90:749-890, 1402-1429): TRANS_VALUE with
+    param = T, or TRANS_GAMMA / TRANS_TBC with param = gamma (a TBC entry is
+    solved to gamma on the host first: abi.gamma_from_tbc).  With one material
+    the kernels draw against T(omega) = 1/(gamma omega/omega_max + 1); with two
+    (the inclusions of material 2 in a matrix of material 1) the threshold is
+    random, t11 + u (1 - t11), t11 = 1/(gamma + 1) (src/RTMCphon.f90:2391-2402)."""
+    import dataclasses
+    if not two_materials:
+        kind_t, tt, ts = _table(param, spec, kind)
+        return dataclasses.replace(model, tt_kind=kind_t, tt_trans=tt, tt_spec=ts, nmaterial=1, nt1=1, nt2=1)
+    # param%X(nt2+1, nt1), nt1 = nt2 = 2: rows 1..2 are materials, row 3 the boundary
+    kind_t = np.full(6, kind, np.int32)
+    tt = np.full(6, float(param))
+    ts = np.full(6, float(spec))
+    for i1 in (1, 2):
+        k = 2 + 3 * (i1 - 1)
+        kind_t[k], tt[k], ts[k] = TRANS_VALUE, 0.0, 0.0
+    return dataclasses.replace(model, tt_kind=kind_t, tt_trans=tt, tt_spec=ts, nmaterial=2, nt1=2, nt2=2,
+                               grain_material=np.full(model.ngrain, 2, np.int32))
+
+
 def write_mcp(model: Model, path: str, np_: int = 100, nangle: int = 11,
               mean_free_path: Optional[str] = None, material: str = "Si", trace: int = 1000):
     """Writes the model as a .mcp file in the reference's layout."""

@@ -1,7 +1,7 @@
 """Writes tests/golden/examples_summary.json from the reference's Examples/*.mcp.
 
-Run here, where the reference is mounted (read-only):
-    python tests/golden/make_examples_summary.py /root/reference/Examples
+Run where a checkout of the reference is at hand:
+    python tests/golden/make_examples_summary.py <P-TRANS checkout>/Examples
 
 The figures are counted by plain text scanning, independently of the C++
 reader under test: grains (the "Ng" value), model surfaces (material_to
@@ -75,4 +75,6 @@ def main(d):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/Examples")
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_examples_summary.py <P-TRANS checkout>/Examples")
+    main(sys.argv[1])

@@ -37,3 +37,43 @@ def test_batch_equals_individual_runs():
         np.testing.assert_allclose(r1["bin_T"][g], k["bin_T"], rtol=1e-12, atol=1e-15)
     assert r1["samples"] == sum(nps) * 40 * 8
     assert r1["lost"] == 0
+
+
+def test_batch_adjoint_equals_individual_adjoints():
+    """ptg_batch_adjoint gives every geometry what ptg_adjoint gives for its
+    own run: the same kappa (the same counts), the same replayed samples, and
+    the same derivatives up to the order of the FP64 sums (the scores of the
+    same samples, added in another order)."""
+    import dataclasses
+    models, _ = synth.film_batch(n=4, seed=5, n_modes=12, nangle=7)
+    models = [dataclasses.replace(m, tt_spec=np.array([0.4, 0.0]), cellspec=(1.0, 1.0, 1.0, 1.0, 0.5, 0.3))
+              for m in models]
+    nps = [200, 50, 400, 10]
+    seeds = [11, 12, 13, 14]
+    streams = [0, 3, 1, 0]
+    spec = synth.spectrum(12, seed=2)
+    bins = (0.0, float(spec.omega.max()))
+    bufs = [A.GeomBuf(m) for m in models]
+    run = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=7, np_=1, nbins=4, bin_omega=bins, precision=A.PREC_FP32)
+    with A.Batch([b.view for b in bufs], nps, seeds, streams, spec, run) as bt:
+        ba = bt.adjoint()
+        fwd = bt.run()
+    assert ba["mismatched"] == 0
+    np.testing.assert_array_equal(ba["kappa"], fwd["kappa"])
+    replayed = 0
+    for g in range(len(models)):
+        single = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=7, np_=nps[g], seed=seeds[g], stream=streams[g],
+                            nbins=4, bin_omega=bins, precision=A.PREC_FP32)
+        with A.Handle(bufs[g].view, spec) as h:
+            sa = h.adjoint(single)
+        replayed += sa["replayed"]
+        assert ba["kappa"][g] == pytest.approx(sa["kappa"], rel=1e-12)
+        assert ba["kappa_stderr"][g] == pytest.approx(sa["kappa_stderr"], rel=1e-10)
+        got, want, se = ba["dk_dp"][g], sa["dk_dp"], sa["dk_dp_stderr"]
+        np.testing.assert_array_equal(np.isnan(got), np.isnan(want))
+        ok = ~np.isnan(want)
+        assert ok.sum() >= 3
+        assert np.all(np.abs(got[ok] - want[ok]) <= 1e-6 * se[ok] + 1e-12 * np.abs(want[ok]))
+        np.testing.assert_allclose(ba["dk_dp_stderr"][g][ok], se[ok], rtol=1e-6)
+        assert abs(ba["dk_dscale"][g] - sa["dk_dscale"]) <= 1e-6 * sa["dk_dscale_stderr"] + 1e-12 * abs(sa["dk_dscale"])
+    assert ba["replayed"] == replayed

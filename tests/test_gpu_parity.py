@@ -20,7 +20,17 @@ from ptrans_b200 import synth
 pytestmark = pytest.mark.gpu
 
 
+def _tbc_gamma(tbc=3.0e8):
+    """gamma of a TBC entry (GammaDeterm on the host) for a fixed material."""
+    st, g = A.gamma_from_tbc(synth.spectrum(200, seed=0), 300.0, tbc)
+    assert st == 0
+    return g
+
+
 def geometries():
+    spheres = synth.spheres_in_box(l=200.0, centres=((70, 90, 100), (140, 110, 90)), radii=(35, 40),
+                                   t=0.5, p=0.3, p_wall=0.2)
+    brick = synth.brick_box(t=0.5, p=0.2, p_wall=0.1)
     return {
         "nanowire_diffuse": synth.nanowire(length=300.0, width=60.0, height=50.0, p_side=0.0),
         "nanowire_mixed": synth.nanowire(length=300.0, width=60.0, height=50.0, p_side=0.6),
@@ -36,6 +46,12 @@ def geometries():
         "capped": synth.spheres_cylinders_box(n_spheres=4, n_cylinders=5, l=300.0, seed=3,
                                               r_sphere=(15.0, 35.0), r_cylinder=20.0, length=(50.0, 150.0),
                                               trans=0.3, p_wall=0.2),
+        # Gamma / TBC interfaces: per-mode threshold (one material) and random
+        # threshold (two materials), src/RTMCphon.f90:1417-1424, 2391-2402
+        "spheres_gamma": synth.with_interface(spheres, A.TRANS_GAMMA, 0.8, spec=0.3),
+        "spheres_gamma_2mat": synth.with_interface(spheres, A.TRANS_GAMMA, 0.8, spec=0.3, two_materials=True),
+        "brick_tbc": synth.with_interface(brick, A.TRANS_TBC, _tbc_gamma(), spec=0.2),
+        "brick_tbc_2mat": synth.with_interface(brick, A.TRANS_TBC, _tbc_gamma(), spec=0.2, two_materials=True),
     }
 
 
@@ -61,7 +77,8 @@ def test_fp64_replay_is_bit_exact(orc, name):
             np.testing.assert_array_equal(fp_g, fp_o)
 
 
-@pytest.mark.parametrize("name", ["nanowire_diffuse", "film_periodic", "spheres", "brick_tris"])
+@pytest.mark.parametrize("name", ["nanowire_diffuse", "film_periodic", "spheres", "brick_tris",
+                                  "spheres_gamma", "brick_tbc_2mat"])
 def test_fp64_counts_equal_oracle(orc, name):
     m, spec, gb = setup(name, nmode=10)
     o = orc.Oracle(model=m, spectrum=spec)
@@ -106,7 +123,8 @@ def _z(c1, c2, n):
 
 
 @pytest.mark.parametrize("name", ["nanowire_diffuse", "film_periodic", "film_mirror_transmit", "spheres",
-                                  "brick_quads", "brick_tris"])
+                                  "brick_quads", "brick_tris", "spheres_gamma", "spheres_gamma_2mat",
+                                  "brick_tbc", "brick_tbc_2mat"])
 def test_fp32_statistical_parity(orc, name):
     """Per-mode transmission sums and kappa of the FP32 kernel vs the oracle:
     every |z| < 5 and the kappa difference within 4 combined standard errors."""
@@ -319,3 +337,35 @@ def test_fp32_diffusive_limit_is_milne(lam):
     sigma = s * math.sqrt(np.sum((c * np.sin(th) * np.cos(th)) ** 2 * t * (1 - t) / npart))
     expect = lam * L / (L + 2 * 0.7104 * lam)
     assert abs(semfp - expect) < 3 * sigma + 0.01 * expect, (semfp, expect, sigma)
+
+
+def test_headline_thin_film_matches_the_oracle(orc):
+    """The bench workload's structure and full spectrum (thin film 300 x 300 x
+    145 nm, 3 void holes r = 50 nm, y periodic, diffuse walls; 2000 modes with
+    MFPs from 1 nm to 10 um, 64 frequency bins) at 20 particles per (mode,
+    angle): the FP32 kernel's kappa within 3 combined standard errors of the
+    FP64 oracle's (independent seeds) and every populated bin's transmission
+    within 4."""
+    model = synth.film_with_holes(lx=300.0, ly=300.0, lz=145.0, nholes=3, radius=50.0, seed=0,
+                                  periodic_y=True, p_hole=0.0, t_hole=0.0, p_z=0.0)
+    spec = synth.spectrum(2000, seed=0)
+    bins = dict(temperature=300.0, nbins=64, bin_omega=(0.0, 15.0 * 2 * math.pi * 1e12))
+    run64 = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=11, np_=20, seed=777, **bins)
+    run32 = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=11, np_=20, seed=12345, precision=A.PREC_FP32,
+                       **bins)
+    o = orc.Oracle(model=model, spectrum=spec)
+    cnt_o, _, _ = o.counts(run64)
+    ko = o.kappa(run64, cnt_o)
+    gb = A.GeomBuf(model)
+    with A.Handle(gb.view, spec) as h:
+        kg = h.kappa(run32)
+        st = h.stats()
+    assert st["lost"] <= 1e-5 * st["samples"]
+    se = math.hypot(kg["kappa_stderr"], ko["kappa_stderr"])
+    z = (kg["kappa"] - ko["kappa"]) / se
+    assert abs(z) < 3.0, (kg["kappa"], ko["kappa"], se)
+    seb = np.hypot(kg["bin_T_stderr"], ko["bin_T_stderr"])
+    live = seb > 0
+    assert live.sum() >= 60
+    zb = (kg["bin_T"][live] - ko["bin_T"][live]) / seb[live]
+    assert np.max(np.abs(zb)) < 4.0, np.max(np.abs(zb))

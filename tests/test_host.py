@@ -145,10 +145,12 @@ def test_anphon_round_trip(tmp_path):
     assert b.nbranch == 1 and b.rtemp == s.rtemp and b.vol == s.vol
 
 
-REF_EXAMPLES = "/root/reference/Examples"
+# the reference's Examples/ folder, where a checkout of it is at hand
+REF_EXAMPLES = os.environ.get("PTRANS_REFERENCE_EXAMPLES", "")
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_EXAMPLES), reason="reference examples not mounted")
+@pytest.mark.skipif(not REF_EXAMPLES or not os.path.isdir(REF_EXAMPLES),
+                    reason="PTRANS_REFERENCE_EXAMPLES does not name the reference's Examples folder")
 def test_reference_examples_parse():
     """Counts from the shipped .mcp inputs (tests/golden/examples_summary.json
     holds the same figures for machines without the reference)."""

@@ -73,3 +73,28 @@ def test_two_gloo_ranks_reproduce_the_single_rank_run(tmp_path):
     ref = o.kappa(run, single)
     k = np.load(tmp_path / "kappa.npy")
     assert abs(k[0] - ref["kappa"]) <= 1e-12 * abs(ref["kappa"])
+
+
+def test_bench_launcher_starts_the_ranks(tmp_path):
+    """bench.py --gpus N, when no launcher set WORLD_SIZE, starts N ranks
+    itself with the environment torchrun would give them; here the ranks are
+    a gloo probe: they join one process group of N and all-reduce."""
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    import bench
+    out = tmp_path / "probe.json"
+    probe = os.path.join(root, "tests", "rank_probe.py")
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    old = dict(os.environ)
+    try:
+        os.environ.clear()
+        os.environ.update(env)
+        rc = bench.spawn_ranks(3, probe, [str(out)], timeout_s=120)
+    finally:
+        os.environ.clear()
+        os.environ.update(old)
+    assert rc == 0
+    import json
+    got = json.load(open(out))
+    assert got == {"world": 3, "sum": 6, "local_rank": 0, "master": "127.0.0.1"}

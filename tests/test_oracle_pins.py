@@ -108,3 +108,47 @@ def test_lost_phonons_counted_with_quirk(orc):
     c1, l1, r1 = o.counts(run, max_flights=1, ref_quirks=1)
     assert r0["capped"] > 0 and r0["lost"] == r0["capped"]
     np.testing.assert_array_equal(c1, c0 + l0)
+
+
+def _film_model(L, d, width=40.0):
+    """A film of thickness d (diffuse z walls) along x, infinite in-plane:
+    specular y walls, which mirror a film without inclusions exactly."""
+    m = synth.nanowire(length=L, width=width, height=d, p_side=0.0)
+    m.cellspec = (1.0, 1.0, 1.0, 1.0, 0.0, 0.0)
+    return m
+
+
+def _oracle_flux_T(orc, model, lam, np_, nangle=11, seed=5):
+    import limits
+    spec = synth.spectrum(1, seed=0)
+    o = orc.Oracle(model=model, spectrum=spec)
+    run = A.make_run(kind_mfp=A.MFP_GRID, nangle=nangle, np_=np_, seed=seed, mfp_grid=[lam])
+    cnt, lost, _ = o.counts(run)
+    assert lost.sum() == 0
+    return limits.flux_transmission(cnt[: nangle - 1] / np_, np_, nangle)
+
+
+@pytest.mark.parametrize("kn", [0.5, 2.0])
+def test_fuchs_sondheimer_film_limit(orc, kn):
+    """In-plane MFP of a fully diffuse film (thickness d = 40 nm, gray MFP
+    Kn * d) from the two-length estimate at L = 10 and 20 max(Lambda, d)
+    against the Fuchs-Sondheimer integral, within 3 standard errors plus 1%
+    for what is left of the contact term at these lengths and the Simpson
+    bias at Nangle = 11 (5.5e-5)."""
+    import limits
+    d = 40.0
+    lam = kn * d
+    L1, L2 = 10 * max(lam, d), 20 * max(lam, d)
+    T1, v1 = _oracle_flux_T(orc, _film_model(L1, d), lam, 30000)
+    T2, v2 = _oracle_flux_T(orc, _film_model(L2, d), lam, 30000)
+    est, se = limits.two_length_mfp(L1, T1, v1, L2, T2, v2)
+    want = lam * limits.fuchs_sondheimer(kn)
+    assert abs(est - want) < 3 * se + 0.01 * want, (est, want, se)
+
+
+def test_casimir_closed_form_equals_its_integral():
+    """The closed form of the square wire's Casimir MFP equals the defining
+    integral 3/(8A) int dA int dphi s(r, phi) evaluated by quadrature."""
+    import limits
+    assert abs(limits.casimir_square(1.0) - limits.casimir_numeric(1.0, 1.0, 400)) < 2e-5
+    assert abs(limits.casimir_square(1.0) - 1.114954) < 1e-6
