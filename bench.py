@@ -362,6 +362,12 @@ def run_structure(args):
         model = synth.voronoi_box(5, box=(1000.0, 1000.0, 1000.0), seed=0, trans=0.5, spec=0.0, p_wall=0.0)
         desc = "5 Voronoi grains in a 1000^3 nm box, internal facets T=0.5 p=0, diffuse walls"
         np_default, np64 = 500, 5
+    elif args.workload == "c4":
+        model = synth.voronoi_box(5, box=(1000.0, 1000.0, 1000.0), seed=0, trans=0.5, spec=0.0, p_wall=0.0,
+                                  tri_levels=4)
+        desc = ("5 Voronoi grains in a 1000^3 nm box as a triangle mesh (43008 FP32 triangles, a BVH per "
+                "grain), grain boundaries T=0.5 p=0, diffuse walls")
+        np_default, np64 = 500, 1
     else:
         model = synth.cube_lattice(n=16, l=1000.0, fill=0.5, trans=0.0, spec=0.0, p_wall=0.0)
         desc = ("16^3 cubic voids (side 31.25 nm, pitch 62.5 nm) in a 1000^3 nm box, "
@@ -401,8 +407,8 @@ def run_structure(args):
                                  "full_flight_fraction": st["full_flights"] / max(st["flights"], 1)},
             "tail": {"max_trajectory_flights": st["max_traj_flights"], "queue_drain_ms": st["drain_ms"],
                      "tail_ms": st["tail_ms"]}}
-    if args.workload == "mesh":
-        # the linear-scan comparators test 49152 triangles per flight, one
+    if args.workload in ("mesh", "c4"):
+        # the linear-scan comparators test every triangle of a grain per flight, one
         # trajectory per thread: a bounded sample of the 100 modes with the
         # longest MFP (short trajectories), one particle per (mode, angle) task,
         # timed for the BVH kernel too
@@ -497,9 +503,11 @@ def main():
     ap.add_argument("--mfp-lo", type=float, default=1e-9,
                     help="smallest bulk MFP of the spectrum [m]; 1e-9 is the metric's spectrum "
                          "(larger values remove the diffusive tail, for throughput diagnostics)")
-    ap.add_argument("--workload", default="thinfilm", choices=["thinfilm", "c3", "c5", "voronoi", "mesh"],
+    ap.add_argument("--workload", default="thinfilm", choices=["thinfilm", "c3", "c4", "c5", "voronoi", "mesh"],
                     help="thinfilm: the metric's configuration; c3: spheres + capped cylinders with "
-                         "the adjoint; c5: 256-film batched screening; voronoi / mesh: the C4 structures")
+                         "the adjoint; c5: 256-film batched screening; c4: the Voronoi polycrystal as a "
+                         "43k-triangle mesh with T=0.5 boundaries; voronoi / mesh: its polygon form and a "
+                         "16^3 cube lattice of voids")
     ap.add_argument("--fp64-subset", type=int, default=16,
                     help="c5: films timed one by one with the plain FP64 kernel")
     ap.add_argument("--cpu-leg", action="store_true", help=argparse.SUPPRESS)
@@ -512,7 +520,7 @@ def main():
         return run_reference(args)
     if args.workload == "c5":
         return run_c5(args)
-    if args.workload in ("voronoi", "mesh"):
+    if args.workload in ("voronoi", "mesh", "c4"):
         return run_structure(args)
     if args.workload == "c3":
         return run_c3(args)

@@ -459,6 +459,22 @@ typedef struct ptg_batch_adjoint_out {
 int ptg_batch_adjoint(ptg_batch* b, ptg_batch_adjoint_out* out);
 void ptg_batch_destroy(ptg_batch* b);
 
+/*
+ * Bounds-checked build (no counterpart in the reference, whose debug aids
+ * are its verbose self-checks, src/RTMCphon.f90:1695-1703, 1711-1731):
+ * libptrans_b200_check.so, the same library built with -DPT_CHECK, checks
+ * every geometry-blob index the FP32 kernels read (surfaces, edges,
+ * candidates, BVH nodes) and that every live phonon's state is finite; a
+ * failed check is counted, its access redirected to a valid element, and
+ * the kernel goes on (it never traps).  ptg_check_report returns, for a
+ * device, the number of failed checks since the last reset, the code of the
+ * first (1 index out of range, 2 non-finite state) and its index (the blob
+ * unit, or the task); reset != 0 clears them.  Regular builds return
+ * PTG_ERR_UNSUPPORTED.
+ */
+int ptg_check_report(int32_t device, int64_t* violations, int32_t* first_code, int32_t* first_index,
+                     int32_t reset);
+
 /* Statistics of the last transport call on h. */
 int ptg_last_stats(const ptg_handle* h, ptg_stats* st);
 

@@ -19,7 +19,10 @@ from typing import Optional
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libptrans_b200.so")
+# PTRANS_B200_LIB selects another build of the library, e.g. the
+# bounds-checked libptrans_b200_check.so
+LIB_PATH = os.environ.get("PTRANS_B200_LIB") or os.path.join(HERE, "libptrans_b200.so")
+CHECK_LIB_PATH = os.path.join(HERE, "libptrans_b200_check.so")
 
 # ---- constants (include/ptrans_gpu.h) --------------------------------------
 PTG_OK = 0
@@ -190,6 +193,8 @@ SIGNATURES = {
     "ptg_kappa_from_counts": (C.c_int, [C.POINTER(PtgGeometry), C.POINTER(PtgSpectrum),
                                         C.POINTER(PtgRun), U64P, C.POINTER(PtgKappaOut)]),
     "ptg_last_stats": (C.c_int, [C.c_void_p, C.POINTER(PtgStats)]),
+    "ptg_check_report": (C.c_int, [C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int32),
+                                   C.POINTER(C.c_int32), C.c_int32]),
     "ptg_write_outputs": (C.c_int, [C.c_char_p, C.POINTER(PtgGeometry), C.POINTER(PtgSpectrum),
                                     C.POINTER(PtgRun), U64P]),
     "ptg_gamma_from_tbc": (C.c_int, [C.POINTER(PtgSpectrum), C.c_double, C.c_double, F64P]),
@@ -716,6 +721,16 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def check_report(device: int = 0, reset: bool = False) -> dict:
+    """ptg_check_report of a bounds-checked build (PTRANS_B200_LIB pointing at
+    libptrans_b200_check.so): failed checks since the last reset."""
+    lib = load_library()
+    n, code, idx = C.c_int64(), C.c_int32(), C.c_int32()
+    _check(lib.ptg_check_report(device, C.byref(n), C.byref(code), C.byref(idx), 1 if reset else 0),
+           "ptg_check_report")
+    return {"violations": n.value, "first_code": code.value, "first_index": idx.value}
 
 
 def kappa_from_counts(geometry: PtgGeometry, spectrum: Spectrum, run: PtgRun, counts: np.ndarray) -> dict:

@@ -431,6 +431,10 @@ struct Transport {
 };
 
 int run_transport(ptg_handle* h, const Transport& T) {
+  ptg::NvtxRange nvtx(T.mode == ptg::MODE_LIST      ? "ptg transport: list"
+                      : T.mode == ptg::MODE_ADJOINT ? "ptg transport: adjoint replay"
+                      : T.mode == ptg::MODE_TRACE   ? "ptg transport: trace replay"
+                                                    : "ptg transport");
   const int64_t ntask = T.ntask;
   CU(cudaSetDevice(h->device));
   CU(h->counts.ensure(sizeof(unsigned long long) * ntask));
@@ -912,6 +916,7 @@ void ptg_destroy(ptg_handle* h) {
 int ptg_transmission(ptg_handle* h, double mfp_nm, int32_t nangle, int64_t np, int32_t rank,
                      int32_t nranks, uint64_t seed, int32_t precision, double* transmit,
                      double* stderr_opt) {
+  ptg::NvtxRange nvtx("ptg_transmission");
   if (!h || !transmit) return PTG_ERR_INVALID;
   if (nangle < 2 || np < 1 || nranks < 1 || rank < 0 || rank >= nranks) return PTG_ERR_INVALID;
   if (precision != PTG_PREC_FP32 && precision != PTG_PREC_FP64) return PTG_ERR_INVALID;
@@ -953,6 +958,7 @@ int ptg_transmission(ptg_handle* h, double mfp_nm, int32_t nangle, int64_t np, i
 }
 
 int ptg_kappa(ptg_handle* h, const ptg_run* run, ptg_kappa_out* out) {
+  ptg::NvtxRange nvtx("ptg_kappa");
   if (!h || !run || !out) return PTG_ERR_INVALID;
   std::string why;
   if (!ptg::run_valid(h->spec, run, &why)) { h->last_error = why; return PTG_ERR_INVALID; }
@@ -1029,9 +1035,12 @@ int ptg_kappa(ptg_handle* h, const ptg_run* run, ptg_kappa_out* out) {
   in.emfp_nm = h->red_emfp.as<double>();
   in.transmit = h->red_trans.as<double>();
   in.result = h->red_result.as<double>();
-  CU(cudaEventRecord(h->ev[2], s));
-  CU(ptg::launch_kappa_reduce(in, s));
-  CU(cudaEventRecord(h->ev[3], s));
+  {
+    ptg::NvtxRange nvtx("ptg kappa reduction");
+    CU(cudaEventRecord(h->ev[2], s));
+    CU(ptg::launch_kappa_reduce(in, s));
+    CU(cudaEventRecord(h->ev[3], s));
+  }
   std::vector<double> res(2 + 3 * (size_t)nbins);
   CU(cudaMemcpyAsync(res.data(), h->red_result.p, sizeof(double) * res.size(), cudaMemcpyDeviceToHost, s));
   if (out->emfp_nm)
@@ -1077,6 +1086,7 @@ int ptg_kappa_from_counts(const ptg_geometry* geom, const ptg_spectrum* spec, co
 
 int ptg_trace(ptg_handle* h, const ptg_run* run, int64_t n, const uint64_t* samples,
               int64_t cap_positions, float* pos, int64_t* npos, int32_t* end_side) {
+  ptg::NvtxRange nvtx("ptg_trace");
   if (!h || !run || n < 1 || !samples || !npos || !end_side) return PTG_ERR_INVALID;
   std::string why;
   if (!ptg::run_valid(h->spec, run, &why)) { h->last_error = why; return PTG_ERR_INVALID; }
@@ -1177,6 +1187,7 @@ int ptg_write_trace(ptg_handle* h, const ptg_run* run, int32_t particle_trace, c
 }
 
 int ptg_adjoint(ptg_handle* h, const ptg_run* run, ptg_adjoint_out* out) {
+  ptg::NvtxRange nvtx("ptg_adjoint");
   if (!h || !run || !out) return PTG_ERR_INVALID;
   std::string why;
   if (!ptg::run_valid(h->spec, run, &why)) { h->last_error = why; return PTG_ERR_INVALID; }
@@ -1277,6 +1288,21 @@ int ptg_adjoint(ptg_handle* h, const ptg_run* run, ptg_adjoint_out* out) {
   out->replayed = nlist;
   out->mismatched = h->mismatch;
   out->kernel_ms = fwd_ms + h->last.kernel_ms;
+  return PTG_OK;
+}
+
+int ptg_check_report(int32_t device, int64_t* violations, int32_t* first_code, int32_t* first_index,
+                     int32_t reset) {
+  if (!violations || !first_code || !first_index) return PTG_ERR_INVALID;
+  long long n = 0;
+  int code = 0, index = 0;
+  if (cudaSetDevice(device) != cudaSuccess) { cudaGetLastError(); return PTG_ERR_NO_DEVICE; }
+  const cudaError_t e = ptg::check_report(&n, &code, &index, reset != 0);
+  if (e == cudaErrorNotSupported) return PTG_ERR_UNSUPPORTED;
+  if (e != cudaSuccess) { cudaGetLastError(); return PTG_ERR_CUDA; }
+  *violations = n;
+  *first_code = code;
+  *first_index = index;
   return PTG_OK;
 }
 

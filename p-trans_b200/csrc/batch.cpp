@@ -339,6 +339,7 @@ extern "C" int ptg_batch_create(const ptg_batch_item* items, int32_t nitems,
 }
 
 extern "C" int ptg_batch_run(ptg_batch* b, ptg_batch_out* out) {
+  ptg::NvtxRange nvtx("ptg_batch_run");
   if (!b || !out) return PTG_ERR_INVALID;
   if (cudaSetDevice(b->device) != cudaSuccess) return PTG_ERR_CUDA;
   if (cudaEventRecord(b->ev0, b->stream) != cudaSuccess ||
@@ -401,6 +402,7 @@ static int batch_launch(ptg_batch* b, const ptg::RunF32& r, int mode, unsigned l
 }
 
 extern "C" int ptg_batch_adjoint(ptg_batch* b, ptg_batch_adjoint_out* out) {
+  ptg::NvtxRange nvtx("ptg_batch_adjoint");
   if (!b || !out) return PTG_ERR_INVALID;
   if (cudaSetDevice(b->device) != cudaSuccess) return PTG_ERR_CUDA;
   const int64_t ntg = b->ntask_per_geo;

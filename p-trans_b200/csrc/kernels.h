@@ -207,6 +207,9 @@ cudaError_t launch_persistent_batch(const RunF32& r, int grid, int block, cudaSt
                                     bool bvh, int mode = MODE_FORWARD);
 cudaError_t persistent_batch_occupancy(int block, int* blocks_per_sm, bool bvh,
                                        int mode = MODE_FORWARD);
+/* Violations recorded by the bounds-checked build (PT_CHECK); other builds
+   return cudaErrorNotSupported. */
+cudaError_t check_report(long long* count, int* code, int* index, bool reset);
 /* Residency of the persistent kernel for a block size and shared memory. */
 cudaError_t persistent_occupancy(int block, size_t smem, int* blocks_per_sm,
                                  int mode = MODE_FORWARD, bool bvh = false);

@@ -70,6 +70,19 @@ constexpr float kPi = 3.14159265358979323846f;
 
 extern __shared__ float4 sblob[];
 
+#ifdef PT_CHECK
+/* Bounds-checked build: [0] violations, [1] code of the first, [2] its
+   index.  A failed check is recorded and the access is redirected to a
+   valid element; the kernel never traps. */
+__device__ int g_check[3];
+__device__ __noinline__ void check_fail(int code, int index) {
+  if (atomicAdd(&g_check[0], 1) == 0) {
+    g_check[1] = code;
+    g_check[2] = index;
+  }
+}
+#endif
+
 /* Geometry blob accessor: SMEM = true reads the copy staged in shared
    memory (shared-memory loads), false reads global memory through the
    read-only path. */
@@ -78,10 +91,16 @@ struct Geo {
   const float4* base;   /* global blob (SMEM = false) */
   BlobLayout lay;
   __device__ __forceinline__ float4 ld(int i) const {
+#ifdef PT_CHECK
+    if ((unsigned)i >= (unsigned)lay.total) { check_fail(1, i); i = 0; }
+#endif
     if (SMEM) return sblob[i];
     return __ldg(base + i);
   }
   __device__ __forceinline__ int ldi(int unit, int k) const {
+#ifdef PT_CHECK
+    if (k < 0 || (unsigned)(unit + k / 4) >= (unsigned)lay.total) { check_fail(1, unit + k / 4); unit = 0; k = 0; }
+#endif
     if (SMEM) return reinterpret_cast<const int*>(sblob + unit)[k];
     return __ldg(reinterpret_cast<const int*>(base + unit) + k);
   }
@@ -119,7 +138,18 @@ __device__ __forceinline__ void sincos2pi(float u, float* s, float* c) {
 struct GeoBatch {
   const float4* base;
   BlobLayout lay;
-  __device__ __forceinline__ float4 ld(int i) const { return __ldg(base + i); }
+  __device__ __forceinline__ float4 ld(int i) const {
+#ifdef PT_CHECK
+    if ((unsigned)i >= (unsigned)lay.total) { check_fail(1, i); i = 0; }
+#endif
+    return __ldg(base + i);
+  }
+  __device__ __forceinline__ int ldi(int unit, int k) const {
+#ifdef PT_CHECK
+    if (k < 0 || (unsigned)(unit + k / 4) >= (unsigned)lay.total) { check_fail(1, unit + k / 4); unit = 0; k = 0; }
+#endif
+    return __ldg(reinterpret_cast<const int*>(base + unit) + k);
+  }
   __device__ __forceinline__ float4 hotA(int s) const { return ld(lay.hot + 2 * s); }
   __device__ __forceinline__ int4 hotB(int s) const {
     const float4 v = ld(lay.hot + 2 * s + 1);
@@ -128,16 +158,10 @@ struct GeoBatch {
   }
   __device__ __forceinline__ float4 cold(int s, int i) const { return ld(lay.cold + 3 * s + i); }
   __device__ __forceinline__ float4 edge(int e) const { return ld(lay.edge + e); }
-  __device__ __forceinline__ int cand_begin(int g) const {
-    return __ldg(reinterpret_cast<const int*>(base + lay.cand_begin) + g);
-  }
-  __device__ __forceinline__ int cand(int k) const {
-    return __ldg(reinterpret_cast<const int*>(base + lay.cand) + k);
-  }
+  __device__ __forceinline__ int cand_begin(int g) const { return ldi(lay.cand_begin, g); }
+  __device__ __forceinline__ int cand(int k) const { return ldi(lay.cand, k); }
   __device__ __forceinline__ float4 start(int i) const { return ld(lay.start + i); }
-  __device__ __forceinline__ int bvh_root(int g) const {
-    return __ldg(reinterpret_cast<const int*>(base + lay.bvh_root) + g);
-  }
+  __device__ __forceinline__ int bvh_root(int g) const { return ldi(lay.bvh_root, g); }
   __device__ __forceinline__ float4 node(int i) const { return ld(lay.bvh_node + i); }
 };
 
@@ -1400,6 +1424,11 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
         }
       }
     }
+#ifdef PT_CHECK
+    if (alive && !(isfinite(px) && isfinite(py) && isfinite(pz) && isfinite(dx) && isfinite(dy) &&
+                   isfinite(dz) && !isnan(fp)))
+      check_fail(2, task);
+#endif
     /* ---- tallies ------------------------------------------------------- */
     const bool fin = alive && end_side >= 0;
     const bool trans = fin && (end_side == 2 || (end_side == 0 && r.ref_quirks));
@@ -1613,6 +1642,29 @@ cudaError_t launch_tail_fp32(const GeoF32& g, const RunF32& r, int grid, int blo
   if (block > kBlock || block % 32) return cudaErrorInvalidConfiguration;
   return g.has_ext ? launch_bvh<true, PH_TAIL>(g, r, grid, block, smem, st, mode)
                    : launch_bvh<false, PH_TAIL>(g, r, grid, block, smem, st, mode);
+}
+
+/* Violations recorded by a bounds-checked build (PT_CHECK): count, code of
+   the first (1 geometry-blob index out of range, 2 non-finite phonon state)
+   and its index; reset = true clears them.  Other builds return
+   cudaErrorNotSupported. */
+cudaError_t check_report(long long* count, int* code, int* index, bool reset) {
+#ifdef PT_CHECK
+  int v[3] = {0, 0, 0};
+  cudaError_t e = cudaMemcpyFromSymbol(v, g_check, sizeof(v));
+  if (e != cudaSuccess) return e;
+  *count = v[0];
+  *code = v[1];
+  *index = v[2];
+  if (reset) {
+    const int z[3] = {0, 0, 0};
+    e = cudaMemcpyToSymbol(g_check, z, sizeof(z));
+  }
+  return e;
+#else
+  (void)count; (void)code; (void)index; (void)reset;
+  return cudaErrorNotSupported;
+#endif
 }
 
 }  // namespace ptg

@@ -11,7 +11,21 @@
 
 #include "../../include/ptrans_gpu.h"
 
+#include <nvtx3/nvToolsExt.h>
+
 namespace ptg {
+
+/* An NVTX range over a scope: the host-side phases of each entry point
+   (transport launches, reductions, adjoint passes) show by name in Nsight
+   Systems and in ncu --nvtx filters; without a tool attached it costs a
+   call that returns at once. */
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
 
 /* Owning, structure-of-arrays copy of a built geometry (ptg_geometry). */
 struct GeomSoA {

@@ -341,14 +341,34 @@ def _clip_cell(faces, labels, nrm, c, label, tol):
     return out_f, out_l
 
 
+def _triangulate(poly, levels):
+    """A convex polygon (vertex loop) as triangles: a fan about the vertex
+    mean, each fan triangle split `levels` times into four by its edge
+    midpoints, every triangle keeping the polygon's orientation.  The two
+    cells sharing a facet hold its vertex loop in opposite orders, and both
+    get the same triangles (reversed)."""
+    c = np.mean(poly, axis=0)
+    tris = [(c, poly[i], poly[(i + 1) % len(poly)]) for i in range(len(poly))]
+    for _ in range(levels):
+        nxt = []
+        for a, b, d in tris:
+            ab, bd, da = 0.5 * (a + b), 0.5 * (b + d), 0.5 * (d + a)
+            nxt += [(a, ab, da), (ab, b, bd), (da, bd, d), (ab, bd, da)]
+        tris = nxt
+    return [list(t) for t in tris]
+
+
 def voronoi_box(n_grains: int = 5, box=(1000.0, 1000.0, 1000.0), seed: int = 0, trans: float = 0.5,
-                spec: float = 0.0, p_wall: float = 0.0, generators=None) -> Model:
+                spec: float = 0.0, p_wall: float = 0.0, generators=None, tri_levels: int = -1) -> Model:
     """Voronoi polycrystal in the box: seeded generators (uniform in the inner
     90% of the box), every cell the box clipped by the bisector planes of the
     other generators.  Facets on the box are Boundary facets (grain_to 0, the
     box's CellSpecularity applies), facets between cells carry material 1 and
     the neighbour's grain id, with the (1,1) transmission-table entry
-    (T = trans, p = spec) as in Examples/04_voronoi_5grain.mcp."""
+    (T = trans, p = spec) as in Examples/04_voronoi_5grain.mcp.  With
+    tri_levels >= 0 every facet is given as a triangle mesh instead (a fan
+    refined tri_levels times, 4^levels triangles per fan triangle), as a
+    grain exported from a mesher or an STL file would be."""
     L = np.asarray(box, np.float64)
     rng = np.random.default_rng(seed)
     gens = (np.asarray(generators, np.float64) if generators is not None
@@ -377,11 +397,13 @@ def voronoi_box(n_grains: int = 5, box=(1000.0, 1000.0, 1000.0), seed: int = 0, 
                     elif abs(v[d] - L[d]) <= tol:
                         v[d] = L[d]
                 fv.append(v)
-            nv.append(len(fv))
-            verts.extend(fv)
-            mto.append(MATERIAL_BOUNDARY if lab < 0 else 1)
-            gto.append(0 if lab < 0 else lab + 1)
-            kept += 1
+            pieces = [fv] if tri_levels < 0 else _triangulate(fv, tri_levels)
+            for pc in pieces:
+                nv.append(len(pc))
+                verts.extend(pc)
+                mto.append(MATERIAL_BOUNDARY if lab < 0 else 1)
+                gto.append(0 if lab < 0 else lab + 1)
+                kept += 1
         nfacet.append(kept)
     kind, tt, ts = _table(trans, spec)
     return Model(

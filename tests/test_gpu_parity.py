@@ -369,3 +369,30 @@ def test_headline_thin_film_matches_the_oracle(orc):
     assert live.sum() >= 60
     zb = (kg["bin_T"][live] - ko["bin_T"][live]) / seb[live]
     assert np.max(np.abs(zb)) < 4.0, np.max(np.abs(zb))
+
+
+def test_triangulated_polycrystal_matches_its_polygon_form(orc):
+    """A Voronoi polycrystal (grain boundaries T = 0.5, p = 0, diffuse walls)
+    given as polygons and as a triangle mesh of the same facets (4^2 triangles
+    per fan triangle, a BVH in every grain) is the same structure: the FP32
+    kappa of the mesh form agrees with the oracle's polygon run within 4
+    combined standard errors, and every per-task |z| < 5."""
+    kw = dict(box=(300.0, 250.0, 250.0), seed=5, trans=0.5, spec=0.0, p_wall=0.0)
+    poly = synth.voronoi_box(5, **kw)
+    mesh = synth.voronoi_box(5, tri_levels=2, **kw)
+    spec = synth.spectrum(12, seed=9, mfp_lo=10e-9, mfp_hi=2e-6)
+    np_ = 1500
+    run64 = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=7, np_=np_, seed=3)
+    run32 = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=7, np_=np_, seed=4, precision=A.PREC_FP32)
+    o = orc.Oracle(model=poly, spectrum=spec)
+    cnt_o, _, _ = o.counts(run64)
+    ko = o.kappa(run64, cnt_o)
+    gb = A.GeomBuf(mesh)
+    with A.Handle(gb.view, spec) as h:
+        kg = h.kappa(run32, want_counts=True)
+        st = h.stats()
+    assert st["box_tests"] > 0  # the grains' BVHs were walked
+    z = _z(kg["counts"].astype(float), cnt_o.astype(float), np_)
+    assert np.max(np.abs(z)) < 5.0
+    se = np.hypot(kg["kappa_stderr"], ko["kappa_stderr"])
+    assert abs(kg["kappa"] - ko["kappa"]) < 4 * se, (kg["kappa"], ko["kappa"], se)

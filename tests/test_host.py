@@ -53,6 +53,10 @@ def models():
         "capped": synth.spheres_cylinders_box(n_spheres=5, n_cylinders=6, l=400.0, seed=2,
                                               r_sphere=(15.0, 40.0), r_cylinder=20.0, length=(60.0, 200.0),
                                               trans=0.3),
+        "voronoi_mesh": synth.voronoi_box(4, box=(300.0, 200.0, 250.0), seed=3, trans=0.5, spec=0.2,
+                                          tri_levels=1),
+        "gamma_2mat": synth.with_interface(synth.brick_box(t=0.5, p=0.25), A.TRANS_GAMMA, 1.2, spec=0.3,
+                                           two_materials=True),
     }
 
 
