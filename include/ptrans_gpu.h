@@ -475,6 +475,15 @@ void ptg_batch_destroy(ptg_batch* b);
 int ptg_check_report(int32_t device, int64_t* violations, int32_t* first_code, int32_t* first_index,
                      int32_t reset);
 
+/*
+ * Test hook (no counterpart in the reference): the next `after` allocations
+ * the library makes succeed and every later one fails - device buffers are
+ * not requested from CUDA and host objects are not created - so that every
+ * entry point's out-of-memory path can be exercised; the calls return
+ * PTG_ERR_NOMEM and leave their handles usable.  after < 0 turns it off.
+ */
+int ptg_debug_fail_allocations(int64_t after);
+
 /* Statistics of the last transport call on h. */
 int ptg_last_stats(const ptg_handle* h, ptg_stats* st);
 

@@ -195,6 +195,7 @@ SIGNATURES = {
     "ptg_last_stats": (C.c_int, [C.c_void_p, C.POINTER(PtgStats)]),
     "ptg_check_report": (C.c_int, [C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int32),
                                    C.POINTER(C.c_int32), C.c_int32]),
+    "ptg_debug_fail_allocations": (C.c_int, [C.c_int64]),
     "ptg_write_outputs": (C.c_int, [C.c_char_p, C.POINTER(PtgGeometry), C.POINTER(PtgSpectrum),
                                     C.POINTER(PtgRun), U64P]),
     "ptg_gamma_from_tbc": (C.c_int, [C.POINTER(PtgSpectrum), C.c_double, C.c_double, F64P]),
@@ -721,6 +722,21 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+class fail_allocations:
+    """Context manager of ptg_debug_fail_allocations: inside it the library's
+    allocations after the first `after` fail (a test hook)."""
+
+    def __init__(self, after: int):
+        self.after = after
+
+    def __enter__(self):
+        load_library().ptg_debug_fail_allocations(self.after)
+        return self
+
+    def __exit__(self, *a):
+        load_library().ptg_debug_fail_allocations(-1)
 
 
 def check_report(device: int = 0, reset: bool = False) -> dict:

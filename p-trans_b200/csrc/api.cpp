@@ -31,6 +31,7 @@ struct DevBuf {
     p = nullptr;
     cap = 0;
     size_t want = bytes < 256 ? 256 : bytes;
+    if (ptg::alloc_should_fail()) return cudaErrorMemoryAllocation;
     cudaError_t e = cudaMalloc(&p, want);
     if (e == cudaSuccess) cap = want;
     return e;
@@ -44,13 +45,13 @@ struct DevBuf {
   T* as() const { return static_cast<T*>(p); }
 };
 
-#define CU(x)                                  \
-  do {                                         \
-    cudaError_t e_ = (x);                      \
-    if (e_ != cudaSuccess) {                   \
-      h->last_error = cudaGetErrorString(e_);  \
-      return PTG_ERR_CUDA;                     \
-    }                                          \
+#define CU(x)                                                                \
+  do {                                                                       \
+    cudaError_t e_ = (x);                                                    \
+    if (e_ != cudaSuccess) {                                                 \
+      h->last_error = cudaGetErrorString(e_);                                \
+      return e_ == cudaErrorMemoryAllocation ? PTG_ERR_NOMEM : PTG_ERR_CUDA; \
+    }                                                                        \
   } while (0)
 
 }  // namespace
@@ -823,45 +824,56 @@ const char* ptg_strerror(int status) {
 
 int ptg_create(const ptg_geometry* geom, const ptg_spectrum* spec, const ptg_options* opt,
                ptg_handle** out) {
-  if (!out) return PTG_ERR_INVALID;
-  *out = nullptr;
-  ptg_handle* h = new (std::nothrow) ptg_handle();
-  if (!h) return PTG_ERR_NOMEM;
-  memset(&h->opt, 0, sizeof(h->opt));
-  if (opt) h->opt = *opt;
-  memset(&h->last, 0, sizeof(h->last));
-  if (h->opt.reserved != 0) { delete h; return PTG_ERR_INVALID; }
-  std::string why;
-  int st = ptg::copy_geometry(geom, &h->geom, &why);
-  if (st == PTG_OK) st = ptg::copy_spectrum(spec, &h->spec, &why);
-  if (st != PTG_OK) { delete h; return st; }
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0 || h->opt.device < 0 ||
-      h->opt.device >= ndev) {
-    cudaGetLastError();
+  ptg_handle* h = nullptr;
+  try {
+    if (!out) return PTG_ERR_INVALID;
+    *out = nullptr;
+    h = ptg::alloc_should_fail() ? nullptr : new (std::nothrow) ptg_handle();
+    if (!h) return PTG_ERR_NOMEM;
+    memset(&h->opt, 0, sizeof(h->opt));
+    if (opt) h->opt = *opt;
+    memset(&h->last, 0, sizeof(h->last));
+    if (h->opt.reserved != 0) { delete h; return PTG_ERR_INVALID; }
+    std::string why;
+    int st = ptg::copy_geometry(geom, &h->geom, &why);
+    if (st == PTG_OK) st = ptg::copy_spectrum(spec, &h->spec, &why);
+    if (st != PTG_OK) { delete h; return st; }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0 || h->opt.device < 0 ||
+        h->opt.device >= ndev) {
+      cudaGetLastError();
+      delete h;
+      return PTG_ERR_NO_DEVICE;
+    }
+    h->device = h->opt.device;
+    cudaDeviceProp prop;
+    if (cudaSetDevice(h->device) != cudaSuccess ||
+        cudaGetDeviceProperties(&prop, h->device) != cudaSuccess || prop.major != 10) {
+      cudaGetLastError();
+      delete h;
+      return PTG_ERR_NO_DEVICE;
+    }
+    h->num_sms = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete h;
+      return PTG_ERR_CUDA;
+    }
+    for (auto& e : h->ev)
+      if (cudaEventCreate(&e) != cudaSuccess) { delete h; return PTG_ERR_CUDA; }
+    st = build_geo64(h);
+    if (st == PTG_OK) st = build_blob(h);
+    if (st != PTG_OK) { delete h; return st; }
+    *out = h;
+    return PTG_OK;
+  } catch (const std::bad_alloc&) {
     delete h;
-    return PTG_ERR_NO_DEVICE;
-  }
-  h->device = h->opt.device;
-  cudaDeviceProp prop;
-  if (cudaSetDevice(h->device) != cudaSuccess ||
-      cudaGetDeviceProperties(&prop, h->device) != cudaSuccess || prop.major != 10) {
-    cudaGetLastError();
+    if (out) *out = nullptr;
+    return PTG_ERR_NOMEM;
+  } catch (...) {
     delete h;
-    return PTG_ERR_NO_DEVICE;
+    if (out) *out = nullptr;
+    return PTG_ERR_INVALID;
   }
-  h->num_sms = prop.multiProcessorCount;
-  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
-    delete h;
-    return PTG_ERR_CUDA;
-  }
-  for (auto& e : h->ev)
-    if (cudaEventCreate(&e) != cudaSuccess) { delete h; return PTG_ERR_CUDA; }
-  st = build_geo64(h);
-  if (st == PTG_OK) st = build_blob(h);
-  if (st != PTG_OK) { delete h; return st; }
-  *out = h;
-  return PTG_OK;
 }
 
 int ptg_set_spectrum(ptg_handle* h, const ptg_spectrum* spec) {
@@ -883,27 +895,33 @@ int ptg_get_options(const ptg_handle* h, ptg_options* out) {
 }
 
 int ptg_set_options(ptg_handle* h, const ptg_options* opt) {
-  if (!h || !opt) return PTG_ERR_INVALID;
-  if (opt->device != h->device) { h->last_error = "options name another device"; return PTG_ERR_INVALID; }
-  if (opt->block_size != 0 && (opt->block_size < 32 || opt->block_size > 256 || opt->block_size % 32)) {
-    h->last_error = "block_size must be 0 or a multiple of 32 up to 256";
+  try {
+    if (!h || !opt) return PTG_ERR_INVALID;
+    if (opt->device != h->device) { h->last_error = "options name another device"; return PTG_ERR_INVALID; }
+    if (opt->block_size != 0 && (opt->block_size < 32 || opt->block_size > 256 || opt->block_size % 32)) {
+      h->last_error = "block_size must be 0 or a multiple of 32 up to 256";
+      return PTG_ERR_INVALID;
+    }
+    if (opt->reserved != 0) { h->last_error = "ptg_options.reserved must be 0"; return PTG_ERR_INVALID; }
+    const bool rebuild = opt->bvh_leaf != h->opt.bvh_leaf;
+    const ptg_options old = h->opt;
+    h->opt = *opt;
+    if (rebuild) {
+      if (cudaSetDevice(h->device) != cudaSuccess) { h->opt = old; return PTG_ERR_CUDA; }
+      if (cudaStreamSynchronize(h->stream) != cudaSuccess) { h->opt = old; return PTG_ERR_CUDA; }
+      const int st = build_blob(h);
+      if (st != PTG_OK) {
+        h->opt = old;
+        build_blob(h);
+        return st;
+      }
+    }
+    return PTG_OK;
+  } catch (const std::bad_alloc&) {
+    return PTG_ERR_NOMEM;
+  } catch (...) {
     return PTG_ERR_INVALID;
   }
-  if (opt->reserved != 0) { h->last_error = "ptg_options.reserved must be 0"; return PTG_ERR_INVALID; }
-  const bool rebuild = opt->bvh_leaf != h->opt.bvh_leaf;
-  const ptg_options old = h->opt;
-  h->opt = *opt;
-  if (rebuild) {
-    if (cudaSetDevice(h->device) != cudaSuccess) { h->opt = old; return PTG_ERR_CUDA; }
-    if (cudaStreamSynchronize(h->stream) != cudaSuccess) { h->opt = old; return PTG_ERR_CUDA; }
-    const int st = build_blob(h);
-    if (st != PTG_OK) {
-      h->opt = old;
-      build_blob(h);
-      return st;
-    }
-  }
-  return PTG_OK;
 }
 
 void ptg_destroy(ptg_handle* h) {
@@ -916,379 +934,415 @@ void ptg_destroy(ptg_handle* h) {
 int ptg_transmission(ptg_handle* h, double mfp_nm, int32_t nangle, int64_t np, int32_t rank,
                      int32_t nranks, uint64_t seed, int32_t precision, double* transmit,
                      double* stderr_opt) {
-  ptg::NvtxRange nvtx("ptg_transmission");
-  if (!h || !transmit) return PTG_ERR_INVALID;
-  if (nangle < 2 || np < 1 || nranks < 1 || rank < 0 || rank >= nranks) return PTG_ERR_INVALID;
-  if (precision != PTG_PREC_FP32 && precision != PTG_PREC_FP64) return PTG_ERR_INVALID;
-  if (!(mfp_nm > 0.0)) return PTG_ERR_INVALID;
-  const int64_t nm = (int64_t)h->spec.nb * h->spec.nk;
-  const int64_t ntask = nm * (nangle - 1);
-  std::vector<ptg::TaskHost> tasks(ntask);
-  const double half_pi = 3.14159265358979323846 * 0.5;
-  for (int64_t t = 0; t < ntask; ++t) {
-    const int64_t m = t % nm, ia = t / nm;
-    const double theta = 0.0 + (double)ia / (double)(nangle - 1) * half_pi;
-    tasks[t] = {mfp_nm, cos(theta), sin(theta), h->spec.omega[m]};
+  try {
+    ptg::NvtxRange nvtx("ptg_transmission");
+    if (!h || !transmit) return PTG_ERR_INVALID;
+    if (nangle < 2 || np < 1 || nranks < 1 || rank < 0 || rank >= nranks) return PTG_ERR_INVALID;
+    if (precision != PTG_PREC_FP32 && precision != PTG_PREC_FP64) return PTG_ERR_INVALID;
+    if (!(mfp_nm > 0.0)) return PTG_ERR_INVALID;
+    const int64_t nm = (int64_t)h->spec.nb * h->spec.nk;
+    const int64_t ntask = nm * (nangle - 1);
+    std::vector<ptg::TaskHost> tasks(ntask);
+    const double half_pi = 3.14159265358979323846 * 0.5;
+    for (int64_t t = 0; t < ntask; ++t) {
+      const int64_t m = t % nm, ia = t / nm;
+      const double theta = 0.0 + (double)ia / (double)(nangle - 1) * half_pi;
+      tasks[t] = {mfp_nm, cos(theta), sin(theta), h->spec.omega[m]};
+    }
+    Transport T;
+    T.ntask = ntask;
+    T.np = np;
+    T.np_local = np_local_of(np, rank, nranks);
+    if (T.np_local > 2147483647LL) return PTG_ERR_INVALID;
+    T.rank = rank;
+    T.nranks = nranks;
+    T.seed = seed;
+    T.precision = precision;
+    T.tasks = &tasks;
+    int st = run_transport(h, T);
+    if (st != PTG_OK) return st;
+    std::vector<unsigned long long> cnt(ntask);
+    CU(cudaMemcpyAsync(cnt.data(), h->counts.p, sizeof(unsigned long long) * ntask,
+                       cudaMemcpyDeviceToHost, h->stream));
+    h->last.d2h_bytes += sizeof(unsigned long long) * ntask;
+    st = finish_stats(h);
+    if (st != PTG_OK) return st;
+    for (int64_t t = 0; t < nm * nangle; ++t) {
+      double v = 0.0;
+      if (t < ntask) v = (double)cnt[t] / (double)np;
+      transmit[t] = v;
+      if (stderr_opt) stderr_opt[t] = sqrt(v * (1.0 - v) / (double)np);
+    }
+    return check_lost(h);
+  } catch (const std::bad_alloc&) {
+    return PTG_ERR_NOMEM;
+  } catch (...) {
+    return PTG_ERR_INVALID;
   }
-  Transport T;
-  T.ntask = ntask;
-  T.np = np;
-  T.np_local = np_local_of(np, rank, nranks);
-  if (T.np_local > 2147483647LL) return PTG_ERR_INVALID;
-  T.rank = rank;
-  T.nranks = nranks;
-  T.seed = seed;
-  T.precision = precision;
-  T.tasks = &tasks;
-  int st = run_transport(h, T);
-  if (st != PTG_OK) return st;
-  std::vector<unsigned long long> cnt(ntask);
-  CU(cudaMemcpyAsync(cnt.data(), h->counts.p, sizeof(unsigned long long) * ntask,
-                     cudaMemcpyDeviceToHost, h->stream));
-  h->last.d2h_bytes += sizeof(unsigned long long) * ntask;
-  st = finish_stats(h);
-  if (st != PTG_OK) return st;
-  for (int64_t t = 0; t < nm * nangle; ++t) {
-    double v = 0.0;
-    if (t < ntask) v = (double)cnt[t] / (double)np;
-    transmit[t] = v;
-    if (stderr_opt) stderr_opt[t] = sqrt(v * (1.0 - v) / (double)np);
-  }
-  return check_lost(h);
 }
 
 int ptg_kappa(ptg_handle* h, const ptg_run* run, ptg_kappa_out* out) {
-  ptg::NvtxRange nvtx("ptg_kappa");
-  if (!h || !run || !out) return PTG_ERR_INVALID;
-  std::string why;
-  if (!ptg::run_valid(h->spec, run, &why)) { h->last_error = why; return PTG_ERR_INVALID; }
-  if (run->precision != PTG_PREC_FP32 && run->precision != PTG_PREC_FP64) return PTG_ERR_INVALID;
-  const int ns = run->kind_mfp == PTG_MFP_GRID ? run->nmfp : 1;
-  if (ns > 64) { h->last_error = "at most 64 grid MFPs"; return PTG_ERR_UNSUPPORTED; }
-  std::vector<ptg::TaskHost> tasks;
-  ptg::run_tasks(h->spec, run, &tasks);
-  Transport T;
-  T.ntask = (int64_t)tasks.size();
-  T.np = run->np;
-  T.np_local = np_local_of(run->np, run->rank, run->nranks);
-  if (T.np_local > 2147483647LL) return PTG_ERR_INVALID;
-  T.rank = run->rank;
-  T.nranks = run->nranks;
-  T.seed = run->seed;
-  T.stream = run->stream;
-  T.precision = run->precision;
-  T.tasks = &tasks;
-  int st = run_transport(h, T);
-  if (st != PTG_OK) return st;
-  /* FP64 reduction on the device */
-  const int64_t nm = h->spec.nmode();
-  ptg::ModeConst mc;
-  ptg::mode_constants(h->spec, run, &mc);
-  std::vector<double> coef;
-  double dS = 0.0;
-  ptg::simpson_weights(run->nangle, h->geom.box[0], &coef, &dS);
-  const int nbins = run->nbins;
-  CU(h->red_coef.ensure(sizeof(double) * coef.size()));
-  CU(h->red_K.ensure(sizeof(double) * nm));
-  CU(h->red_W.ensure(sizeof(double) * nm));
-  CU(h->red_mfp.ensure(sizeof(double) * nm));
-  CU(h->red_bin.ensure(sizeof(int) * nm));
-  CU(h->red_grid.ensure(sizeof(double) * ns));
-  CU(h->red_tc.ensure(sizeof(double) * nm));
-  CU(h->red_kv.ensure(sizeof(double) * nm));
-  CU(h->red_bw.ensure(sizeof(double) * nm));
-  CU(h->red_bv.ensure(sizeof(double) * nm));
-  CU(h->red_emfp.ensure(sizeof(double) * nm));
-  CU(h->red_trans.ensure(sizeof(double) * nm * ns * run->nangle));
-  CU(h->red_result.ensure(sizeof(double) * (2 + 3 * (size_t)nbins)));
-  cudaStream_t s = h->stream;
-  CU(cudaMemcpyAsync(h->red_coef.p, coef.data(), sizeof(double) * coef.size(), cudaMemcpyHostToDevice, s));
-  CU(cudaMemcpyAsync(h->red_K.p, mc.K.data(), sizeof(double) * nm, cudaMemcpyHostToDevice, s));
-  CU(cudaMemcpyAsync(h->red_W.p, mc.W.data(), sizeof(double) * nm, cudaMemcpyHostToDevice, s));
-  CU(cudaMemcpyAsync(h->red_mfp.p, mc.mfp_m.data(), sizeof(double) * nm, cudaMemcpyHostToDevice, s));
-  CU(cudaMemcpyAsync(h->red_bin.p, mc.bin.data(), sizeof(int) * nm, cudaMemcpyHostToDevice, s));
-  if (run->kind_mfp == PTG_MFP_GRID)
-    CU(cudaMemcpyAsync(h->red_grid.p, run->mfp_grid_nm, sizeof(double) * ns, cudaMemcpyHostToDevice, s));
-  h->last.h2d_bytes += sizeof(double) * (coef.size() + 3 * (size_t)nm) + sizeof(int) * nm +
-                       (run->kind_mfp == PTG_MFP_GRID ? sizeof(double) * ns : 0);
-  ptg::ReduceIn in;
-  memset(&in, 0, sizeof(in));
-  in.counts = h->counts.as<const unsigned long long>();
-  in.nmode = nm;
-  in.nangle = run->nangle;
-  in.ns = ns;
-  in.kind_mfp = run->kind_mfp;
-  in.nbins = nbins;
-  in.np = (double)run->np;
-  in.dS = dS;
-  in.tnorm = 0.75 * h->geom.box[0];
-  in.coef = h->red_coef.as<const double>();
-  in.K = h->red_K.as<const double>();
-  in.W = h->red_W.as<const double>();
-  in.mfp_m = h->red_mfp.as<const double>();
-  in.bin = h->red_bin.as<const int>();
-  in.grid = h->red_grid.as<const double>();
-  in.tc = h->red_tc.as<double>();
-  in.kv = h->red_kv.as<double>();
-  in.bw = h->red_bw.as<double>();
-  in.bv = h->red_bv.as<double>();
-  in.emfp_nm = h->red_emfp.as<double>();
-  in.transmit = h->red_trans.as<double>();
-  in.result = h->red_result.as<double>();
-  {
-    ptg::NvtxRange nvtx("ptg kappa reduction");
-    CU(cudaEventRecord(h->ev[2], s));
-    CU(ptg::launch_kappa_reduce(in, s));
-    CU(cudaEventRecord(h->ev[3], s));
+  try {
+    ptg::NvtxRange nvtx("ptg_kappa");
+    if (!h || !run || !out) return PTG_ERR_INVALID;
+    std::string why;
+    if (!ptg::run_valid(h->spec, run, &why)) { h->last_error = why; return PTG_ERR_INVALID; }
+    if (run->precision != PTG_PREC_FP32 && run->precision != PTG_PREC_FP64) return PTG_ERR_INVALID;
+    const int ns = run->kind_mfp == PTG_MFP_GRID ? run->nmfp : 1;
+    if (ns > 64) { h->last_error = "at most 64 grid MFPs"; return PTG_ERR_UNSUPPORTED; }
+    std::vector<ptg::TaskHost> tasks;
+    ptg::run_tasks(h->spec, run, &tasks);
+    Transport T;
+    T.ntask = (int64_t)tasks.size();
+    T.np = run->np;
+    T.np_local = np_local_of(run->np, run->rank, run->nranks);
+    if (T.np_local > 2147483647LL) return PTG_ERR_INVALID;
+    T.rank = run->rank;
+    T.nranks = run->nranks;
+    T.seed = run->seed;
+    T.stream = run->stream;
+    T.precision = run->precision;
+    T.tasks = &tasks;
+    int st = run_transport(h, T);
+    if (st != PTG_OK) return st;
+    /* FP64 reduction on the device */
+    const int64_t nm = h->spec.nmode();
+    ptg::ModeConst mc;
+    ptg::mode_constants(h->spec, run, &mc);
+    std::vector<double> coef;
+    double dS = 0.0;
+    ptg::simpson_weights(run->nangle, h->geom.box[0], &coef, &dS);
+    const int nbins = run->nbins;
+    CU(h->red_coef.ensure(sizeof(double) * coef.size()));
+    CU(h->red_K.ensure(sizeof(double) * nm));
+    CU(h->red_W.ensure(sizeof(double) * nm));
+    CU(h->red_mfp.ensure(sizeof(double) * nm));
+    CU(h->red_bin.ensure(sizeof(int) * nm));
+    CU(h->red_grid.ensure(sizeof(double) * ns));
+    CU(h->red_tc.ensure(sizeof(double) * nm));
+    CU(h->red_kv.ensure(sizeof(double) * nm));
+    CU(h->red_bw.ensure(sizeof(double) * nm));
+    CU(h->red_bv.ensure(sizeof(double) * nm));
+    CU(h->red_emfp.ensure(sizeof(double) * nm));
+    CU(h->red_trans.ensure(sizeof(double) * nm * ns * run->nangle));
+    CU(h->red_result.ensure(sizeof(double) * (2 + 3 * (size_t)nbins)));
+    cudaStream_t s = h->stream;
+    CU(cudaMemcpyAsync(h->red_coef.p, coef.data(), sizeof(double) * coef.size(), cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(h->red_K.p, mc.K.data(), sizeof(double) * nm, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(h->red_W.p, mc.W.data(), sizeof(double) * nm, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(h->red_mfp.p, mc.mfp_m.data(), sizeof(double) * nm, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(h->red_bin.p, mc.bin.data(), sizeof(int) * nm, cudaMemcpyHostToDevice, s));
+    if (run->kind_mfp == PTG_MFP_GRID)
+      CU(cudaMemcpyAsync(h->red_grid.p, run->mfp_grid_nm, sizeof(double) * ns, cudaMemcpyHostToDevice, s));
+    h->last.h2d_bytes += sizeof(double) * (coef.size() + 3 * (size_t)nm) + sizeof(int) * nm +
+                         (run->kind_mfp == PTG_MFP_GRID ? sizeof(double) * ns : 0);
+    ptg::ReduceIn in;
+    memset(&in, 0, sizeof(in));
+    in.counts = h->counts.as<const unsigned long long>();
+    in.nmode = nm;
+    in.nangle = run->nangle;
+    in.ns = ns;
+    in.kind_mfp = run->kind_mfp;
+    in.nbins = nbins;
+    in.np = (double)run->np;
+    in.dS = dS;
+    in.tnorm = 0.75 * h->geom.box[0];
+    in.coef = h->red_coef.as<const double>();
+    in.K = h->red_K.as<const double>();
+    in.W = h->red_W.as<const double>();
+    in.mfp_m = h->red_mfp.as<const double>();
+    in.bin = h->red_bin.as<const int>();
+    in.grid = h->red_grid.as<const double>();
+    in.tc = h->red_tc.as<double>();
+    in.kv = h->red_kv.as<double>();
+    in.bw = h->red_bw.as<double>();
+    in.bv = h->red_bv.as<double>();
+    in.emfp_nm = h->red_emfp.as<double>();
+    in.transmit = h->red_trans.as<double>();
+    in.result = h->red_result.as<double>();
+    {
+      ptg::NvtxRange nvtx("ptg kappa reduction");
+      CU(cudaEventRecord(h->ev[2], s));
+      CU(ptg::launch_kappa_reduce(in, s));
+      CU(cudaEventRecord(h->ev[3], s));
+    }
+    std::vector<double> res(2 + 3 * (size_t)nbins);
+    CU(cudaMemcpyAsync(res.data(), h->red_result.p, sizeof(double) * res.size(), cudaMemcpyDeviceToHost, s));
+    if (out->emfp_nm)
+      CU(cudaMemcpyAsync(out->emfp_nm, h->red_emfp.p, sizeof(double) * nm, cudaMemcpyDeviceToHost, s));
+    if (out->transmit)
+      CU(cudaMemcpyAsync(out->transmit, h->red_trans.p, sizeof(double) * nm * ns * run->nangle,
+                         cudaMemcpyDeviceToHost, s));
+    if (out->counts)
+      CU(cudaMemcpyAsync(out->counts, h->counts.p, sizeof(unsigned long long) * T.ntask,
+                         cudaMemcpyDeviceToHost, s));
+    h->last.d2h_bytes += sizeof(double) * res.size() + (out->emfp_nm ? sizeof(double) * nm : 0) +
+                         (out->transmit ? sizeof(double) * nm * ns * run->nangle : 0) +
+                         (out->counts ? sizeof(unsigned long long) * T.ntask : 0);
+    st = finish_stats(h);
+    if (st != PTG_OK) return st;
+    float rms = 0.f;
+    CU(cudaEventElapsedTime(&rms, h->ev[2], h->ev[3]));
+    h->last.reduce_ms = rms;
+    h->last.launches += 2;
+    out->kappa = res[0];
+    out->kappa_stderr = sqrt(res[1]);
+    for (int b = 0; b < nbins; ++b) {
+      const double sw = res[2 + 3 * b], swt = res[3 + 3 * b], sv = res[4 + 3 * b];
+      if (out->bin_T) out->bin_T[b] = sw > 0 ? swt / sw : 0.0;
+      if (out->bin_T_stderr) out->bin_T_stderr[b] = sw > 0 ? sqrt(sv) / sw : 0.0;
+    }
+    out->flights = h->last.flights;
+    out->lost = h->last.lost;
+    out->samples = h->last.samples;
+    out->kernel_ms = h->last.kernel_ms;
+    return check_lost(h);
+  } catch (const std::bad_alloc&) {
+    return PTG_ERR_NOMEM;
+  } catch (...) {
+    return PTG_ERR_INVALID;
   }
-  std::vector<double> res(2 + 3 * (size_t)nbins);
-  CU(cudaMemcpyAsync(res.data(), h->red_result.p, sizeof(double) * res.size(), cudaMemcpyDeviceToHost, s));
-  if (out->emfp_nm)
-    CU(cudaMemcpyAsync(out->emfp_nm, h->red_emfp.p, sizeof(double) * nm, cudaMemcpyDeviceToHost, s));
-  if (out->transmit)
-    CU(cudaMemcpyAsync(out->transmit, h->red_trans.p, sizeof(double) * nm * ns * run->nangle,
-                       cudaMemcpyDeviceToHost, s));
-  if (out->counts)
-    CU(cudaMemcpyAsync(out->counts, h->counts.p, sizeof(unsigned long long) * T.ntask,
-                       cudaMemcpyDeviceToHost, s));
-  h->last.d2h_bytes += sizeof(double) * res.size() + (out->emfp_nm ? sizeof(double) * nm : 0) +
-                       (out->transmit ? sizeof(double) * nm * ns * run->nangle : 0) +
-                       (out->counts ? sizeof(unsigned long long) * T.ntask : 0);
-  st = finish_stats(h);
-  if (st != PTG_OK) return st;
-  float rms = 0.f;
-  CU(cudaEventElapsedTime(&rms, h->ev[2], h->ev[3]));
-  h->last.reduce_ms = rms;
-  h->last.launches += 2;
-  out->kappa = res[0];
-  out->kappa_stderr = sqrt(res[1]);
-  for (int b = 0; b < nbins; ++b) {
-    const double sw = res[2 + 3 * b], swt = res[3 + 3 * b], sv = res[4 + 3 * b];
-    if (out->bin_T) out->bin_T[b] = sw > 0 ? swt / sw : 0.0;
-    if (out->bin_T_stderr) out->bin_T_stderr[b] = sw > 0 ? sqrt(sv) / sw : 0.0;
-  }
-  out->flights = h->last.flights;
-  out->lost = h->last.lost;
-  out->samples = h->last.samples;
-  out->kernel_ms = h->last.kernel_ms;
-  return check_lost(h);
 }
 
 int ptg_kappa_from_counts(const ptg_geometry* geom, const ptg_spectrum* spec, const ptg_run* run,
                           const uint64_t* counts, ptg_kappa_out* out) {
-  if (!geom || !spec || !run || !counts || !out) return PTG_ERR_INVALID;
-  ptg::SpecSoA S;
-  std::string why;
-  if (ptg::copy_spectrum(spec, &S, &why) != PTG_OK) return PTG_ERR_INVALID;
-  if (!ptg::run_valid(S, run, &why)) return PTG_ERR_INVALID;
-  return ptg::assemble_host(S, run, geom->box[0], counts, out, nullptr, nullptr);
+  try {
+    if (!geom || !spec || !run || !counts || !out) return PTG_ERR_INVALID;
+    ptg::SpecSoA S;
+    std::string why;
+    if (ptg::copy_spectrum(spec, &S, &why) != PTG_OK) return PTG_ERR_INVALID;
+    if (!ptg::run_valid(S, run, &why)) return PTG_ERR_INVALID;
+    return ptg::assemble_host(S, run, geom->box[0], counts, out, nullptr, nullptr);
+  } catch (const std::bad_alloc&) {
+    return PTG_ERR_NOMEM;
+  } catch (...) {
+    return PTG_ERR_INVALID;
+  }
 }
 
 int ptg_trace(ptg_handle* h, const ptg_run* run, int64_t n, const uint64_t* samples,
               int64_t cap_positions, float* pos, int64_t* npos, int32_t* end_side) {
-  ptg::NvtxRange nvtx("ptg_trace");
-  if (!h || !run || n < 1 || !samples || !npos || !end_side) return PTG_ERR_INVALID;
-  std::string why;
-  if (!ptg::run_valid(h->spec, run, &why)) { h->last_error = why; return PTG_ERR_INVALID; }
-  std::vector<ptg::TaskHost> tasks;
-  ptg::run_tasks(h->spec, run, &tasks);
-  const uint64_t total = (uint64_t)tasks.size() * (uint64_t)run->np;
-  for (int64_t i = 0; i < n; ++i)
-    if (samples[i] >= total) { h->last_error = "sample id beyond ntask * np"; return PTG_ERR_INVALID; }
-  CU(cudaSetDevice(h->device));
-  CU(h->adj_list.ensure(sizeof(unsigned long long) * n));
-  CU(h->tr_npos.ensure(sizeof(long long) * n));
-  CU(h->tr_end.ensure(sizeof(int) * n));
-  CU(h->tr_off.ensure(sizeof(long long) * (n + 1)));
-  CU(cudaMemcpyAsync(h->adj_list.p, samples, sizeof(unsigned long long) * n, cudaMemcpyHostToDevice,
-                     h->stream));
-  Transport T;
-  T.ntask = (int64_t)tasks.size();
-  T.np = run->np;
-  T.np_local = 0;  /* no chunk queue: the kernel walks the replay list */
-  T.seed = run->seed;
-  T.stream = run->stream;
-  T.precision = PTG_PREC_FP32;
-  T.tasks = &tasks;
-  T.mode = ptg::MODE_TRACE;
-  T.alist = h->adj_list.as<const unsigned long long>();
-  T.alist_n = (long long)n;
-  T.trace_off = h->tr_off.as<const long long>();
-  T.trace_npos = h->tr_npos.as<long long>();
-  T.trace_end = h->tr_end.as<int>();
-  /* pass 1: lengths and exits */
-  int st = run_transport(h, T);
-  if (st != PTG_OK) return st;
-  std::vector<long long> cnt(n);
-  std::vector<int> ends(n);
-  CU(cudaMemcpyAsync(cnt.data(), h->tr_npos.p, sizeof(long long) * n, cudaMemcpyDeviceToHost, h->stream));
-  CU(cudaMemcpyAsync(ends.data(), h->tr_end.p, sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream));
-  st = finish_stats(h);
-  if (st != PTG_OK) return st;
-  long long sum = 0;
-  for (int64_t i = 0; i < n; ++i) {
-    npos[i] = cnt[i];
-    end_side[i] = ends[i];
-    sum += cnt[i];
+  try {
+    ptg::NvtxRange nvtx("ptg_trace");
+    if (!h || !run || n < 1 || !samples || !npos || !end_side) return PTG_ERR_INVALID;
+    std::string why;
+    if (!ptg::run_valid(h->spec, run, &why)) { h->last_error = why; return PTG_ERR_INVALID; }
+    std::vector<ptg::TaskHost> tasks;
+    ptg::run_tasks(h->spec, run, &tasks);
+    const uint64_t total = (uint64_t)tasks.size() * (uint64_t)run->np;
+    for (int64_t i = 0; i < n; ++i)
+      if (samples[i] >= total) { h->last_error = "sample id beyond ntask * np"; return PTG_ERR_INVALID; }
+    CU(cudaSetDevice(h->device));
+    CU(h->adj_list.ensure(sizeof(unsigned long long) * n));
+    CU(h->tr_npos.ensure(sizeof(long long) * n));
+    CU(h->tr_end.ensure(sizeof(int) * n));
+    CU(h->tr_off.ensure(sizeof(long long) * (n + 1)));
+    CU(cudaMemcpyAsync(h->adj_list.p, samples, sizeof(unsigned long long) * n, cudaMemcpyHostToDevice,
+                       h->stream));
+    Transport T;
+    T.ntask = (int64_t)tasks.size();
+    T.np = run->np;
+    T.np_local = 0;  /* no chunk queue: the kernel walks the replay list */
+    T.seed = run->seed;
+    T.stream = run->stream;
+    T.precision = PTG_PREC_FP32;
+    T.tasks = &tasks;
+    T.mode = ptg::MODE_TRACE;
+    T.alist = h->adj_list.as<const unsigned long long>();
+    T.alist_n = (long long)n;
+    T.trace_off = h->tr_off.as<const long long>();
+    T.trace_npos = h->tr_npos.as<long long>();
+    T.trace_end = h->tr_end.as<int>();
+    /* pass 1: lengths and exits */
+    int st = run_transport(h, T);
+    if (st != PTG_OK) return st;
+    std::vector<long long> cnt(n);
+    std::vector<int> ends(n);
+    CU(cudaMemcpyAsync(cnt.data(), h->tr_npos.p, sizeof(long long) * n, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaMemcpyAsync(ends.data(), h->tr_end.p, sizeof(int) * n, cudaMemcpyDeviceToHost, h->stream));
+    st = finish_stats(h);
+    if (st != PTG_OK) return st;
+    long long sum = 0;
+    for (int64_t i = 0; i < n; ++i) {
+      npos[i] = cnt[i];
+      end_side[i] = ends[i];
+      sum += cnt[i];
+    }
+    if (!pos) return PTG_OK;
+    if (sum > cap_positions) { h->last_error = "position buffer smaller than the trajectories"; return PTG_ERR_INVALID; }
+    /* pass 2: the same trajectories, positions recorded at exclusive offsets */
+    std::vector<long long> off(n + 1, 0);
+    for (int64_t i = 0; i < n; ++i) off[i + 1] = off[i] + cnt[i];
+    CU(h->tr_pos.ensure(sizeof(float) * 3 * (size_t)(sum > 0 ? sum : 1)));
+    CU(cudaMemcpyAsync(h->tr_off.p, off.data(), sizeof(long long) * (n + 1), cudaMemcpyHostToDevice,
+                       h->stream));
+    T.trace = h->tr_pos.as<float>();
+    st = run_transport(h, T);
+    if (st != PTG_OK) return st;
+    CU(cudaMemcpyAsync(pos, h->tr_pos.p, sizeof(float) * 3 * (size_t)sum, cudaMemcpyDeviceToHost,
+                       h->stream));
+    st = finish_stats(h);
+    if (st != PTG_OK) return st;
+    h->last.d2h_bytes += sizeof(float) * 3 * (size_t)sum;
+    return PTG_OK;
+  } catch (const std::bad_alloc&) {
+    return PTG_ERR_NOMEM;
+  } catch (...) {
+    return PTG_ERR_INVALID;
   }
-  if (!pos) return PTG_OK;
-  if (sum > cap_positions) { h->last_error = "position buffer smaller than the trajectories"; return PTG_ERR_INVALID; }
-  /* pass 2: the same trajectories, positions recorded at exclusive offsets */
-  std::vector<long long> off(n + 1, 0);
-  for (int64_t i = 0; i < n; ++i) off[i + 1] = off[i] + cnt[i];
-  CU(h->tr_pos.ensure(sizeof(float) * 3 * (size_t)(sum > 0 ? sum : 1)));
-  CU(cudaMemcpyAsync(h->tr_off.p, off.data(), sizeof(long long) * (n + 1), cudaMemcpyHostToDevice,
-                     h->stream));
-  T.trace = h->tr_pos.as<float>();
-  st = run_transport(h, T);
-  if (st != PTG_OK) return st;
-  CU(cudaMemcpyAsync(pos, h->tr_pos.p, sizeof(float) * 3 * (size_t)sum, cudaMemcpyDeviceToHost,
-                     h->stream));
-  st = finish_stats(h);
-  if (st != PTG_OK) return st;
-  h->last.d2h_bytes += sizeof(float) * 3 * (size_t)sum;
-  return PTG_OK;
 }
 
 int ptg_write_trace(ptg_handle* h, const ptg_run* run, int32_t particle_trace, const char* path) {
-  if (!h || !run || particle_trace < 1 || !path) return PTG_ERR_INVALID;
-  std::string why;
-  if (!ptg::run_valid(h->spec, run, &why)) { h->last_error = why; return PTG_ERR_INVALID; }
-  const uint64_t total = (uint64_t)ptg::run_ntask(h->spec, run) * (uint64_t)run->np;
-  /* interval_trace of RayTrace, src/RTMCphon.f90:3373-3375 (one rank) */
-  uint64_t interval = total / (uint64_t)particle_trace;
-  if (interval < 1) interval = 1;
-  std::vector<uint64_t> samples;
-  for (uint64_t k = 0; k < (uint64_t)particle_trace && k * interval < total; ++k)
-    samples.push_back(k * interval);
-  const int64_t n = (int64_t)samples.size();
-  std::vector<int64_t> npos(n);
-  std::vector<int32_t> ends(n);
-  int st = ptg_trace(h, run, n, samples.data(), 0, nullptr, npos.data(), ends.data());
-  if (st != PTG_OK) return st;
-  int64_t sum = 0;
-  for (int64_t v : npos) sum += v;
-  std::vector<float> pos(3 * (size_t)(sum > 0 ? sum : 1));
-  st = ptg_trace(h, run, n, samples.data(), sum, pos.data(), npos.data(), ends.data());
-  if (st != PTG_OK) return st;
-  FILE* f = fopen(path, "w");
-  if (!f) return PTG_ERR_IO;
-  fprintf(f, "# Datatype = trace\n");
-  fprintf(f, "# particle_trace = %8d\n", (int)particle_trace);
-  fprintf(f, "# interval_trace = %8lld\n", (long long)interval);
-  fprintf(f, "\n");
-  size_t k = 0;
-  for (int64_t i = 0; i < n; ++i) {
-    for (int64_t j = 0; j < npos[i]; ++j, ++k)
-      fprintf(f, " %15.8E %15.8E %15.8E\n", pos[3 * k], pos[3 * k + 1], pos[3 * k + 2]);
-    fprintf(f, "\n\n");
+  try {
+    if (!h || !run || particle_trace < 1 || !path) return PTG_ERR_INVALID;
+    std::string why;
+    if (!ptg::run_valid(h->spec, run, &why)) { h->last_error = why; return PTG_ERR_INVALID; }
+    const uint64_t total = (uint64_t)ptg::run_ntask(h->spec, run) * (uint64_t)run->np;
+    /* interval_trace of RayTrace, src/RTMCphon.f90:3373-3375 (one rank) */
+    uint64_t interval = total / (uint64_t)particle_trace;
+    if (interval < 1) interval = 1;
+    std::vector<uint64_t> samples;
+    for (uint64_t k = 0; k < (uint64_t)particle_trace && k * interval < total; ++k)
+      samples.push_back(k * interval);
+    const int64_t n = (int64_t)samples.size();
+    std::vector<int64_t> npos(n);
+    std::vector<int32_t> ends(n);
+    int st = ptg_trace(h, run, n, samples.data(), 0, nullptr, npos.data(), ends.data());
+    if (st != PTG_OK) return st;
+    int64_t sum = 0;
+    for (int64_t v : npos) sum += v;
+    std::vector<float> pos(3 * (size_t)(sum > 0 ? sum : 1));
+    st = ptg_trace(h, run, n, samples.data(), sum, pos.data(), npos.data(), ends.data());
+    if (st != PTG_OK) return st;
+    FILE* f = fopen(path, "w");
+    if (!f) return PTG_ERR_IO;
+    fprintf(f, "# Datatype = trace\n");
+    fprintf(f, "# particle_trace = %8d\n", (int)particle_trace);
+    fprintf(f, "# interval_trace = %8lld\n", (long long)interval);
+    fprintf(f, "\n");
+    size_t k = 0;
+    for (int64_t i = 0; i < n; ++i) {
+      for (int64_t j = 0; j < npos[i]; ++j, ++k)
+        fprintf(f, " %15.8E %15.8E %15.8E\n", pos[3 * k], pos[3 * k + 1], pos[3 * k + 2]);
+      fprintf(f, "\n\n");
+    }
+    return fclose(f) == 0 ? PTG_OK : PTG_ERR_IO;
+  } catch (const std::bad_alloc&) {
+    return PTG_ERR_NOMEM;
+  } catch (...) {
+    return PTG_ERR_INVALID;
   }
-  return fclose(f) == 0 ? PTG_OK : PTG_ERR_IO;
 }
 
 int ptg_adjoint(ptg_handle* h, const ptg_run* run, ptg_adjoint_out* out) {
-  ptg::NvtxRange nvtx("ptg_adjoint");
-  if (!h || !run || !out) return PTG_ERR_INVALID;
-  std::string why;
-  if (!ptg::run_valid(h->spec, run, &why)) { h->last_error = why; return PTG_ERR_INVALID; }
-  const int ns = run->kind_mfp == PTG_MFP_GRID ? run->nmfp : 1;
-  if (ns > 64) return PTG_ERR_UNSUPPORTED;
-  std::vector<ptg::TaskHost> tasks;
-  ptg::run_tasks(h->spec, run, &tasks);
-  const int64_t ntask = (int64_t)tasks.size();
-  const int nsurf = h->geom.nsurf();
-  const unsigned long long cap = 1ull << 25;
-  CU(cudaSetDevice(h->device));
-  /* 1. forward pass that lists the samples leaving through x+ */
-  Transport T;
-  T.ntask = ntask;
-  T.np = run->np;
-  T.np_local = np_local_of(run->np, run->rank, run->nranks);
-  if (T.np_local > 2147483647LL) return PTG_ERR_INVALID;
-  T.rank = run->rank;
-  T.nranks = run->nranks;
-  T.seed = run->seed;
-  T.stream = run->stream;
-  T.precision = PTG_PREC_FP32;
-  T.tasks = &tasks;
-  T.mode = ptg::MODE_LIST;
-  const unsigned long long total = (unsigned long long)ntask * (unsigned long long)T.np_local;
-  T.tlist_cap = total < cap ? total : cap;
-  CU(h->adj_list.ensure(sizeof(unsigned long long) * (T.tlist_cap ? T.tlist_cap : 1)));
-  T.tlist = h->adj_list.as<unsigned long long>();
-  int st = run_transport(h, T);
-  if (st != PTG_OK) return st;
-  std::vector<uint64_t> counts(ntask);
-  CU(cudaMemcpyAsync(counts.data(), h->counts.p, sizeof(uint64_t) * ntask, cudaMemcpyDeviceToHost,
-                     h->stream));
-  st = finish_stats(h);
-  if (st != PTG_OK) return st;
-  const double fwd_ms = h->last.kernel_ms;
-  const uint64_t fwd_flights = h->last.flights;
-  const unsigned long long nlist = h->list_n;
-  if (nlist > T.tlist_cap) { h->last_error = "more than 2^25 transmitted samples"; return PTG_ERR_UNSUPPORTED; }
-  /* 2. kappa and d kappa / d T_task on the host */
-  ptg_kappa_out ko;
-  memset(&ko, 0, sizeof(ko));
-  std::vector<double> wtask;
-  double dks_an = 0.0;
-  st = ptg::assemble_host(h->spec, run, h->geom.box[0], counts.data(), &ko, &wtask, &dks_an);
-  if (st != PTG_OK) return st;
-  std::vector<float> wsample(ntask);
-  for (int64_t t = 0; t < ntask; ++t) wsample[t] = (float)(wtask[t] / (double)run->np);
-  CU(h->adj_w.ensure(sizeof(float) * ntask));
-  CU(cudaMemcpyAsync(h->adj_w.p, wsample.data(), sizeof(float) * ntask, cudaMemcpyHostToDevice,
-                     h->stream));
-  const size_t nacc = (size_t)ptg::kAdjBatches * (nsurf + 1);
-  CU(h->adj_acc.ensure(sizeof(double) * nacc));
-  CU(cudaMemsetAsync(h->adj_acc.p, 0, sizeof(double) * nacc, h->stream));
-  /* 3. replay of the listed samples with the score accumulation */
-  T.mode = ptg::MODE_ADJOINT;
-  T.tlist = nullptr;
-  T.tlist_cap = 0;
-  T.alist = h->adj_list.as<const unsigned long long>();
-  T.alist_n = (long long)nlist;
-  T.wsample = h->adj_w.as<const float>();
-  T.adj = h->adj_acc.as<double>();
-  st = run_transport(h, T);
-  if (st != PTG_OK) return st;
-  std::vector<double> acc(nacc);
-  CU(cudaMemcpyAsync(acc.data(), h->adj_acc.p, sizeof(double) * nacc, cudaMemcpyDeviceToHost,
-                     h->stream));
-  st = finish_stats(h);
-  if (st != PTG_OK) return st;
-  /* 4. batch sums and standard errors */
-  const int B = ptg::kAdjBatches;
-  auto reduce = [&](int col, double* mean_total, double* se) {
-    double sum = 0.0, sq = 0.0;
-    for (int b = 0; b < B; ++b) sum += acc[(size_t)b * (nsurf + 1) + col];
-    const double mb = sum / B;
-    for (int b = 0; b < B; ++b) {
-      const double d = acc[(size_t)b * (nsurf + 1) + col] - mb;
-      sq += d * d;
+  try {
+    ptg::NvtxRange nvtx("ptg_adjoint");
+    if (!h || !run || !out) return PTG_ERR_INVALID;
+    std::string why;
+    if (!ptg::run_valid(h->spec, run, &why)) { h->last_error = why; return PTG_ERR_INVALID; }
+    const int ns = run->kind_mfp == PTG_MFP_GRID ? run->nmfp : 1;
+    if (ns > 64) return PTG_ERR_UNSUPPORTED;
+    std::vector<ptg::TaskHost> tasks;
+    ptg::run_tasks(h->spec, run, &tasks);
+    const int64_t ntask = (int64_t)tasks.size();
+    const int nsurf = h->geom.nsurf();
+    const unsigned long long cap = 1ull << 25;
+    CU(cudaSetDevice(h->device));
+    /* 1. forward pass that lists the samples leaving through x+ */
+    Transport T;
+    T.ntask = ntask;
+    T.np = run->np;
+    T.np_local = np_local_of(run->np, run->rank, run->nranks);
+    if (T.np_local > 2147483647LL) return PTG_ERR_INVALID;
+    T.rank = run->rank;
+    T.nranks = run->nranks;
+    T.seed = run->seed;
+    T.stream = run->stream;
+    T.precision = PTG_PREC_FP32;
+    T.tasks = &tasks;
+    T.mode = ptg::MODE_LIST;
+    const unsigned long long total = (unsigned long long)ntask * (unsigned long long)T.np_local;
+    T.tlist_cap = total < cap ? total : cap;
+    CU(h->adj_list.ensure(sizeof(unsigned long long) * (T.tlist_cap ? T.tlist_cap : 1)));
+    T.tlist = h->adj_list.as<unsigned long long>();
+    int st = run_transport(h, T);
+    if (st != PTG_OK) return st;
+    std::vector<uint64_t> counts(ntask);
+    CU(cudaMemcpyAsync(counts.data(), h->counts.p, sizeof(uint64_t) * ntask, cudaMemcpyDeviceToHost,
+                       h->stream));
+    st = finish_stats(h);
+    if (st != PTG_OK) return st;
+    const double fwd_ms = h->last.kernel_ms;
+    const uint64_t fwd_flights = h->last.flights;
+    const unsigned long long nlist = h->list_n;
+    if (nlist > T.tlist_cap) { h->last_error = "more than 2^25 transmitted samples"; return PTG_ERR_UNSUPPORTED; }
+    /* 2. kappa and d kappa / d T_task on the host */
+    ptg_kappa_out ko;
+    memset(&ko, 0, sizeof(ko));
+    std::vector<double> wtask;
+    double dks_an = 0.0;
+    st = ptg::assemble_host(h->spec, run, h->geom.box[0], counts.data(), &ko, &wtask, &dks_an);
+    if (st != PTG_OK) return st;
+    std::vector<float> wsample(ntask);
+    for (int64_t t = 0; t < ntask; ++t) wsample[t] = (float)(wtask[t] / (double)run->np);
+    CU(h->adj_w.ensure(sizeof(float) * ntask));
+    CU(cudaMemcpyAsync(h->adj_w.p, wsample.data(), sizeof(float) * ntask, cudaMemcpyHostToDevice,
+                       h->stream));
+    const size_t nacc = (size_t)ptg::kAdjBatches * (nsurf + 1);
+    CU(h->adj_acc.ensure(sizeof(double) * nacc));
+    CU(cudaMemsetAsync(h->adj_acc.p, 0, sizeof(double) * nacc, h->stream));
+    /* 3. replay of the listed samples with the score accumulation */
+    T.mode = ptg::MODE_ADJOINT;
+    T.tlist = nullptr;
+    T.tlist_cap = 0;
+    T.alist = h->adj_list.as<const unsigned long long>();
+    T.alist_n = (long long)nlist;
+    T.wsample = h->adj_w.as<const float>();
+    T.adj = h->adj_acc.as<double>();
+    st = run_transport(h, T);
+    if (st != PTG_OK) return st;
+    std::vector<double> acc(nacc);
+    CU(cudaMemcpyAsync(acc.data(), h->adj_acc.p, sizeof(double) * nacc, cudaMemcpyDeviceToHost,
+                       h->stream));
+    st = finish_stats(h);
+    if (st != PTG_OK) return st;
+    /* 4. batch sums and standard errors */
+    const int B = ptg::kAdjBatches;
+    auto reduce = [&](int col, double* mean_total, double* se) {
+      double sum = 0.0, sq = 0.0;
+      for (int b = 0; b < B; ++b) sum += acc[(size_t)b * (nsurf + 1) + col];
+      const double mb = sum / B;
+      for (int b = 0; b < B; ++b) {
+        const double d = acc[(size_t)b * (nsurf + 1) + col] - mb;
+        sq += d * d;
+      }
+      *mean_total = sum;
+      *se = sqrt((double)B * sq / (B - 1));
+    };
+    for (int k = 0; k < nsurf; ++k) {
+      double v, e;
+      reduce(k, &v, &e);
+      const double p = h->geom.specularity[k];
+      const bool interior = p > 0.0 && p < 1.0;
+      if (out->dk_dp) out->dk_dp[k] = interior ? v : NAN;
+      if (out->dk_dp_stderr) out->dk_dp_stderr[k] = interior ? e : NAN;
     }
-    *mean_total = sum;
-    *se = sqrt((double)B * sq / (B - 1));
-  };
-  for (int k = 0; k < nsurf; ++k) {
-    double v, e;
-    reduce(k, &v, &e);
-    const double p = h->geom.specularity[k];
-    const bool interior = p > 0.0 && p < 1.0;
-    if (out->dk_dp) out->dk_dp[k] = interior ? v : NAN;
-    if (out->dk_dp_stderr) out->dk_dp_stderr[k] = interior ? e : NAN;
+    double vs, es;
+    reduce(nsurf, &vs, &es);
+    out->dk_dscale = (run->kind_mfp == PTG_MFP_PER_MODE ? vs : 0.0) + dks_an;
+    out->dk_dscale_stderr = run->kind_mfp == PTG_MFP_PER_MODE ? es : 0.0;
+    out->kappa = ko.kappa;
+    out->kappa_stderr = ko.kappa_stderr;
+    out->flights = fwd_flights + h->last.flights;
+    out->replayed = nlist;
+    out->mismatched = h->mismatch;
+    out->kernel_ms = fwd_ms + h->last.kernel_ms;
+    return PTG_OK;
+  } catch (const std::bad_alloc&) {
+    return PTG_ERR_NOMEM;
+  } catch (...) {
+    return PTG_ERR_INVALID;
   }
-  double vs, es;
-  reduce(nsurf, &vs, &es);
-  out->dk_dscale = (run->kind_mfp == PTG_MFP_PER_MODE ? vs : 0.0) + dks_an;
-  out->dk_dscale_stderr = run->kind_mfp == PTG_MFP_PER_MODE ? es : 0.0;
-  out->kappa = ko.kappa;
-  out->kappa_stderr = ko.kappa_stderr;
-  out->flights = fwd_flights + h->last.flights;
-  out->replayed = nlist;
-  out->mismatched = h->mismatch;
-  out->kernel_ms = fwd_ms + h->last.kernel_ms;
-  return PTG_OK;
 }
 
 int ptg_check_report(int32_t device, int64_t* violations, int32_t* first_code, int32_t* first_index,

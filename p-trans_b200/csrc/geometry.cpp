@@ -262,6 +262,7 @@ int build_geometry(const ptg_model* m, GeomSoA* out, std::string* why) {
   int fpos = 0, vpos = 0, mpos = 0;
   int32_t built = 6;
   for (int ig = 1; ig <= m->ngrain; ++ig) {
+    ptg::alloc_check();  /* allocation-failure injection point (tests) */
     GrainRec& g = grains[ig];
     for (int d = 0; d < 3; ++d) g.gen[d] = m->grain_generatrix[3 * (ig - 1) + d];
     const int shape = bricks ? m->grain_shape[ig - 1] : PTG_SHAPE_POLYGON;
@@ -643,16 +644,25 @@ struct ptg_geombuf {
 
 extern "C" int ptg_geometry_build(const ptg_model* model, const ptg_spectrum* spec,
                                   ptg_geombuf** out) {
-  (void)spec;
-  if (!out) return PTG_ERR_INVALID;
-  *out = nullptr;
-  ptg_geombuf* b = new (std::nothrow) ptg_geombuf();
-  if (!b) return PTG_ERR_NOMEM;
-  std::string why;
-  int st = ptg::build_geometry(model, &b->g, &why);
-  if (st != PTG_OK) { delete b; return st; }
-  *out = b;
-  return PTG_OK;
+  ptg_geombuf* b = nullptr;
+  try {
+    (void)spec;
+    if (!out) return PTG_ERR_INVALID;
+    *out = nullptr;
+    b = ptg::alloc_should_fail() ? nullptr : new (std::nothrow) ptg_geombuf();
+    if (!b) return PTG_ERR_NOMEM;
+    std::string why;
+    int st = ptg::build_geometry(model, &b->g, &why);
+    if (st != PTG_OK) { delete b; return st; }
+    *out = b;
+    return PTG_OK;
+  } catch (const std::bad_alloc&) {
+    delete b;
+    return PTG_ERR_NOMEM;
+  } catch (...) {
+    delete b;
+    return PTG_ERR_INVALID;
+  }
 }
 
 extern "C" const ptg_geometry* ptg_geombuf_view(const ptg_geombuf* buf) {

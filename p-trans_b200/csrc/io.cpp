@@ -342,16 +342,25 @@ struct ptg_anphonbuf {
 extern "C" {
 
 int ptg_mcp_load(const char* path, ptg_mcpbuf** out) {
-  if (!path || !out) return PTG_ERR_INVALID;
-  *out = nullptr;
-  Lines L;
-  if (!read_file(path, &L)) return PTG_ERR_IO;
-  ptg_mcpbuf* b = new (std::nothrow) ptg_mcpbuf();
-  if (!b) return PTG_ERR_NOMEM;
-  int st = parse_mcp(L, b);
-  if (st != PTG_OK) { delete b; return st; }
-  *out = b;
-  return PTG_OK;
+  ptg_mcpbuf* b = nullptr;
+  try {
+    if (!path || !out) return PTG_ERR_INVALID;
+    *out = nullptr;
+    Lines L;
+    if (!read_file(path, &L)) return PTG_ERR_IO;
+    b = ptg::alloc_should_fail() ? nullptr : new (std::nothrow) ptg_mcpbuf();
+    if (!b) return PTG_ERR_NOMEM;
+    int st = parse_mcp(L, b);
+    if (st != PTG_OK) { delete b; return st; }
+    *out = b;
+    return PTG_OK;
+  } catch (const std::bad_alloc&) {
+    delete b;
+    return PTG_ERR_NOMEM;
+  } catch (...) {
+    delete b;
+    return PTG_ERR_INVALID;
+  }
 }
 
 const ptg_model* ptg_mcpbuf_model(const ptg_mcpbuf* b) { return b ? &b->m : nullptr; }
@@ -377,53 +386,66 @@ int ptg_mcpbuf_info(const ptg_mcpbuf* b, int64_t* np, int32_t* nangle, int32_t* 
 void ptg_mcpbuf_free(ptg_mcpbuf* b) { delete b; }
 
 int ptg_anphon_load(const char* path, ptg_anphonbuf** out) {
-  if (!path || !out) return PTG_ERR_INVALID;
-  *out = nullptr;
-  Lines L;
-  if (!read_file(path, &L) || L.l.size() < 7) return PTG_ERR_IO;
-  auto value_after = [](const std::string& line, size_t nwords, double* v) {
-    std::vector<std::string> t = tokens(line);
-    return t.size() > nwords && to_double(t[nwords], v);
-  };
-  double rtemp, vol, nk, nb;
-  if (!value_after(L.l[2], 5, &rtemp) || !value_after(L.l[3], 3, &vol) ||
-      !value_after(L.l[4], 4, &nk) || !value_after(L.l[5], 4, &nb) || nk < 1 || nb < 1)
-    return PTG_ERR_IO;
-  ptg_anphonbuf* b = new (std::nothrow) ptg_anphonbuf();
-  if (!b) return PTG_ERR_NOMEM;
-  const int ik_n = (int)nk, ib_n = (int)nb;
-  const size_t n = (size_t)ik_n * ib_n;
-  b->omega.resize(n); b->tau.resize(n); b->vel.resize(n); b->mfp.resize(n); b->weight.resize(n);
-  size_t li = 7;
-  const double conv = 0.03 * (3.14159265358979323846 * 2.0) * 1.0e12;
-  for (int ik = 0; ik < ik_n; ++ik) {
-    for (int ib = 0; ib < ib_n; ++ib, ++li) {
-      if (li >= L.l.size()) { delete b; return PTG_ERR_IO; }
-      std::vector<std::string> t = tokens(L.l[li]);
-      double v[5];
-      if (t.size() < 7) { delete b; return PTG_ERR_IO; }
-      for (int k = 0; k < 5; ++k)
-        if (!to_double(t[2 + k], &v[k])) { delete b; return PTG_ERR_IO; }
-      const size_t m = (size_t)ib + (size_t)ib_n * ik;
-      b->omega[m] = v[0] * conv;
-      b->tau[m] = v[1];
-      b->vel[m] = v[2];
-      b->mfp[m] = v[3];
-      b->weight[m] = v[4];
+  ptg_anphonbuf* b = nullptr;
+  try {
+    if (!path || !out) return PTG_ERR_INVALID;
+    *out = nullptr;
+    Lines L;
+    if (!read_file(path, &L) || L.l.size() < 7) return PTG_ERR_IO;
+    auto value_after = [](const std::string& line, size_t nwords, double* v) {
+      std::vector<std::string> t = tokens(line);
+      return t.size() > nwords && to_double(t[nwords], v);
+    };
+    double rtemp, vol, nk, nb;
+    if (!value_after(L.l[2], 5, &rtemp) || !value_after(L.l[3], 3, &vol) ||
+        !value_after(L.l[4], 4, &nk) || !value_after(L.l[5], 4, &nb) || nk < 1 || nb < 1)
+      return PTG_ERR_IO;
+    /* one record per (k-point, branch) follows: counts the file cannot hold
+       are malformed, not an allocation to attempt */
+    if (!(nk <= 2147483647.0) || !(nb <= 2147483647.0) || nk * nb > (double)L.l.size())
+      return PTG_ERR_IO;
+    b = ptg::alloc_should_fail() ? nullptr : new (std::nothrow) ptg_anphonbuf();
+    if (!b) return PTG_ERR_NOMEM;
+    const int ik_n = (int)nk, ib_n = (int)nb;
+    const size_t n = (size_t)ik_n * ib_n;
+    b->omega.resize(n); b->tau.resize(n); b->vel.resize(n); b->mfp.resize(n); b->weight.resize(n);
+    size_t li = 7;
+    const double conv = 0.03 * (3.14159265358979323846 * 2.0) * 1.0e12;
+    for (int ik = 0; ik < ik_n; ++ik) {
+      for (int ib = 0; ib < ib_n; ++ib, ++li) {
+        if (li >= L.l.size()) { delete b; return PTG_ERR_IO; }
+        std::vector<std::string> t = tokens(L.l[li]);
+        double v[5];
+        if (t.size() < 7) { delete b; return PTG_ERR_IO; }
+        for (int k = 0; k < 5; ++k)
+          if (!to_double(t[2 + k], &v[k])) { delete b; return PTG_ERR_IO; }
+        const size_t m = (size_t)ib + (size_t)ib_n * ik;
+        b->omega[m] = v[0] * conv;
+        b->tau[m] = v[1];
+        b->vel[m] = v[2];
+        b->mfp[m] = v[3];
+        b->weight[m] = v[4];
+      }
     }
+    ptg_spectrum& s = b->s;
+    s.nbranch = ib_n;
+    s.nkpoint = ik_n;
+    s.rtemp = rtemp;
+    s.vol = vol;
+    s.omega = b->omega.data();
+    s.tau = b->tau.data();
+    s.vel = b->vel.data();
+    s.mfp = b->mfp.data();
+    s.weight = b->weight.data();
+    *out = b;
+    return PTG_OK;
+  } catch (const std::bad_alloc&) {
+    delete b;
+    return PTG_ERR_NOMEM;
+  } catch (...) {
+    delete b;
+    return PTG_ERR_INVALID;
   }
-  ptg_spectrum& s = b->s;
-  s.nbranch = ib_n;
-  s.nkpoint = ik_n;
-  s.rtemp = rtemp;
-  s.vol = vol;
-  s.omega = b->omega.data();
-  s.tau = b->tau.data();
-  s.vel = b->vel.data();
-  s.mfp = b->mfp.data();
-  s.weight = b->weight.data();
-  *out = b;
-  return PTG_OK;
 }
 
 const ptg_spectrum* ptg_anphonbuf_spectrum(const ptg_anphonbuf* b) { return b ? &b->s : nullptr; }

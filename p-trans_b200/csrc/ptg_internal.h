@@ -12,8 +12,15 @@
 #include "../../include/ptrans_gpu.h"
 
 #include <nvtx3/nvToolsExt.h>
+#include <new>
 
 namespace ptg {
+
+/* Allocation-failure injection (ptg_debug_fail_allocations): true when the
+   allocation about to be made must fail; alloc_check() throws
+   std::bad_alloc then. */
+bool alloc_should_fail();
+void alloc_check();
 
 /* An NVTX range over a scope: the host-side phases of each entry point
    (transport launches, reductions, adjoint passes) show by name in Nsight

@@ -56,50 +56,56 @@ int time_once(ptg_handle* h, const ptg_run* run, int reps, double* ms) {
 
 extern "C" int ptg_autotune(ptg_handle* h, const ptg_run* run, int32_t reps, ptg_options* best,
                             double* best_ms) {
-  if (!h || !run || !best) return PTG_ERR_INVALID;
-  if (reps < 1) reps = 1;
-  ptg_options cur;
-  int st = ptg_get_options(h, &cur);
-  if (st != PTG_OK) return st;
-  const ptg_options start = cur;
-  const bool has_bvh = ptg::handle_has_bvh(h);
-  std::vector<Param> params;
-  if (has_bvh) params.push_back({&ptg_options::bvh_leaf, nullptr, {1, 2, 4, 8, 16}});
-  params.push_back({&ptg_options::block_size, nullptr, {128, 256}});
-  params.push_back({&ptg_options::blocks_per_sm, nullptr, {1, 2}});
-  params.push_back({&ptg_options::coop_lanes, nullptr, {4, 8, 16, 32}});
-  params.push_back({&ptg_options::fast_steps, nullptr, {4, 8, 16}});
-  params.push_back({&ptg_options::regen_threshold, nullptr, {1, 2, 4, 8}});
-  params.push_back({nullptr, &ptg_options::chunk, {32, 64, 128}});
-
-  double cur_ms = 0.0;
-  st = time_once(h, run, reps, &cur_ms);
-  if (st != PTG_OK) { ptg_set_options(h, &start); return st; }
-  for (const Param& p : params) {
-    ptg_options keep = cur;
-    double keep_ms = cur_ms;
-    for (long long v : p.values) {
-      ptg_options trial = cur;
-      if (p.i32) {
-        if (trial.*(p.i32) == (int32_t)v) continue;
-        trial.*(p.i32) = (int32_t)v;
-      } else {
-        if (trial.*(p.i64) == (int64_t)v) continue;
-        trial.*(p.i64) = (int64_t)v;
-      }
-      st = ptg_set_options(h, &trial);
-      if (st != PTG_OK) { ptg_set_options(h, &start); return st; }
-      double ms = 0.0;
-      st = time_once(h, run, reps, &ms);
-      if (st != PTG_OK) { ptg_set_options(h, &start); return st; }
-      if (ms < keep_ms * 0.99) { keep = trial; keep_ms = ms; }
-    }
-    cur = keep;
-    cur_ms = keep_ms;
-    st = ptg_set_options(h, &cur);
+  try {
+    if (!h || !run || !best) return PTG_ERR_INVALID;
+    if (reps < 1) reps = 1;
+    ptg_options cur;
+    int st = ptg_get_options(h, &cur);
+    if (st != PTG_OK) return st;
+    const ptg_options start = cur;
+    const bool has_bvh = ptg::handle_has_bvh(h);
+    std::vector<Param> params;
+    if (has_bvh) params.push_back({&ptg_options::bvh_leaf, nullptr, {1, 2, 4, 8, 16}});
+    params.push_back({&ptg_options::block_size, nullptr, {128, 256}});
+    params.push_back({&ptg_options::blocks_per_sm, nullptr, {1, 2}});
+    params.push_back({&ptg_options::coop_lanes, nullptr, {4, 8, 16, 32}});
+    params.push_back({&ptg_options::fast_steps, nullptr, {4, 8, 16}});
+    params.push_back({&ptg_options::regen_threshold, nullptr, {1, 2, 4, 8}});
+    params.push_back({nullptr, &ptg_options::chunk, {32, 64, 128}});
+  
+    double cur_ms = 0.0;
+    st = time_once(h, run, reps, &cur_ms);
     if (st != PTG_OK) { ptg_set_options(h, &start); return st; }
+    for (const Param& p : params) {
+      ptg_options keep = cur;
+      double keep_ms = cur_ms;
+      for (long long v : p.values) {
+        ptg_options trial = cur;
+        if (p.i32) {
+          if (trial.*(p.i32) == (int32_t)v) continue;
+          trial.*(p.i32) = (int32_t)v;
+        } else {
+          if (trial.*(p.i64) == (int64_t)v) continue;
+          trial.*(p.i64) = (int64_t)v;
+        }
+        st = ptg_set_options(h, &trial);
+        if (st != PTG_OK) { ptg_set_options(h, &start); return st; }
+        double ms = 0.0;
+        st = time_once(h, run, reps, &ms);
+        if (st != PTG_OK) { ptg_set_options(h, &start); return st; }
+        if (ms < keep_ms * 0.99) { keep = trial; keep_ms = ms; }
+      }
+      cur = keep;
+      cur_ms = keep_ms;
+      st = ptg_set_options(h, &cur);
+      if (st != PTG_OK) { ptg_set_options(h, &start); return st; }
+    }
+    *best = cur;
+    if (best_ms) *best_ms = cur_ms;
+    return PTG_OK;
+  } catch (const std::bad_alloc&) {
+    return PTG_ERR_NOMEM;
+  } catch (...) {
+    return PTG_ERR_INVALID;
   }
-  *best = cur;
-  if (best_ms) *best_ms = cur_ms;
-  return PTG_OK;
 }

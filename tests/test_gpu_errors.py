@@ -51,3 +51,28 @@ def test_reserved_option_and_bad_block_size_are_rejected():
             assert e.value.status == A.PTG_ERR_INVALID
         t, _ = h.transmission(20.0, 5, 50, seed=1, precision=A.PREC_FP32)
         assert t.shape == (1, spec.nmode, 5)
+
+
+def test_injected_device_allocation_failures_return_nomem():
+    """ptg_debug_fail_allocations makes the library's device-buffer requests
+    fail on the host side (cudaMalloc is never called): handle creation and a
+    first kappa run (whose tallies and tables are allocated then) return
+    PTG_ERR_NOMEM, and after injection is off the same handle computes the
+    same result as a fresh one."""
+    gb, spec = _film()
+    run = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=7, np_=200, seed=4, precision=A.PREC_FP32)
+    with A.Handle(gb.view, spec) as ref:
+        want = ref.kappa(run, want_counts=True)
+    for after in (0, 2):
+        with A.fail_allocations(after):
+            with pytest.raises(A.PtgError) as e:
+                A.Handle(gb.view, spec)
+        assert e.value.status == A.PTG_ERR_NOMEM
+    with A.Handle(gb.view, spec) as h:
+        with A.fail_allocations(0):
+            with pytest.raises(A.PtgError) as e:
+                h.kappa(run)
+            assert e.value.status == A.PTG_ERR_NOMEM
+        got = h.kappa(run, want_counts=True)
+    np.testing.assert_array_equal(got["counts"], want["counts"])
+    assert got["kappa"] == want["kappa"]
