@@ -432,6 +432,93 @@ def run_structure(args):
     return 0
 
 
+def run_c1(args):
+    """C1: the plain method on a square nanowire 100 x 100 x 1000 nm (x
+    transport), fully diffuse side walls, 2000-mode spectrum, 10^5 samples
+    (5 particles per (mode, angle) task), FP64 throughout, seed 0.  Timed
+    three ways on the same workload: the plain FP64 GPU kernel (the
+    configuration's precision), the persistent FP32 kernel, and the CPU
+    oracle (OpenMP, all host threads, in a process without torch), with the
+    FP64 GPU counts checked against the oracle's exactly."""
+    import subprocess
+    import torch
+    torch.cuda.set_device(0)
+    pkg = load_pkg()
+    A, synth = pkg.abi, pkg.synth
+    model = synth.nanowire(length=1000.0, width=100.0, height=100.0, p_side=0.0)
+    spec = synth.spectrum(2000, seed=0)
+    gb = A.GeomBuf(model)
+    bins = dict(temperature=300.0, nbins=64, bin_omega=(0.0, 15.0 * 2 * math.pi * 1e12))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda:0")
+    res = {}
+    with A.Handle(gb.view, spec) as h:
+        for name, prec in (("fp64", A.PREC_FP64), ("fp32", A.PREC_FP32)):
+            run = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=11, np_=5, seed=0, precision=prec, **bins)
+            for _ in range(args.warmup):
+                h.kappa(run)
+            ms = fl = 0.0
+            for _ in range(args.steps):
+                flush.zero_()
+                torch.cuda.synchronize()
+                out = h.kappa(run, want_counts=True)
+                st = h.stats()
+                ms += st["kernel_ms"] + st["reduce_ms"]
+                fl += st["flights"]
+            res[name] = {"value": fl / (ms * 1e-3), "ms_per_step": ms / args.steps, "kappa": out["kappa"],
+                         "kappa_stderr": out["kappa_stderr"], "counts": out["counts"],
+                         "flights": fl / args.steps}
+    threads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    p = subprocess.run([sys.executable, os.path.abspath(__file__), "--c1-oracle"], capture_output=True, text=True,
+                       env=env, timeout=1800)
+    if p.returncode != 0:
+        raise RuntimeError(p.stderr[-2000:])
+    orc = json.loads(p.stdout.strip().splitlines()[-1])
+    counts_equal = orc["counts_sha"] == _sha(res["fp64"]["counts"])
+    line = {"metric": "phonon free-flights/s, C1 square nanowire (plain method, FP64)",
+            "value": res["fp64"]["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": res["fp64"]["ms_per_step"], "higher_is_better": True,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "nanowire 100x100x1000 nm, diffuse side walls, 2000-mode spectrum, "
+                                   "64 bins, 5 particles per (mode, angle): 1e5 samples, seed 0",
+                       "l2": "256 MiB written between timed steps"},
+            "flights_per_step": res["fp64"]["flights"], "kappa": res["fp64"]["kappa"],
+            "kappa_stderr": res["fp64"]["kappa_stderr"],
+            "persistent_fp32": {"value": res["fp32"]["value"], "unit": UNIT,
+                                "ms_per_step": res["fp32"]["ms_per_step"], "kappa": res["fp32"]["kappa"],
+                                "kappa_stderr": res["fp32"]["kappa_stderr"]},
+            "cpu_oracle": {"value": orc["value"], "unit": UNIT, "cores": orc["cores"], "seconds": orc["seconds"],
+                           "kappa": orc["kappa"], "sample": "the whole C1 workload"},
+            "fp64_counts_equal_oracle": counts_equal}
+    print(json.dumps(line))
+    return 0
+
+
+def _sha(a):
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(a, dtype=np.uint64).tobytes()).hexdigest()
+
+
+def c1_oracle():
+    """The CPU oracle on the whole C1 workload (bench.py --c1-oracle, a
+    process without torch): rate, kappa and a digest of the counts."""
+    pkg = load_pkg()
+    A, synth = pkg.abi, pkg.synth
+    if ROOT not in sys.path:
+        sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    model = synth.nanowire(length=1000.0, width=100.0, height=100.0, p_side=0.0)
+    spec = synth.spectrum(2000, seed=0)
+    o = O.Oracle(model=model, spectrum=spec)
+    run = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=11, np_=5, seed=0, precision=A.PREC_FP64,
+                     temperature=300.0, nbins=64, bin_omega=(0.0, 15.0 * 2 * math.pi * 1e12))
+    cnt, _, r = o.counts(run)
+    k = o.kappa(run, cnt)
+    print(json.dumps({"value": r["flights"] / r["seconds"], "cores": int(r["threads"]), "seconds": r["seconds"],
+                      "kappa": k["kappa"], "counts_sha": _sha(cnt)}))
+    return 0
+
+
 def run_c3(args):
     """C3: 64 spheres (r ~ U(20, 80) nm) and 16 capped cylinders of random
     axis (r = 30 nm, length ~ U(100, 400) nm) as voids in a 1000^3 nm box,
@@ -503,7 +590,8 @@ def main():
     ap.add_argument("--mfp-lo", type=float, default=1e-9,
                     help="smallest bulk MFP of the spectrum [m]; 1e-9 is the metric's spectrum "
                          "(larger values remove the diffusive tail, for throughput diagnostics)")
-    ap.add_argument("--workload", default="thinfilm", choices=["thinfilm", "c3", "c4", "c5", "voronoi", "mesh"],
+    ap.add_argument("--workload", default="thinfilm",
+                    choices=["thinfilm", "c1", "c3", "c4", "c5", "voronoi", "mesh"],
                     help="thinfilm: the metric's configuration; c3: spheres + capped cylinders with "
                          "the adjoint; c5: 256-film batched screening; c4: the Voronoi polycrystal as a "
                          "43k-triangle mesh with T=0.5 boundaries; voronoi / mesh: its polygon form and a "
@@ -511,15 +599,20 @@ def main():
     ap.add_argument("--fp64-subset", type=int, default=16,
                     help="c5: films timed one by one with the plain FP64 kernel")
     ap.add_argument("--cpu-leg", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--c1-oracle", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--cpu-target-s", type=float, default=20.0,
                     help="seconds of CPU work the cpu_baseline leg is sized to")
     args = ap.parse_args()
     if args.cpu_leg:
         return cpu_leg(args)
+    if args.c1_oracle:
+        return c1_oracle()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "c5":
         return run_c5(args)
+    if args.workload == "c1":
+        return run_c1(args)
     if args.workload in ("voronoi", "mesh", "c4"):
         return run_structure(args)
     if args.workload == "c3":

@@ -1042,10 +1042,22 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
               const float* const drow = frow + kRowStride * (cc + 1);
               float* const qrow = frow + kRowStride * (cc + 4);
               float a = cc == 0 ? cpx : (cc == 1 ? cpy : cpz);
+              /* the rows' loads run two blocks ahead of the chain: a block's
+                 loads are issued before the previous block's store, which
+                 the compiler may not move them across */
+              float4 fa = *reinterpret_cast<const float4*>(frow);
+              float4 da = *reinterpret_cast<const float4*>(drow);
+              float4 fb = *reinterpret_cast<const float4*>(frow + 4);
+              float4 db = *reinterpret_cast<const float4*>(drow + 4);
 #pragma unroll
               for (int b = 0; b < 32; b += 4) {
-                const float4 f = *reinterpret_cast<const float4*>(frow + b);
-                const float4 d = *reinterpret_cast<const float4*>(drow + b);
+                const float4 f = fa, d = da;
+                fa = fb;
+                da = db;
+                if (b + 8 < 32) {
+                  fb = *reinterpret_cast<const float4*>(frow + b + 8);
+                  db = *reinterpret_cast<const float4*>(drow + b + 8);
+                }
                 float4 q;
                 a = fmaf(f.x, d.x, a);
                 q.x = a;
