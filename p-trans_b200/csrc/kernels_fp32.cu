@@ -1004,9 +1004,14 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           uint4 sR = make_uint4(0u, 0u, 0u, 0u);
           float stb = 0.0f;
           int ssb = -1;
+          /* the blocks of the next round are drawn while this one runs,
+             assuming it advances all 32 flights (counters alone fix them);
+             a round that advances fewer draws them again */
+          uint4 Rnext = philox10(cfl + 1u + (uint32_t)lane, c1, cslo, cshi, key);
           for (int round = 0; round < max_rounds; ++round) {
             ++crounds;
-            const uint4 R = philox10(cfl + 1u + (uint32_t)lane, c1, cslo, cshi, key);
+            const uint4 R = Rnext;
+            Rnext = philox10(cfl + 33u + (uint32_t)lane, c1, cslo, cshi, key);
             /* direction and free path after a p-p event ending flight `lane` */
             const float ct = fmaf(u23f(R.x), 2.0f, -1.0f);
             const float st = sqrt_approx(fmaxf(0.0f, fmaf(-ct, ct, 1.0f)));
@@ -1143,6 +1148,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
               cdz = __shfl_sync(FULL, nz, 31); cfp = __shfl_sync(FULL, nf, 31);
             }
             cfl += (uint32_t)j;
+            if (j != 32) Rnext = philox10(cfl + 1u + (uint32_t)lane, c1, cslo, cshi, key);
             /* a new ball where the walk left the old one */
             if (!__shfl_sync(FULL, in_ball, j - 1) && r.fast_steps > 0) {
               float dg;

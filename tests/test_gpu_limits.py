@@ -1,0 +1,51 @@
+"""Analytic limits on the GPU kernels (the formulas and their derivation are
+in tests/limits.py): the Fuchs-Sondheimer in-plane MFP of a fully diffuse
+film and the Casimir MFP of a ballistic wire with fully diffuse walls, from
+the reference's effective MFP Lambda_eff(L) = 0.75 L <T> (src/RTMCphon.f90:
+2418-2451) with diffuse walls re-emitting by Lambert's law (:2332-2380).
+These pin the persistent FP32 kernel and the plain FP64 kernel to numbers
+that do not come from the oracle."""
+import math
+
+import numpy as np
+import pytest
+
+import limits
+from ptrans_b200 import abi as A
+from ptrans_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _wire(L, w, h, py, pz):
+    m = synth.nanowire(length=L, width=w, height=h, p_side=0.0)
+    m.cellspec = (1.0, 1.0, py, py, pz, pz)
+    return m
+
+
+def _flux_T(model, lam, np_, precision, seed=7, nangle=11):
+    gb = A.GeomBuf(model)
+    spec = synth.spectrum(1, seed=0)
+    with A.Handle(gb.view, spec) as h:
+        t, _ = h.transmission(lam, nangle, np_, seed=seed, precision=precision)
+        st = h.stats()
+    assert st["lost"] == 0
+    return limits.flux_transmission(t[0, 0, :], np_, nangle)
+
+
+@pytest.mark.parametrize("kn,precision,np_", [(0.5, A.PREC_FP32, 400000), (1.0, A.PREC_FP32, 400000),
+                                              (2.0, A.PREC_FP32, 400000), (1.0, A.PREC_FP64, 60000)])
+def test_fuchs_sondheimer_film(kn, precision, np_):
+    """In-plane MFP of a film 40 nm thick with fully diffuse walls (specular
+    side walls: an infinite film) at Knudsen number kn, two-length estimate
+    at L = 10 and 20 max(Lambda, d), against the Fuchs-Sondheimer integral:
+    within 3 standard errors plus 0.5% (what is left of the bath term at
+    these lengths, and the Simpson bias at Nangle = 11, 5.5e-5)."""
+    d = 40.0
+    lam = kn * d
+    L1, L2 = 10 * max(lam, d), 20 * max(lam, d)
+    T1, v1 = _flux_T(_wire(L1, 40.0, d, 1.0, 0.0), lam, np_, precision)
+    T2, v2 = _flux_T(_wire(L2, 40.0, d, 1.0, 0.0), lam, np_, precision, seed=8)
+    est, se = limits.two_length_mfp(L1, T1, v1, L2, T2, v2)
+    want = lam * limits.fuchs_sondheimer(kn)
+    assert abs(est - want) < 3 * se + 0.005 * want, (est, want, se)
