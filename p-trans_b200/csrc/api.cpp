@@ -45,6 +45,30 @@ struct DevBuf {
   T* as() const { return static_cast<T*>(p); }
 };
 
+/* Pinned host staging for a call's tables: copied to the device
+   asynchronously, reused once the copy recorded on `done` has finished. */
+struct PinBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= cap) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    if (ptg::alloc_should_fail()) return cudaErrorMemoryAllocation;
+    cudaError_t e = cudaMallocHost(&p, bytes);
+    if (e == cudaSuccess) cap = bytes;
+    return e;
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+  }
+  template <class T>
+  T* as() const { return static_cast<T*>(p); }
+};
+
 #define CU(x)                                                                \
   do {                                                                       \
     cudaError_t e_ = (x);                                                    \
@@ -76,7 +100,12 @@ struct ptg_handle {
   ptg::GeoF32 g32;
   size_t blob_bytes = 0;
   /* work buffers */
-  DevBuf task, chunk, counts, lost, stats, queue;
+  DevBuf task, chunk, counts, lost, stats, queue, order;
+  /* pinned staging of the FP32 task table and queue order; h2d_done marks
+     the end of their last copy */
+  PinBuf pin_task, pin_order;
+  cudaEvent_t h2d_done = nullptr;
+  bool h2d_pending = false;
   /* FP32 tail phase: phonons the drain phase hands over */
   DevBuf tail;
   /* reduction */
@@ -94,9 +123,13 @@ struct ptg_handle {
     DevBuf* all[] = {&blob, &task, &chunk, &counts, &lost, &stats, &queue, &red_coef, &red_K,
                      &red_W, &red_mfp, &red_bin, &red_grid, &red_tc, &red_kv, &red_bw, &red_bv,
                      &red_emfp, &red_trans, &red_result, &adj_list, &adj_w, &adj_acc,
-                     &tr_off, &tr_npos, &tr_end, &tr_pos, &tail};
+                     &tr_off, &tr_npos, &tr_end, &tr_pos, &tail, &order};
     for (DevBuf* b : all) b->release();
+    if (stream) cudaStreamSynchronize(stream);
+    pin_task.release();
+    pin_order.release();
     for (cudaEvent_t e : ev) if (e) cudaEventDestroy(e);
+    if (h2d_done) cudaEventDestroy(h2d_done);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -416,6 +449,9 @@ struct Transport {
   int32_t stream = 0;
   int32_t precision = PTG_PREC_FP32;
   const std::vector<ptg::TaskHost>* tasks = nullptr;
+  /* tasks whose MFP can differ: task t has the MFP of task t % npair (the
+     (mode, grid point) pairs of the first angle; 0: every task) */
+  int64_t npair = 0;
   /* persistent kernel mode and the adjoint buffers */
   int mode = ptg::MODE_FORWARD;
   unsigned long long* tlist = nullptr;
@@ -488,44 +524,62 @@ int run_transport(ptg_handle* h, const Transport& T) {
     h->last.launches = 1;
     h->fp32_split = false;
   } else {
-    std::vector<float4> t32(ntask);
-    std::vector<int64_t> order;
-    order.reserve(ntask);
+    /* the FP32 task table and the queue order (longest expected
+       trajectories first: ascending MFP) are written to pinned staging and
+       copied without a host wait; the chunk table (task, first local
+       particle, count) is expanded from the order on the device.  The MFP
+       depends on (mode, grid point) only, so those pairs are sorted and
+       every angle's task follows its pair; equal MFPs keep index order. */
+    if (h->h2d_pending) {
+      CU(cudaEventSynchronize(h->h2d_done));
+      h->h2d_pending = false;
+    }
+    CU(h->pin_task.ensure(sizeof(float4) * (ntask > 0 ? ntask : 1)));
+    CU(h->pin_order.ensure(sizeof(int) * (ntask > 0 ? ntask : 1)));
+    float4* t32 = h->pin_task.as<float4>();
+    int* order = h->pin_order.as<int>();
+    const int64_t npair = T.npair > 0 ? std::min<int64_t>(ntask, T.npair) : ntask;
+    std::vector<int64_t> pairs;
+    pairs.reserve(npair);
     for (int64_t i = 0; i < ntask; ++i) {
       const ptg::TaskHost& th = (*T.tasks)[i];
       float lam = th.lambda == 1.0e10 ? INFINITY : (float)th.lambda;
       if (!(th.lambda > 0.0)) lam = 0.0f;
       t32[i] = make_float4(lam, (float)th.cth, (float)th.sth,
                            (float)(th.omega / h->spec.max_omega));
-      if (th.lambda > 0.0) order.push_back(i);
+      if (i < npair && th.lambda > 0.0) pairs.push_back(i);
     }
-    /* longest expected trajectories first: small mean free paths first */
-    std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
+    std::stable_sort(pairs.begin(), pairs.end(), [&](int64_t a, int64_t b) {
       return (*T.tasks)[a].lambda < (*T.tasks)[b].lambda;
     });
-    const int64_t csz = h->opt.chunk > 0 ? h->opt.chunk : 64;
-    std::vector<int4> chunks;
-    for (int64_t t : order) {
-      for (int64_t j = 0; j < T.np_local; j += csz) {
-        const int64_t cnt = std::min(csz, T.np_local - j);
-        chunks.push_back(make_int4((int)t, (int)j, (int)cnt, 0));
+    int64_t norder = 0;
+    const int64_t nrep = npair > 0 ? (ntask + npair - 1) / npair : 0;
+    for (int64_t pi : pairs)
+      for (int64_t k = 0; k < nrep; ++k) {
+        const int64_t t = pi + k * npair;
+        if (t < ntask) order[norder++] = (int)t;
       }
-    }
-    if (chunks.size() > 2147483647ull) { h->last_error = "too many chunks"; return PTG_ERR_INVALID; }
+    const int64_t csz = h->opt.chunk > 0 ? h->opt.chunk : 64;
+    const int64_t per_task = T.np_local > 0 ? (T.np_local + csz - 1) / csz : 0;
+    const int64_t nchunk = norder * per_task;
+    if (nchunk > 2147483647LL) { h->last_error = "too many chunks"; return PTG_ERR_INVALID; }
     CU(h->task.ensure(sizeof(float4) * ntask));
-    CU(cudaMemcpyAsync(h->task.p, t32.data(), sizeof(float4) * ntask, cudaMemcpyHostToDevice,
-                       h->stream));
-    CU(h->chunk.ensure(sizeof(int4) * (chunks.size() + 1)));
-    if (!chunks.empty())
-      CU(cudaMemcpyAsync(h->chunk.p, chunks.data(), sizeof(int4) * chunks.size(),
-                         cudaMemcpyHostToDevice, h->stream));
-    CU(cudaStreamSynchronize(h->stream));  /* t32 and chunks are local buffers */
-    h->last.h2d_bytes += sizeof(float4) * ntask + sizeof(int4) * chunks.size();
+    CU(h->order.ensure(sizeof(int) * (norder > 0 ? norder : 1)));
+    CU(h->chunk.ensure(sizeof(int4) * (nchunk + 1)));
+    CU(cudaMemcpyAsync(h->task.p, t32, sizeof(float4) * ntask, cudaMemcpyHostToDevice, h->stream));
+    if (norder > 0)
+      CU(cudaMemcpyAsync(h->order.p, order, sizeof(int) * norder, cudaMemcpyHostToDevice, h->stream));
+    CU(cudaEventRecord(h->h2d_done, h->stream));
+    h->h2d_pending = true;
+    if (nchunk > 0)
+      CU(ptg::launch_expand_chunks(h->order.as<const int>(), (int)norder, (int)per_task, (int)csz,
+                                   (int)T.np_local, h->chunk.as<int4>(), h->stream));
+    h->last.h2d_bytes += sizeof(float4) * ntask + sizeof(int) * norder;
     ptg::RunF32 r;
     memset(&r, 0, sizeof(r));
     r.task = h->task.as<const float4>();
     r.chunk = h->chunk.as<const int4>();
-    r.nchunk = (int32_t)chunks.size();
+    r.nchunk = (int32_t)nchunk;
     r.np = T.np;
     r.rank = T.rank;
     r.nranks = T.nranks;
@@ -595,7 +649,7 @@ int run_transport(ptg_handle* h, const Transport& T) {
     CU(cudaEventRecord(h->ev[1], h->stream));
     h->last.grid = grid;
     h->last.block = block;
-    h->last.launches = work ? (tail ? 2 : 1) : 0;
+    h->last.launches = (work ? (tail ? 2 : 1) : 0) + (r.nchunk > 0 ? 1 : 0);
     h->fp32_split = work;
     h->tail_cap = tail ? r.tail_cap : 0;
   }
@@ -860,6 +914,10 @@ int ptg_create(const ptg_geometry* geom, const ptg_spectrum* spec, const ptg_opt
     }
     for (auto& e : h->ev)
       if (cudaEventCreate(&e) != cudaSuccess) { delete h; return PTG_ERR_CUDA; }
+    if (cudaEventCreateWithFlags(&h->h2d_done, cudaEventDisableTiming) != cudaSuccess) {
+      delete h;
+      return PTG_ERR_CUDA;
+    }
     st = build_geo64(h);
     if (st == PTG_OK) st = build_blob(h);
     if (st != PTG_OK) { delete h; return st; }
@@ -959,6 +1017,7 @@ int ptg_transmission(ptg_handle* h, double mfp_nm, int32_t nangle, int64_t np, i
     T.seed = seed;
     T.precision = precision;
     T.tasks = &tasks;
+    T.npair = h->spec.nmode();
     int st = run_transport(h, T);
     if (st != PTG_OK) return st;
     std::vector<unsigned long long> cnt(ntask);
@@ -1003,6 +1062,7 @@ int ptg_kappa(ptg_handle* h, const ptg_run* run, ptg_kappa_out* out) {
     T.stream = run->stream;
     T.precision = run->precision;
     T.tasks = &tasks;
+    T.npair = h->spec.nmode() * ns;
     int st = run_transport(h, T);
     if (st != PTG_OK) return st;
     /* FP64 reduction on the device */
@@ -1260,6 +1320,7 @@ int ptg_adjoint(ptg_handle* h, const ptg_run* run, ptg_adjoint_out* out) {
     T.stream = run->stream;
     T.precision = PTG_PREC_FP32;
     T.tasks = &tasks;
+    T.npair = h->spec.nmode() * ns;
     T.mode = ptg::MODE_LIST;
     const unsigned long long total = (unsigned long long)ntask * (unsigned long long)T.np_local;
     T.tlist_cap = total < cap ? total : cap;

@@ -571,22 +571,34 @@ void run_tasks(const SpecSoA& s, const ptg_run* r, std::vector<TaskHost>* tasks)
   const int64_t nt = run_ntask(s, r);
   const double half_pi = 3.14159265358979323846 * 0.5;
   const double scale = (r->scatter_scale > 0.0) ? r->scatter_scale : 1.0;
+  /* the angle's cos / sin and the (mode, grid point) MFP, each computed once */
+  std::vector<double> ca(r->nangle), sa(r->nangle), lam((size_t)(nm * ns));
+  for (int ia = 0; ia < r->nangle; ++ia) {
+    const double theta = 0.0 + (double)ia / (double)(r->nangle - 1) * half_pi;
+    ca[ia] = cos(theta);
+    sa[ia] = sin(theta);
+  }
+  for (int64_t sg = 0; sg < ns; ++sg)
+    for (int64_t m = 0; m < nm; ++m) {
+      double l;
+      if (r->kind_mfp == PTG_MFP_MATTHIESSEN) {
+        l = 1.0e10;
+      } else if (r->kind_mfp == PTG_MFP_GRID) {
+        l = r->mfp_grid_nm[sg];   /* grid points are sampling points */
+      } else {
+        const double tau_s = s.tau[m] * 1.0e-12 * (s.rtemp / r->temperature);
+        l = tau_s * s.vel[m] * 1.0e9 / scale;
+      }
+      lam[(size_t)(m + nm * sg)] = l;
+    }
   tasks->resize(nt);
   for (int64_t t = 0; t < nt; ++t) {
     const int64_t m = t % nm, rest = t / nm, sg = rest % ns, ia = rest / ns;
     TaskHost& th = (*tasks)[t];
-    const double theta = 0.0 + (double)ia / (double)(r->nangle - 1) * half_pi;
-    th.cth = cos(theta);
-    th.sth = sin(theta);
+    th.cth = ca[ia];
+    th.sth = sa[ia];
     th.omega = s.omega[m];
-    if (r->kind_mfp == PTG_MFP_MATTHIESSEN) {
-      th.lambda = 1.0e10;
-    } else if (r->kind_mfp == PTG_MFP_GRID) {
-      th.lambda = r->mfp_grid_nm[sg];   /* grid points are sampling points */
-    } else {
-      const double tau_s = s.tau[m] * 1.0e-12 * (s.rtemp / r->temperature);
-      th.lambda = tau_s * s.vel[m] * 1.0e9 / scale;
-    }
+    th.lambda = lam[(size_t)(m + nm * sg)];
   }
 }
 

@@ -207,6 +207,10 @@ cudaError_t launch_persistent_batch(const RunF32& r, int grid, int block, cudaSt
                                     bool bvh, int mode = MODE_FORWARD);
 cudaError_t persistent_batch_occupancy(int block, int* blocks_per_sm, bool bvh,
                                        int mode = MODE_FORWARD);
+/* Fills the chunk table (task, first local particle, count, 0): per_task
+   chunks of csz particles for each task of `order`, in that order. */
+cudaError_t launch_expand_chunks(const int* order, int norder, int per_task, int csz, int np_local,
+                                 int4* chunks, cudaStream_t st);
 /* Violations recorded by the bounds-checked build (PT_CHECK); other builds
    return cudaErrorNotSupported. */
 cudaError_t check_report(long long* count, int* code, int* index, bool reset);

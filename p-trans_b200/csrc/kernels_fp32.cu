@@ -1662,6 +1662,31 @@ cudaError_t launch_tail_fp32(const GeoF32& g, const RunF32& r, int grid, int blo
                    : launch_bvh<false, PH_TAIL>(g, r, grid, block, smem, st, mode);
 }
 
+namespace {
+/* Chunk table of a run: chunk c is particles [j, j + count) of task
+   order[c / per_task], j = (c % per_task) * csz, in the queue's order. */
+__global__ void k_expand_chunks(const int* __restrict__ order, int norder, int per_task, int csz,
+                                int np_local, int4* __restrict__ chunks) {
+  const long long n = (long long)norder * per_task;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(c / per_task);
+    const int j = (int)(c - (long long)k * per_task) * csz;
+    chunks[c] = make_int4(__ldg(order + k), j, min(csz, np_local - j), 0);
+  }
+}
+}  // namespace
+
+cudaError_t launch_expand_chunks(const int* order, int norder, int per_task, int csz, int np_local,
+                                 int4* chunks, cudaStream_t st) {
+  const long long n = (long long)norder * per_task;
+  if (n <= 0) return cudaSuccess;
+  const long long blocks = (n + 255) / 256;
+  k_expand_chunks<<<(unsigned)(blocks < 4096 ? blocks : 4096), 256, 0, st>>>(order, norder, per_task, csz,
+                                                                            np_local, chunks);
+  return cudaGetLastError();
+}
+
 /* Violations recorded by a bounds-checked build (PT_CHECK): count, code of
    the first (1 geometry-blob index out of range, 2 non-finite phonon state)
    and its index; reset = true clears them.  Other builds return
