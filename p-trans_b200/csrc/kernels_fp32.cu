@@ -326,12 +326,15 @@ constexpr int kBvhStack = 32;
 
 /* BVH traversal of a grain (root >= 0): ordered descent, the far child
    pushed with its entry distance and popped only while it can still hold a
-   nearer hit.  Kept out of line so the linear scan that every small grain
-   uses stays compact in the instruction cache. */
+   nearer hit.  Nodes entered beyond tcut (the flight's free path) are
+   skipped as well: a flight only needs every hit up to its free path (a hit
+   there ends it; with none, a p-p event ends it), so the decision, and the
+   trajectory, are those of the full search.  Kept out of line so the linear
+   scan that every small grain uses stays compact in the instruction cache. */
 template <bool EXT, class G_t>
 __device__ __noinline__ void scan_bvh(const G_t& G, int root, float px, float py, float pz,
                                       float dx, float dy, float dz, int last_geom, float eps,
-                                      float zmax, float& tr, int& sb, unsigned& nbox,
+                                      float zmax, float tcut, float& tr, int& sb, unsigned& nbox,
                                       unsigned& nsurf) {
   const float ix = inv_dir(dx), iy = inv_dir(dy), iz = inv_dir(dz);
   int stk[kBvhStack];
@@ -349,8 +352,9 @@ __device__ __noinline__ void scan_bvh(const G_t& G, int root, float px, float py
         test_surface<EXT>(G, G.cand(k), px, py, pz, dx, dy, dz, last_geom, eps, zmax, tr, sb);
     } else {
       nbox += 2u;
-      const float tl = box_entry(G.node(2 * a), G.node(2 * a + 1), px, py, pz, ix, iy, iz, tr, eps);
-      const float tg = box_entry(G.node(2 * a + 2), G.node(2 * a + 3), px, py, pz, ix, iy, iz, tr,
+      const float tm = fminf(tr, tcut);
+      const float tl = box_entry(G.node(2 * a), G.node(2 * a + 1), px, py, pz, ix, iy, iz, tm, eps);
+      const float tg = box_entry(G.node(2 * a + 2), G.node(2 * a + 3), px, py, pz, ix, iy, iz, tm,
                                  eps);
       const bool hl = tl < 3.0e38f, hg = tg < 3.0e38f;
       if (hl && hg) {
@@ -371,7 +375,7 @@ __device__ __noinline__ void scan_bvh(const G_t& G, int root, float px, float py
     bool found = false;
     while (sp > 0) {
       --sp;
-      if (stt[sp] <= tr) {
+      if (stt[sp] <= fminf(tr, tcut)) {
         node = stk[sp];
         found = true;
         break;
@@ -384,11 +388,13 @@ __device__ __noinline__ void scan_bvh(const G_t& G, int root, float px, float py
 /* Nearest surface of a grain: its BVH when it has one (kernels built with
    EXT = true, for structures with a BVH or capped cylinders; the others
    never look for either), else every candidate.  tb
-   (the box-grain exit, >= 0) and sb are updated; tb stays >= 0. */
+   (the box-grain exit, >= 0) and sb are updated; tb stays >= 0.  fp is the
+   flight's free path: a BVH search skips what lies beyond it (a hit farther
+   away cannot end the flight). */
 template <bool EXT, class G_t>
 __device__ __forceinline__ void scan_grain(const G_t& G, int grain, float px, float py, float pz,
                                            float dx, float dy, float dz, int last_geom, float eps,
-                                           float zmax, float& tb, int& sb, unsigned& nbox,
+                                           float zmax, float fp, float& tb, int& sb, unsigned& nbox,
                                            unsigned& nsurf) {
   float tr = tb;
   const int root = EXT ? G.bvh_root(grain) : -1;
@@ -398,7 +404,7 @@ __device__ __forceinline__ void scan_grain(const G_t& G, int grain, float px, fl
     for (int k = kb; k < ke; ++k)
       test_surface<EXT>(G, G.cand(k), px, py, pz, dx, dy, dz, last_geom, eps, zmax, tr, sb);
   } else {
-    scan_bvh<EXT>(G, root, px, py, pz, dx, dy, dz, last_geom, eps, zmax, tr, sb, nbox, nsurf);
+    scan_bvh<EXT>(G, root, px, py, pz, dx, dy, dz, last_geom, eps, zmax, fp, tr, sb, nbox, nsurf);
   }
   tb = fmaxf(tr, 0.0f);
 }
@@ -1103,7 +1109,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
               slab_exit(qx, qy, qz, sdx, sdy, sdz, X, Y, Z, tb, sb);
               if (cgrain > 0 && !in_gball)
                 scan_grain<EXT>(G, cgrain, qx, qy, qz, sdx, sdy, sdz, lane == 0 ? clast : -1, eps,
-                                Z, tb, sb, my_box_tests, my_surf_tests);
+                                Z, sfp, tb, sb, my_box_tests, my_surf_tests);
             }
             const bool brk = !inbox || capd;
             const unsigned sm =
@@ -1286,7 +1292,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           const bool in_gball = fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < gr2 &&
                                 fmaf(sx, sx, fmaf(sy, sy, sz * sz)) < gr2;
           if (grain > 0 && !in_gball)
-            scan_grain<EXT>(G, grain, px, py, pz, dx, dy, dz, last_geom, eps, Z, tb, sb, my_box_tests,
+            scan_grain<EXT>(G, grain, px, py, pz, dx, dy, dz, last_geom, eps, Z, fp, tb, sb, my_box_tests,
                        my_surf_tests);
           go = true;
         }
