@@ -321,6 +321,49 @@ int blob_from_geometry(const GeomSoA& G, int bvh_leaf, std::vector<float4>* out,
       nodes.insert(nodes.end(), gn.begin(), gn.end());
     }
   }
+  if (!nodes.empty()) {
+    /* breadth first over all grains' trees (every root first, then level
+       by level): the front of the node region holds the top levels of
+       every tree, the part staged in shared memory when the whole blob is
+       too large to stage.  Child pairs stay adjacent; a root keeps an
+       unused partner slot. */
+    const int nn = (int)(nodes.size() / 2);
+    auto word = [](const float4& v) { int w; memcpy(&w, &v.w, 4); return w; };
+    std::vector<int> newidx(nn, -1), queue;
+    queue.reserve(nn);
+    int next = 0;
+    for (int g = 1; g < ngt; ++g)
+      if (root[g] >= 0) {
+        newidx[root[g]] = next;
+        next += 2;
+        queue.push_back(root[g]);
+      }
+    for (size_t qi = 0; qi < queue.size(); ++qi) {
+      const int o = queue[qi];
+      if (word(nodes[2 * (size_t)o + 1]) != 0) continue;  /* leaf */
+      const int a = word(nodes[2 * (size_t)o]);
+      newidx[a] = next;
+      newidx[a + 1] = next + 1;
+      next += 2;
+      queue.push_back(a);
+      queue.push_back(a + 1);
+    }
+    std::vector<float4> bfs(2 * (size_t)next, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+    for (int o = 0; o < nn; ++o) {
+      if (newidx[o] < 0) continue;
+      float4 a = nodes[2 * (size_t)o];
+      const float4 b = nodes[2 * (size_t)o + 1];
+      if (word(b) == 0) {
+        const int na = newidx[word(a)];
+        memcpy(&a.w, &na, 4);
+      }
+      bfs[2 * (size_t)newidx[o]] = a;
+      bfs[2 * (size_t)newidx[o] + 1] = b;
+    }
+    for (int g = 1; g < ngt; ++g)
+      if (root[g] >= 0) root[g] = newidx[root[g]];
+    nodes.swap(bfs);
+  }
   std::vector<float4> start;
   for (int g = 1; g <= G.ngrain; ++g) {
     if (!G.grain_incident[g]) continue;
@@ -403,6 +446,9 @@ int build_blob(ptg_handle* h) {
   g32.nmaterial = G.nmaterial;
   g32.stage_smem = h->blob_bytes <= 96 * 1024 ? 1 : 0;
   g32.has_ext = (L.nbvh > 0 || L.ncap > 0) ? 1 : 0;
+  /* a blob too large to stage keeps the top levels of its BVHs (the front of
+     the breadth-first node region) in shared memory */
+  g32.node_stage = (!g32.stage_smem && L.nbvh > 0) ? std::min(2 * L.nbvh, ptg::kNodeStageUnits) : 0;
   return PTG_OK;
 }
 
@@ -618,9 +664,9 @@ int run_transport(ptg_handle* h, const Transport& T) {
     r.nsurf = h->geom.nsurf();
     const int bs = h->opt.block_size;
     const int block = (bs >= 32 && bs <= 256 && bs % 32 == 0) ? bs : 256;
-    const size_t smem = h->g32.stage_smem ? h->blob_bytes : 0;
+    const size_t smem = ptg::dynamic_smem_bytes(h->g32, h->blob_bytes);
     int bps = 0;
-    CU(ptg::persistent_occupancy(block, smem, &bps, T.mode, h->g32.has_ext != 0));
+    CU(ptg::persistent_occupancy(block, smem, &bps, T.mode, h->g32.has_ext != 0, h->g32.stage_smem != 0));
     if (h->opt.blocks_per_sm > 0 && h->opt.blocks_per_sm < bps) bps = h->opt.blocks_per_sm;
     if (bps < 1) bps = 1;
     const int grid = h->num_sms * bps;
@@ -635,7 +681,7 @@ int run_transport(ptg_handle* h, const Transport& T) {
     int tgrid = 0;
     if (tail) {
       int tbps = 0;
-      CU(ptg::tail_occupancy(block, smem, &tbps, T.mode, h->g32.has_ext != 0));
+      CU(ptg::tail_occupancy(block, smem, &tbps, T.mode, h->g32.has_ext != 0, h->g32.stage_smem != 0));
       tgrid = h->num_sms * (tbps < 1 ? 1 : tbps);
     }
     CU(cudaEventRecord(h->ev[0], h->stream));

@@ -99,6 +99,8 @@ struct GeoF32 {
   int periodic_mask;   /* bit f set: box face f is periodic              */
   int kind_grain, igrain_fill, nmaterial;
   int stage_smem;      /* 1: copy the blob to shared memory (bulk copy)  */
+  int node_stage;      /* else: float4 units of the BVH node region (its  */
+                       /*    top levels, breadth first) copied instead    */
   int has_ext;         /* 1: a BVH or capped cylinders (kernels built for  */
                        /*    them; the others leave both out)             */
 };
@@ -199,7 +201,7 @@ cudaError_t launch_persistent_fp32(const GeoF32& g, const RunF32& r, int grid, i
 cudaError_t launch_tail_fp32(const GeoF32& g, const RunF32& r, int grid, int block, size_t smem,
                              cudaStream_t st, int mode = MODE_FORWARD);
 cudaError_t tail_occupancy(int block, size_t smem, int* blocks_per_sm, int mode = MODE_FORWARD,
-                           bool bvh = false);
+                           bool bvh = false, bool whole = true);
 /* Batched launch over several geometries (geometry in global memory):
    forward, list (ids of transmitted samples as (global task << 32) |
    particle) or adjoint replay of such a list. */
@@ -207,6 +209,16 @@ cudaError_t launch_persistent_batch(const RunF32& r, int grid, int block, cudaSt
                                     bool bvh, int mode = MODE_FORWARD);
 cudaError_t persistent_batch_occupancy(int block, int* blocks_per_sm, bool bvh,
                                        int mode = MODE_FORWARD);
+/* Shared memory for staged BVH nodes when the whole blob is not staged:
+   64 KB, the top ten or so levels of the trees, small enough that two
+   blocks of the tail kernel (28.5 KB of its own) still fit on an SM. */
+constexpr int kNodeStageUnits = 4096;
+/* Dynamic shared memory of a transport launch: the whole blob, or the
+   staged BVH nodes, or none. */
+inline size_t dynamic_smem_bytes(const GeoF32& g, size_t blob_bytes) {
+  if (g.stage_smem) return blob_bytes;
+  return (size_t)g.node_stage * 16u;
+}
 /* Fills the chunk table (task, first local particle, count, 0): per_task
    chunks of csz particles for each task of `order`, in that order. */
 cudaError_t launch_expand_chunks(const int* order, int norder, int per_task, int csz, int np_local,
@@ -216,7 +228,7 @@ cudaError_t launch_expand_chunks(const int* order, int norder, int per_task, int
 cudaError_t check_report(long long* count, int* code, int* index, bool reset);
 /* Residency of the persistent kernel for a block size and shared memory. */
 cudaError_t persistent_occupancy(int block, size_t smem, int* blocks_per_sm,
-                                 int mode = MODE_FORWARD, bool bvh = false);
+                                 int mode = MODE_FORWARD, bool bvh = false, bool whole = true);
 
 /* ---------------- FP64 kappa reduction ---------------------------------- */
 

@@ -90,6 +90,7 @@ template <bool SMEM>
 struct Geo {
   const float4* base;   /* global blob (SMEM = false) */
   BlobLayout lay;
+  int nstage = 0;       /* SMEM = false: BVH node units staged in shared memory */
   __device__ __forceinline__ float4 ld(int i) const {
 #ifdef PT_CHECK
     if ((unsigned)i >= (unsigned)lay.total) { check_fail(1, i); i = 0; }
@@ -116,7 +117,10 @@ struct Geo {
   __device__ __forceinline__ int cand(int k) const { return ldi(lay.cand, k); }
   __device__ __forceinline__ float4 start(int i) const { return ld(lay.start + i); }
   __device__ __forceinline__ int bvh_root(int g) const { return ldi(lay.bvh_root, g); }
-  __device__ __forceinline__ float4 node(int i) const { return ld(lay.bvh_node + i); }
+  __device__ __forceinline__ float4 node(int i) const {
+    if (!SMEM && i < nstage) return sblob[i];  /* a top level, staged */
+    return ld(lay.bvh_node + i);
+  }
 };
 
 /* Square root from the hardware approximation (relative error ~2^-22). */
@@ -138,6 +142,7 @@ __device__ __forceinline__ void sincos2pi(float u, float* s, float* c) {
 struct GeoBatch {
   const float4* base;
   BlobLayout lay;
+  int nstage = 0;       /* unused: a batched launch stages nothing */
   __device__ __forceinline__ float4 ld(int i) const {
 #ifdef PT_CHECK
     if ((unsigned)i >= (unsigned)lay.total) { check_fail(1, i); i = 0; }
@@ -683,6 +688,11 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
     /* on a timeout the block records the error and takes no work: the host
        reports it */
     if (!stage_blob(gp.blob, sblob, gp.lay.total, r.queue + 1, r.stage_test == 0)) return;
+  } else if (EXT && !BATCH && gp.node_stage > 0) {
+    /* a blob too large to stage: its BVHs' top levels only */
+    if (!stage_blob(gp.blob + gp.lay.bvh_node, sblob, gp.node_stage, r.queue + 1, r.stage_test == 0))
+      return;
+    G.nstage = gp.node_stage;
   }
   const int lane = threadIdx.x & 31;
   /* geometry and run scalars: kernel-wide, or per lane in a batched launch */
@@ -1554,22 +1564,26 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
 /* Static shared memory (the adjoint accumulators, the cooperative rows) plus
    the staged blob can pass the 48 KB a launch gets without opting in, so
    every launch with a staged blob opts in to its dynamic size. */
-template <int MODE, bool EXT, int PH>
+template <int MODE, bool EXT, int PH, bool SMEM = true>
 cudaError_t allow_dynamic_smem(size_t smem) {
-  return cudaFuncSetAttribute(k_persistent<true, MODE, false, EXT, PH>,
+  return cudaFuncSetAttribute(k_persistent<SMEM, MODE, false, EXT, PH>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
 template <int MODE, bool EXT, int PH>
-cudaError_t occupancy_mode(int block, size_t smem, int* bps) {
-  if (smem > 0) {
+cudaError_t occupancy_mode(int block, size_t smem, int* bps, bool whole) {
+  if (smem > 0 && whole) {
     cudaError_t e = allow_dynamic_smem<MODE, EXT, PH>(smem);
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
         bps, k_persistent<true, MODE, false, EXT, PH>, block, smem);
   }
+  if (smem > 0) {  /* staged BVH nodes of a blob read from global memory */
+    cudaError_t e = allow_dynamic_smem<MODE, EXT, PH, false>(smem);
+    if (e != cudaSuccess) return e;
+  }
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      bps, k_persistent<false, MODE, false, EXT, PH>, block, 0);
+      bps, k_persistent<false, MODE, false, EXT, PH>, block, smem);
 }
 
 template <int MODE, bool EXT, int PH>
@@ -1580,7 +1594,13 @@ cudaError_t launch_mode(const GeoF32& g, const RunF32& r, int grid, int block, s
     if (e != cudaSuccess) return e;
     k_persistent<true, MODE, false, EXT, PH><<<grid, block, smem, st>>>(g, r);
   } else {
-    k_persistent<false, MODE, false, EXT, PH><<<grid, block, 0, st>>>(g, r);
+    /* the staged BVH nodes (node_stage units) are the only dynamic part */
+    const size_t ns = g.node_stage > 0 ? (size_t)g.node_stage * 16u : 0;
+    if (ns > 0) {
+      cudaError_t e = allow_dynamic_smem<MODE, EXT, PH, false>(ns);
+      if (e != cudaSuccess) return e;
+    }
+    k_persistent<false, MODE, false, EXT, PH><<<grid, block, ns, st>>>(g, r);
   }
   return cudaGetLastError();
 }
@@ -1622,24 +1642,24 @@ cudaError_t launch_persistent_batch(const RunF32& r, int grid, int block, cudaSt
 /* The tail phase exists for the modes with cooperative rounds (forward,
    list, adjoint replay); a trace replay runs every flight on one lane. */
 template <bool EXT, int PH>
-cudaError_t occupancy_bvh(int block, size_t smem, int* bps, int mode) {
-  if (mode == MODE_LIST) return occupancy_mode<MODE_LIST, EXT, PH>(block, smem, bps);
-  if (mode == MODE_ADJOINT) return occupancy_mode<MODE_ADJOINT, EXT, PH>(block, smem, bps);
+cudaError_t occupancy_bvh(int block, size_t smem, int* bps, int mode, bool whole) {
+  if (mode == MODE_LIST) return occupancy_mode<MODE_LIST, EXT, PH>(block, smem, bps, whole);
+  if (mode == MODE_ADJOINT) return occupancy_mode<MODE_ADJOINT, EXT, PH>(block, smem, bps, whole);
   if (mode == MODE_TRACE) {
     if (PH == PH_TAIL) return cudaErrorInvalidValue;
-    return occupancy_mode<MODE_TRACE, EXT, PH_DRAIN>(block, smem, bps);
+    return occupancy_mode<MODE_TRACE, EXT, PH_DRAIN>(block, smem, bps, whole);
   }
-  return occupancy_mode<MODE_FORWARD, EXT, PH>(block, smem, bps);
+  return occupancy_mode<MODE_FORWARD, EXT, PH>(block, smem, bps, whole);
 }
 
-cudaError_t persistent_occupancy(int block, size_t smem, int* bps, int mode, bool bvh) {
-  return bvh ? occupancy_bvh<true, PH_DRAIN>(block, smem, bps, mode)
-             : occupancy_bvh<false, PH_DRAIN>(block, smem, bps, mode);
+cudaError_t persistent_occupancy(int block, size_t smem, int* bps, int mode, bool bvh, bool whole) {
+  return bvh ? occupancy_bvh<true, PH_DRAIN>(block, smem, bps, mode, whole)
+             : occupancy_bvh<false, PH_DRAIN>(block, smem, bps, mode, whole);
 }
 
-cudaError_t tail_occupancy(int block, size_t smem, int* bps, int mode, bool bvh) {
-  return bvh ? occupancy_bvh<true, PH_TAIL>(block, smem, bps, mode)
-             : occupancy_bvh<false, PH_TAIL>(block, smem, bps, mode);
+cudaError_t tail_occupancy(int block, size_t smem, int* bps, int mode, bool bvh, bool whole) {
+  return bvh ? occupancy_bvh<true, PH_TAIL>(block, smem, bps, mode, whole)
+             : occupancy_bvh<false, PH_TAIL>(block, smem, bps, mode, whole);
 }
 
 template <bool EXT, int PH>

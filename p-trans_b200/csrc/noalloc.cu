@@ -182,9 +182,9 @@ extern "C" int ptg_transmission_noalloc(ptg_handle* h, double mfp_nm, int32_t na
      multiple of 32 up to 256, else 256 */
   const int bs = v.opt.block_size;
   const int block = (bs >= 32 && bs <= 256 && bs % 32 == 0) ? bs : 256;
-  const size_t smem = v.g32.stage_smem ? v.blob_bytes : 0;
+  const size_t smem = ptg::dynamic_smem_bytes(v.g32, v.blob_bytes);
   int bps = 0;
-  if (ptg::persistent_occupancy(block, smem, &bps, ptg::MODE_FORWARD, v.g32.has_ext != 0) !=
+  if (ptg::persistent_occupancy(block, smem, &bps, ptg::MODE_FORWARD, v.g32.has_ext != 0, v.g32.stage_smem != 0) !=
       cudaSuccess)
     return PTG_ERR_CUDA;
   if (v.opt.blocks_per_sm > 0 && v.opt.blocks_per_sm < bps) bps = v.opt.blocks_per_sm;
@@ -198,7 +198,7 @@ extern "C" int ptg_transmission_noalloc(ptg_handle* h, double mfp_nm, int32_t na
     r.tail = reinterpret_cast<float4*>(base + kOffTail);
     r.tail_cap = std::min(kMaxTail, grid * block);
     int tbps = 0;
-    if (ptg::tail_occupancy(block, smem, &tbps, ptg::MODE_FORWARD, v.g32.has_ext != 0) != cudaSuccess)
+    if (ptg::tail_occupancy(block, smem, &tbps, ptg::MODE_FORWARD, v.g32.has_ext != 0, v.g32.stage_smem != 0) != cudaSuccess)
       return PTG_ERR_CUDA;
     tgrid = v.num_sms * (tbps < 1 ? 1 : tbps);
   }
