@@ -617,6 +617,9 @@ int run_transport(ptg_handle* h, const Transport& T) {
       CU(cudaMemcpyAsync(h->order.p, order, sizeof(int) * norder, cudaMemcpyHostToDevice, h->stream));
     CU(cudaEventRecord(h->h2d_done, h->stream));
     h->h2d_pending = true;
+    /* the timed transport starts here, with the tables resident: the chunk
+       expansion is part of it */
+    CU(cudaEventRecord(h->ev[0], h->stream));
     if (nchunk > 0)
       CU(ptg::launch_expand_chunks(h->order.as<const int>(), (int)norder, (int)per_task, (int)csz,
                                    (int)T.np_local, h->chunk.as<int4>(), h->stream));
@@ -684,7 +687,6 @@ int run_transport(ptg_handle* h, const Transport& T) {
       CU(ptg::tail_occupancy(block, smem, &tbps, T.mode, h->g32.has_ext != 0, h->g32.stage_smem != 0));
       tgrid = h->num_sms * (tbps < 1 ? 1 : tbps);
     }
-    CU(cudaEventRecord(h->ev[0], h->stream));
     const bool work = (T.mode == ptg::MODE_ADJOINT || T.mode == ptg::MODE_TRACE) ? T.alist_n > 0
                                                                                    : r.nchunk > 0;
     if (work) {

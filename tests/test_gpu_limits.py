@@ -49,3 +49,27 @@ def test_fuchs_sondheimer_film(kn, precision, np_):
     est, se = limits.two_length_mfp(L1, T1, v1, L2, T2, v2)
     want = lam * limits.fuchs_sondheimer(kn)
     assert abs(est - want) < 3 * se + 0.005 * want, (est, want, se)
+
+
+def test_casimir_wire():
+    """Ballistic square wire (side a = 20 nm, fully diffuse walls, no
+    intrinsic scattering) at lengths 40a ... 640a: a weighted least-squares
+    fit of 1/<T(L)> = 3 L / (4 Lambda_C) + alpha ln(L/a) + beta (the bath term
+    of a wire grows like ln L, tests/limits.py) gives Lambda_C within 3
+    standard errors plus 0.5% of the Casimir length 1.114954 a."""
+    a = 20.0
+    ks = np.array([40, 80, 160, 320, 640], float)
+    ys, ws = [], []
+    for k in ks:
+        T, v = _flux_T(_wire(k * a, a, a, 0.0, 0.0), 1.0e10, 2000000 if k <= 160 else 1000000, A.PREC_FP32,
+                       seed=int(k))
+        ys.append(1.0 / T)
+        ws.append(T ** 4 / v)  # 1 / var(1/T)
+    y, w = np.array(ys), np.array(ws)
+    X = np.column_stack([0.75 * ks, np.log(ks), np.ones_like(ks)])  # lengths in units of a
+    cov = np.linalg.inv(X.T @ (w[:, None] * X))
+    p = cov @ X.T @ (w * y)
+    lam = 1.0 / p[0]
+    se = math.sqrt(cov[0, 0]) / p[0] ** 2
+    want = limits.casimir_square(1.0)
+    assert abs(lam - want) < 3 * se + 0.005 * want, (lam, se, want, p)
