@@ -353,7 +353,18 @@ def run_c5(args):
             r = bt.run()
             ms += r["graph_ms"]
             fl += r["flights"]
+        # per-geometry adjoint: one batched listing launch + one batched replay
+        t0 = time.perf_counter()
+        adj = bt.adjoint()
+        adj_s = time.perf_counter() - t0
     batch_rate = fl / (ms * 1e-3)
+    dks = np.concatenate([d for d in adj["dk_dp"]])
+    dke = np.concatenate([e for e in adj["dk_dp_stderr"]])
+    ok = ~np.isnan(dks)
+    adjoint = {"wall_s": adj_s, "kernel_ms": adj["kernel_ms"], "replayed": adj["replayed"],
+               "mismatched": adj["mismatched"], "geometries": len(adj["dk_dp"]),
+               "surface_records": int(ok.sum()), "resolved_3sigma": int(np.sum(np.abs(dks[ok]) > 3 * dke[ok])),
+               "dk_dscale_resolved_3sigma": int(np.sum(np.abs(adj["dk_dscale"]) > 3 * adj["dk_dscale_stderr"]))}
     # sequential plain FP64 runs of a subset of the films
     idx = list(range(0, 256, max(1, 256 // args.fp64_subset)))[: args.fp64_subset]
     f64_ms = f64_fl = 0.0
@@ -375,6 +386,7 @@ def run_c5(args):
                    "samples_total": int(sum(nps) * 20000), "fp64_subset": len(idx)},
         "plain_fp64_sequential": {"value": f64_rate, "unit": UNIT, "films": len(idx),
                                   "speedup_batch_over_fp64": batch_rate / f64_rate},
+        "adjoint": adjoint,
         "flights_per_step": fl / args.steps}))
     return 0
 
