@@ -59,7 +59,8 @@ def test_batch_adjoint_equals_individual_adjoints():
         ba = bt.adjoint()
         fwd = bt.run()
     assert ba["mismatched"] == 0
-    np.testing.assert_array_equal(ba["kappa"], fwd["kappa"])
+    # the same counts; host (adjoint) and device (forward) FP64 assembly differ in rounding only
+    np.testing.assert_allclose(ba["kappa"], fwd["kappa"], rtol=1e-12)
     replayed = 0
     for g in range(len(models)):
         single = A.make_run(kind_mfp=A.MFP_PER_MODE, nangle=7, np_=nps[g], seed=seeds[g], stream=streams[g],
