@@ -161,36 +161,46 @@ def issue_profile(phase="drain"):
 
 
 def cpu_leg(args):
-    """The cpu_baseline leg in a process of its own (bench.py --cpu-leg): the
-    oracle (OpenMP, all host threads) on the workload with this run's
-    particles per task, or fewer when that would take more than about 20 s.
-    torch is never imported here: next to torch's OpenMP runtime the oracle
-    ran about three times slower.  Prints one JSON line: the rate, the
-    sample, and the oracle's kappa and per-bin transmission with their
-    standard errors (the FP64 side of the parity object)."""
+    """The cpu_baseline leg in a process of its own (bench.py --cpu-leg; torch
+    is never imported here: next to torch's OpenMP runtime the oracle ran
+    about three times slower).  Two oracle runs (OpenMP, all host threads):
+      - the timed baseline, sized exactly as the reference arm sizes a step
+        (--impl reference: seed 12345, particles per task from a 2-particle
+        probe so that the run takes about 5 s), so the two rates compare; the
+        reference's schedule(static) loop makes the rate depend on where the
+        few 10^5-flight trajectories fall, i.e. on the sample;
+      - the parity run: the workload with this run's particles per task (or
+        fewer, when that would take more than --cpu-target-s), seed 777,
+        independent of the GPU run's draws, for kappa and the per-bin
+        transmission with their standard errors.
+    Prints one JSON line."""
     pkg = load_pkg()
     model, spec, _ = workload(pkg, np_per_task=args.np, mfp_lo=args.mfp_lo)
     if ROOT not in sys.path:
         sys.path.insert(0, ROOT)
     from oracle import oracle as O
     o = O.Oracle(model=model, spectrum=spec)
-    n = 2
-    run = make_run(pkg, spec, n, 0, 1, 0, seed=ORACLE_SEED)
-    _, _, r = o.counts(run)
-    probe_rate = r["flights"] / max(r["seconds"], 1e-6)
-    per_particle = r["seconds"] / n
-    n = max(2, min(args.np, int(args.cpu_target_s / max(per_particle, 1e-9))))
-    run = make_run(pkg, spec, n, 0, 1, 0, seed=ORACLE_SEED)
-    cnt, _, r = o.counts(run)
-    k = o.kappa(run, cnt)
     ntask = spec.nmode * 10
+    # timed baseline: the reference arm's recipe
+    _, _, r = o.counts(make_run(pkg, spec, 2, 0, 1, 0))
+    probe_rate = r["flights"] / max(r["seconds"], 1e-6)
+    nb = max(2, min(args.np, int(5.0 / max(r["seconds"] / 2, 1e-9))))
+    _, _, rb = o.counts(make_run(pkg, spec, nb, 0, 1, 0))
+    # parity run
+    n = 2
+    _, _, r = o.counts(make_run(pkg, spec, n, 0, 1, 0, seed=ORACLE_SEED))
+    n = max(2, min(args.np, int(args.cpu_target_s / max(r["seconds"] / n, 1e-9))))
+    run = make_run(pkg, spec, n, 0, 1, 0, seed=ORACLE_SEED)
+    cnt, _, rp = o.counts(run)
+    k = o.kappa(run, cnt)
     print(json.dumps({
-        "value": r["flights"] / r["seconds"], "unit": UNIT, "cores": int(r["threads"]), "kind": "port",
-        "seconds": r["seconds"], "flights": int(r["flights"]), "probe_rate": probe_rate,
-        "particles_per_task": n,
-        "sample": (f"all {ntask} (mode, angle) tasks with {n} particles each " +
-                   ("(the whole workload)" if n >= args.np else f"instead of {args.np}") +
-                   f", {r['samples']} trajectories, same geometry and spectrum, seed {ORACLE_SEED}"),
+        "value": rb["flights"] / rb["seconds"], "unit": UNIT, "cores": int(rb["threads"]), "kind": "port",
+        "seconds": rb["seconds"], "flights": int(rb["flights"]), "probe_rate": probe_rate,
+        "sample": (f"all {ntask} (mode, angle) tasks with {nb} particles each, seed 12345 (the reference "
+                   f"arm's step)"),
+        "parity_sample": (f"all {ntask} (mode, angle) tasks with {n} particles each, {rp['samples']} "
+                          f"trajectories, seed {ORACLE_SEED}, {rp['seconds']:.1f} s"),
+        "parity_run_rate": rp["flights"] / rp["seconds"],
         "kappa": k["kappa"], "kappa_stderr": k["kappa_stderr"],
         "bin_T": [float(x) for x in k["bin_T"]], "bin_T_stderr": [float(x) for x in k["bin_T_stderr"]]}))
     return 0
@@ -826,7 +836,8 @@ def main():
             leg = cpu_baseline(args)
             result["cpu_baseline"] = {k: leg[k] for k in ("value", "unit", "cores", "kind", "sample",
                                                           "seconds", "flights", "probe_rate")}
-            result["parity"] = parity(out, leg)
+            result["parity"] = dict(parity(out, leg), oracle_sample=leg["parity_sample"],
+                                    oracle_run_rate=leg["parity_run_rate"])
     h.close()
     del flush
     if dist is not None:

@@ -389,8 +389,9 @@ int ptg_fortran_format(int32_t kind, double v, int32_t w, int32_t d, char* out, 
  * the analytic term of the bulk-MFP dependence of their kappa rule).
  * Derivatives are per surface record of the built geometry; records with
  * p = 0 or 1 get NaN (the estimator is biased at the end points).  Standard
- * errors come from 8 interleaved sample batches.  At most 2^25 transmitted
- * samples per call (PTG_ERR_UNSUPPORTED beyond).
+ * errors come from 8 interleaved sample batches.  The listing pass keeps
+ * 8 bytes per sample of the run on the device (at most 2^31 samples per
+ * call, PTG_ERR_UNSUPPORTED beyond).
  */
 typedef struct ptg_adjoint_out {
   double kappa, kappa_stderr;

@@ -1354,7 +1354,7 @@ int ptg_adjoint(ptg_handle* h, const ptg_run* run, ptg_adjoint_out* out) {
     ptg::run_tasks(h->spec, run, &tasks);
     const int64_t ntask = (int64_t)tasks.size();
     const int nsurf = h->geom.nsurf();
-    const unsigned long long cap = 1ull << 25;
+    const unsigned long long cap = 1ull << 31;  /* listed ids: at most every sample of the run */
     CU(cudaSetDevice(h->device));
     /* 1. forward pass that lists the samples leaving through x+ */
     Transport T;
@@ -1384,7 +1384,7 @@ int ptg_adjoint(ptg_handle* h, const ptg_run* run, ptg_adjoint_out* out) {
     const double fwd_ms = h->last.kernel_ms;
     const uint64_t fwd_flights = h->last.flights;
     const unsigned long long nlist = h->list_n;
-    if (nlist > T.tlist_cap) { h->last_error = "more than 2^25 transmitted samples"; return PTG_ERR_UNSUPPORTED; }
+    if (nlist > T.tlist_cap) { h->last_error = "more than 2^31 transmitted samples"; return PTG_ERR_UNSUPPORTED; }
     /* 2. kappa and d kappa / d T_task on the host */
     ptg_kappa_out ko;
     memset(&ko, 0, sizeof(ko));

@@ -437,7 +437,8 @@ extern "C" int ptg_batch_adjoint(ptg_batch* b, ptg_batch_adjoint_out* out) {
                               ? (b->np[g] - b->run.rank + b->run.nranks - 1) / b->run.nranks : 0;
       total += (unsigned long long)ntg * (unsigned long long)npl;
     }
-    const unsigned long long cap = std::min<unsigned long long>(total, 1ull << 26);
+    /* room for every sample of the run (at most 2^31 ids, 16 GB) */
+  const unsigned long long cap = std::min<unsigned long long>(total, 1ull << 31);
     if (b->adj_list_cap < cap || !b->adj_list.p) {
       if (b->adj_list.p) { cudaFree(b->adj_list.p); b->adj_list.p = nullptr; }
       if (b->adj_list.alloc(sizeof(unsigned long long) * (cap ? cap : 1)) != cudaSuccess) return PTG_ERR_NOMEM;

@@ -41,9 +41,10 @@ def test_batch_equals_individual_runs():
 
 def test_batch_adjoint_equals_individual_adjoints():
     """ptg_batch_adjoint gives every geometry what ptg_adjoint gives for its
-    own run: the same kappa (the same counts), the same replayed samples, and
-    the same derivatives up to the order of the FP64 sums (the scores of the
-    same samples, added in another order)."""
+    own run: the same kappa (the same counts), the same replayed samples, the
+    same specularity derivatives up to the order of the FP64 sums (the scores
+    of the same samples, added in another order), and the scale derivative up
+    to the FP32 summation order of the samples' path lengths."""
     import dataclasses
     models, _ = synth.film_batch(n=4, seed=5, n_modes=12, nangle=7)
     models = [dataclasses.replace(m, tt_spec=np.array([0.4, 0.0]), cellspec=(1.0, 1.0, 1.0, 1.0, 0.5, 0.3))
@@ -76,5 +77,7 @@ def test_batch_adjoint_equals_individual_adjoints():
         assert ok.sum() >= 3
         assert np.all(np.abs(got[ok] - want[ok]) <= 1e-6 * se[ok] + 1e-12 * np.abs(want[ok]))
         np.testing.assert_allclose(ba["dk_dp_stderr"][g][ok], se[ok], rtol=1e-6)
-        assert abs(ba["dk_dscale"][g] - sa["dk_dscale"]) <= 1e-6 * sa["dk_dscale_stderr"] + 1e-12 * abs(sa["dk_dscale"])
+        # the scale score sums each sample's FP32 path length, in another order
+        # where the single run's tail phase adds a round's flights by warp shuffles
+        assert abs(ba["dk_dscale"][g] - sa["dk_dscale"]) <= 1e-3 * sa["dk_dscale_stderr"] + 1e-5 * abs(sa["dk_dscale"])
     assert ba["replayed"] == replayed
