@@ -396,7 +396,7 @@ __device__ __noinline__ void scan_bvh(const G_t& G, int root, float px, float py
    (the box-grain exit, >= 0) and sb are updated; tb stays >= 0.  fp is the
    flight's free path: a BVH search skips what lies beyond it (a hit farther
    away cannot end the flight). */
-template <bool EXT, int UNROLL = 1, class G_t>
+template <bool EXT, class G_t>
 __device__ __forceinline__ void scan_grain(const G_t& G, int grain, float px, float py, float pz,
                                            float dx, float dy, float dz, int last_geom, float eps,
                                            float zmax, float fp, float& tb, int& sb, unsigned& nbox,
@@ -406,9 +406,6 @@ __device__ __forceinline__ void scan_grain(const G_t& G, int grain, float px, fl
   if (root < 0) {
     const int kb = G.cand_begin(grain), ke = G.cand_begin(grain + 1);
     nsurf += (unsigned)(ke - kb);
-    /* UNROLL > 1 (the tail kernel, latency-bound): the candidates' tests
-       overlap; the comparisons keep their order */
-#pragma unroll UNROLL
     for (int k = kb; k < ke; ++k)
       test_surface<EXT>(G, G.cand(k), px, py, pz, dx, dy, dz, last_geom, eps, zmax, tr, sb);
   } else {
@@ -533,7 +530,7 @@ __device__ __noinline__ float safety_bvh(const G_t& G, int root, float px, float
    receives the bound over the candidate surfaces alone (the grain ball: a
    flight inside it needs the box-face test only); for a BVH grain it is
    searched no farther than the full bound, so it costs no extra nodes. */
-template <bool EXT, int UNROLL = 1, class G_t>
+template <bool EXT, class G_t>
 __device__ __forceinline__ float safety(const G_t& G, int grain, float px, float py, float pz,
                                         float X, float Y, float Z, float eps, float cap,
                                         float& dgrain) {
@@ -543,7 +540,6 @@ __device__ __forceinline__ float safety(const G_t& G, int grain, float px, float
     const int root = EXT ? G.bvh_root(grain) : -1;
     if (root < 0) {
       const int kb = G.cand_begin(grain), ke = G.cand_begin(grain + 1);
-#pragma unroll UNROLL
       for (int k = kb; k < ke; ++k) dc = fminf(dc, surface_lb<EXT>(G, G.cand(k), px, py, pz));
     } else {
       dc = safety_bvh<EXT>(G, root, px, py, pz, fminf(dbox, cap));
@@ -1122,8 +1118,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             if (!in_ball && lane < jw) {
               slab_exit(qx, qy, qz, sdx, sdy, sdz, X, Y, Z, tb, sb);
               if (cgrain > 0 && !in_gball)
-                scan_grain<EXT, 4>(G, cgrain, qx, qy, qz, sdx, sdy, sdz, lane == 0 ? clast : -1, eps,
-                                   Z, sfp, tb, sb, my_box_tests, my_surf_tests);
+                scan_grain<EXT>(G, cgrain, qx, qy, qz, sdx, sdy, sdz, lane == 0 ? clast : -1, eps,
+                                Z, sfp, tb, sb, my_box_tests, my_surf_tests);
             }
             const bool brk = !inbox || capd;
             const unsigned sm =
@@ -1173,7 +1169,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             if (!__shfl_sync(FULL, in_ball, j - 1) && r.fast_steps > 0) {
               float dg;
               const float d =
-                  safety<EXT, 4>(G, cgrain, cpx, cpy, cpz, X, Y, Z, eps, kBallCapMfp * clam, dg);
+                  safety<EXT>(G, cgrain, cpx, cpy, cpz, X, Y, Z, eps, kBallCapMfp * clam, dg);
               cbx = cpx; cby = cpy; cbz = cpz;
               cbr2 = d > 0.0f ? d * d : 0.0f;
               cgr2 = dg > 0.0f ? dg * dg : 0.0f;
