@@ -677,7 +677,7 @@ int run_transport(ptg_handle* h, const Transport& T) {
        dry), so the drain grid's lanes bound the tail list */
     const bool tail = r.coop_lanes > 0 && T.mode != ptg::MODE_TRACE;
     if (tail) {
-      CU(h->tail.ensure(sizeof(float4) * 6 * (size_t)grid * block));
+      CU(h->tail.ensure(sizeof(float4) * ptg::kTailUnits * (size_t)grid * block));
       r.tail = h->tail.as<float4>();
       r.tail_cap = grid * block;
     }

@@ -138,7 +138,7 @@ struct RunF32 {
                                  live phonons moves its diffusive ones to the tail
                                  list, where each gets a warp of its own that
                                  advances it 32 flights a round (0: off)          */
-  float4* tail;               /* tail list: 6 float4 per phonon                    */
+  float4* tail;               /* tail list: kTailUnits float4 per phonon           */
   int32_t tail_cap;           /* its capacity in phonons                           */
   int32_t stage_test;         /* test only: set up the shared-memory staging
                                  barrier without issuing the copy, so its
@@ -209,6 +209,11 @@ cudaError_t launch_persistent_batch(const RunF32& r, int grid, int block, cudaSt
                                     bool bvh, int mode = MODE_FORWARD);
 cudaError_t persistent_batch_occupancy(int block, int* blocks_per_sm, bool bvh,
                                        int mode = MODE_FORWARD);
+/* float4 per phonon in the tail list: the state of a phonon handed from the
+   drain phase to the tail phase (position, direction, free path, MFP, the
+   ball centre and radii, grain, last surface, task, omega, sample id,
+   flight, adjoint terms, second ball). */
+constexpr int kTailUnits = 7;
 /* Shared memory for staged BVH nodes when the whole blob is not staged:
    64 KB, the top ten or so levels of the trees, small enough that two
    blocks of the tail kernel (28.5 KB of its own) still fit on an SM. */

@@ -533,20 +533,43 @@ __device__ __noinline__ float safety_bvh(const G_t& G, int root, float px, float
 template <bool EXT, class G_t>
 __device__ __forceinline__ float safety(const G_t& G, int grain, float px, float py, float pz,
                                         float X, float Y, float Z, float eps, float cap,
-                                        float& dgrain) {
+                                        float& dgrain, float& dgrain2, int& near) {
   const float dbox = fminf(fminf(fminf(px, X - px), fminf(py, Y - py)), fminf(pz, Z - pz));
-  float dc = 3.0e38f;
+  float dc = 3.0e38f, dc2 = 3.0e38f;
+  near = -1;
   if (grain > 0) {
     const int root = EXT ? G.bvh_root(grain) : -1;
     if (root < 0) {
+      /* the nearest candidate and the bound of all the others */
       const int kb = G.cand_begin(grain), ke = G.cand_begin(grain + 1);
-      for (int k = kb; k < ke; ++k) dc = fminf(dc, surface_lb<EXT>(G, G.cand(k), px, py, pz));
+      for (int k = kb; k < ke; ++k) {
+        const int sk = G.cand(k);
+        const float d = surface_lb<EXT>(G, sk, px, py, pz);
+        const bool nearer = d < dc;
+        dc2 = nearer ? dc : fminf(dc2, d);
+        near = nearer ? sk : near;
+        dc = nearer ? d : dc;
+      }
     } else {
       dc = safety_bvh<EXT>(G, root, px, py, pz, fminf(dbox, cap));
+      dc2 = dc;  /* no second ball for a grain searched by its BVH */
     }
   }
   dgrain = dc - 4.0f * eps;
+  dgrain2 = dc2 - 4.0f * eps;
   return fminf(dbox, dc) - 4.0f * eps;
+}
+
+/* One candidate surface, where the second ball has shown it to be the only
+   one a flight can reach: scan_grain's result for that flight. */
+template <bool EXT, class G_t>
+__device__ __forceinline__ void test_near(const G_t& G, int s, float px, float py, float pz,
+                                          float dx, float dy, float dz, int last_geom, float eps,
+                                          float zmax, float& tb, int& sb, unsigned& nsurf) {
+  float tr = tb;
+  nsurf += 1u;
+  test_surface<EXT>(G, s, px, py, pz, dx, dy, dz, last_geom, eps, zmax, tr, sb);
+  tb = fmaxf(tr, 0.0f);
 }
 
 /* Trace replay: position after flight f of the sample in replay-list slot t
@@ -666,8 +689,7 @@ constexpr int kTestWindow = 4;
    lane 0 and advances it with cooperative rounds, so the longest
    trajectories get a warp each instead of sharing one. */
 enum { PH_DRAIN = 0, PH_TAIL = 1 };
-/* float4 per phonon in the tail list */
-constexpr int kTailUnits = 6;
+/* float4 per phonon in the tail list: kTailUnits (kernels.h) */
 /* A phonon handed over past this many flights goes to the front of the tail
    list, which the tail phase takes first, the others to the back: a phonon
    that has lasted long is the likeliest to last longer, and the tail ends
@@ -710,8 +732,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
      different banks */
   __shared__ __align__(16) float coop_rowf[PH == PH_TAIL ? kBlock / 32 : 1][kRowStride * 7];
   float* const crow = coop_rowf[PH == PH_TAIL ? (threadIdx.x >> 5) : 0];
-  /* ... and five rows where the lanes' own phonons wait during the rounds */
-  __shared__ float4 coop_park[PH == PH_TAIL ? kBlock / 32 : 1][5][32];
+  /* ... and six rows where the lanes' own phonons wait during the rounds */
+  __shared__ float4 coop_park[PH == PH_TAIL ? kBlock / 32 : 1][6][32];
   float4 (*const park)[32] = coop_park[PH == PH_TAIL ? (threadIdx.x >> 5) : 0];
   /* tail phase: phonons the drain left (the counts are final at launch),
      long ones from the front of the list, the others from the back */
@@ -744,6 +766,11 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
      ball: no candidate surface of the grain closer than sqrt(gr2) to the
      same centre (box faces excepted), kept until the phonon changes grain */
   float bx = 0, by = 0, bz = 0, br2 = 0, gr2 = 0;
+  /* second ball about the same centre: every candidate but the nearest
+     (gnear) farther than sqrt(g2r2), so a flight inside it can hit only
+     gnear (or a box face) */
+  float g2r2 = 0;
+  int gnear = -1;
   int grain = 0, last_geom = -1, task = 0;
   uint32_t slo = 0, shi = 0, flight = 0;
   unsigned long long my_flights = 0, my_samples = 0, my_capped = 0, my_lost = 0, my_max = 0;
@@ -770,6 +797,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
         task = __float_as_int(e3.z); omr = e3.w;
         slo = __float_as_uint(e4.x); shi = __float_as_uint(e4.y);
         flight = __float_as_uint(e4.z); gr2 = e4.w;
+        const float4 e6 = e[6];
+        g2r2 = e6.x; gnear = __float_as_int(e6.y);
         if (MODE == MODE_ADJOINT) {
           const float4 e5 = e[5];
           adj_w = e5.x; adj_len = e5.y;
@@ -901,6 +930,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           last_geom = -1;
           br2 = 0.0f;
           gr2 = 0.0f;
+          g2r2 = 0.0f;
+          gnear = -1;
           flight = 0;
           alive = true;
           my_samples += 1;
@@ -953,6 +984,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
                              __int_as_float(task), omr);
           e[4] = make_float4(__uint_as_float(slo), __uint_as_float(shi), __uint_as_float(flight),
                              gr2);
+          e[6] = make_float4(g2r2, __int_as_float(gnear), 0.0f, 0.0f);
           if (MODE == MODE_ADJOINT)
             e[5] = make_float4(adj_w, adj_len, __uint_as_float(adj_npp), __int_as_float(adj_b));
           atomicAdd(r.stats + 16, (unsigned long long)flight);
@@ -998,6 +1030,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
                                     __int_as_float(task), omr);
         park[4][lane] = make_float4(__uint_as_float(slo), __uint_as_float(shi),
                                     __uint_as_float(flight), gr2);
+        park[5][lane] = make_float4(g2r2, __int_as_float(gnear), 0.0f, 0.0f);
         __syncwarp();
         unsigned todo = todo0;
         while (todo) {
@@ -1005,6 +1038,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           todo &= todo - 1;
           const float4 s0 = park[0][L], s1 = park[1][L], s2 = park[2][L], s3 = park[3][L];
           const float4 s4 = park[4][L];
+          const float4 s5 = park[5][L];
           float cpx = s0.x, cpy = s0.y, cpz = s0.z;
           float cdx = s0.w, cdy = s1.x, cdz = s1.y, cfp = s1.z;
           const float clam = s1.w;
@@ -1014,6 +1048,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           int clast = __float_as_int(s3.y);
           /* the phonon's safe ball: flights ending inside it skip the test */
           float cbx = s2.x, cby = s2.y, cbz = s2.z, cbr2 = s2.w, cgr2 = s4.w;
+          float cg2r2 = s5.x;
+          int cnear = __float_as_int(s5.y);
           float clen = 0.0f;
           unsigned cnpp = 0, ctaken = 0, crounds = 0;
           int stop = 0;  /* 0 round limit, 1 surface hit, 2 lost or capped */
@@ -1109,17 +1145,24 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             const float de2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
             const float ds2 = fmaf(sx, sx, fmaf(sy, sy, sz * sz));
             const bool in_ball = de2 < cbr2 && ds2 < cbr2;
-            /* in the grain ball only the box faces can be hit */
+            /* in the grain ball only the box faces can be hit, in the second
+               ball only they and the grain's nearest candidate */
             const bool in_gball = de2 < cgr2 && ds2 < cgr2;
+            const bool in_g2 = de2 < cg2r2 && ds2 < cg2r2;
             const unsigned outm = __ballot_sync(FULL, !in_ball);
             const int jw = (EXT && outm) ? min(32, __ffs(outm) - 1 + kTestWindow) : 32;
             float tb = 3.0e38f;
             int sb = -1;
             if (!in_ball && lane < jw) {
               slab_exit(qx, qy, qz, sdx, sdy, sdz, X, Y, Z, tb, sb);
-              if (cgrain > 0 && !in_gball)
-                scan_grain<EXT>(G, cgrain, qx, qy, qz, sdx, sdy, sdz, lane == 0 ? clast : -1, eps,
-                                Z, sfp, tb, sb, my_box_tests, my_surf_tests);
+              if (cgrain > 0 && !in_gball) {
+                if (in_g2)
+                  test_near<EXT>(G, cnear, qx, qy, qz, sdx, sdy, sdz, lane == 0 ? clast : -1, eps, Z,
+                                 tb, sb, my_surf_tests);
+                else
+                  scan_grain<EXT>(G, cgrain, qx, qy, qz, sdx, sdy, sdz, lane == 0 ? clast : -1, eps,
+                                  Z, sfp, tb, sb, my_box_tests, my_surf_tests);
+              }
             }
             const bool brk = !inbox || capd;
             const unsigned sm =
@@ -1167,12 +1210,13 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             if (j != 32) Rnext = philox10(cfl + 1u + (uint32_t)lane, c1, cslo, cshi, key);
             /* a new ball where the walk left the old one */
             if (!__shfl_sync(FULL, in_ball, j - 1) && r.fast_steps > 0) {
-              float dg;
-              const float d =
-                  safety<EXT>(G, cgrain, cpx, cpy, cpz, X, Y, Z, eps, kBallCapMfp * clam, dg);
+              float dg, dg2;
+              const float d = safety<EXT>(G, cgrain, cpx, cpy, cpz, X, Y, Z, eps,
+                                          kBallCapMfp * clam, dg, dg2, cnear);
               cbx = cpx; cby = cpy; cbz = cpz;
               cbr2 = d > 0.0f ? d * d : 0.0f;
               cgr2 = dg > 0.0f ? dg * dg : 0.0f;
+              cg2r2 = (dg2 > 0.0f && cnear >= 0) ? dg2 * dg2 : 0.0f;
             }
             clast = -1;
           }
@@ -1183,6 +1227,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             park[3][lane] = make_float4(__int_as_float(cgrain), __int_as_float(clast),
                                         s3.z, s3.w);
             park[4][lane] = make_float4(s4.x, s4.y, __uint_as_float(cfl), cgr2);
+            park[5][lane] = make_float4(cg2r2, __int_as_float(cnear), 0.0f, 0.0f);
             if (MODE == MODE_ADJOINT) {
               adj_len += clen;
               adj_npp += cnpp;
@@ -1203,7 +1248,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
         /* every lane takes its phonon back (each slot was last written by its
            own lane) */
         const float4 s0 = park[0][lane], s1 = park[1][lane], s2 = park[2][lane];
-        const float4 s3 = park[3][lane], s4 = park[4][lane];
+        const float4 s3 = park[3][lane], s4 = park[4][lane], s5 = park[5][lane];
         px = s0.x; py = s0.y; pz = s0.z; dx = s0.w;
         dy = s1.x; dz = s1.y; fp = s1.z; lam = s1.w;
         bx = s2.x; by = s2.y; bz = s2.z; br2 = s2.w;
@@ -1211,6 +1256,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
         task = __float_as_int(s3.z); omr = s3.w;
         slo = __float_as_uint(s4.x); shi = __float_as_uint(s4.y); flight = __float_as_uint(s4.z);
         gr2 = s4.w;
+        g2r2 = s5.x; gnear = __float_as_int(s5.y);
       }
     }
 
@@ -1299,11 +1345,17 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           const float ex = fmaf(fp, dx, px) - bx, ey = fmaf(fp, dy, py) - by;
           const float ez = fmaf(fp, dz, pz) - bz;
           const float sx = px - bx, sy = py - by, sz = pz - bz;
-          const bool in_gball = fmaf(ex, ex, fmaf(ey, ey, ez * ez)) < gr2 &&
-                                fmaf(sx, sx, fmaf(sy, sy, sz * sz)) < gr2;
-          if (grain > 0 && !in_gball)
-            scan_grain<EXT>(G, grain, px, py, pz, dx, dy, dz, last_geom, eps, Z, fp, tb, sb, my_box_tests,
-                       my_surf_tests);
+          const float fe2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+          const float fs2 = fmaf(sx, sx, fmaf(sy, sy, sz * sz));
+          const bool in_gball = fe2 < gr2 && fs2 < gr2;
+          if (grain > 0 && !in_gball) {
+            if (fe2 < g2r2 && fs2 < g2r2)
+              test_near<EXT>(G, gnear, px, py, pz, dx, dy, dz, last_geom, eps, Z, tb, sb,
+                             my_surf_tests);
+            else
+              scan_grain<EXT>(G, grain, px, py, pz, dx, dy, dz, last_geom, eps, Z, fp, tb, sb,
+                              my_box_tests, my_surf_tests);
+          }
           go = true;
         }
         if (go) {
@@ -1328,13 +1380,17 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             last_geom = -1;
             br2 = 0.0f;
             if (MODE != MODE_TRACE && r.fast_steps > 0 && lam < flmax) {
-              float dg;
-              const float d = safety<EXT>(G, grain, px, py, pz, X, Y, Z, eps, kBallCapMfp * lam, dg);
+              float dg, dg2;
+              int nr;
+              const float d =
+                  safety<EXT>(G, grain, px, py, pz, X, Y, Z, eps, kBallCapMfp * lam, dg, dg2, nr);
               ++my_balls;
               if (dg > 0.0f) {
                 bx = px; by = py; bz = pz;
                 br2 = d > 0.0f ? d * d : 0.0f;
                 gr2 = dg * dg;
+                g2r2 = (dg2 > 0.0f && nr >= 0) ? dg2 * dg2 : 0.0f;
+                gnear = nr;
               }
             }
           } else {
@@ -1446,6 +1502,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
               if (transmitted) {
                 grain = meta >> 8;
                 gr2 = 0.0f;
+                g2r2 = 0.0f;
               }
               last_geom = B.w;
             }

@@ -39,7 +39,7 @@ namespace {
 constexpr int64_t kMaxTasks = PTG_NOALLOC_MAX_TASKS;
 constexpr int64_t kMaxChunks = PTG_NOALLOC_MAX_CHUNKS;
 constexpr int kMaxAngles = 64;
-constexpr int kMaxTail = 65536;   /* tail-list phonons, 96 B each */
+constexpr int kMaxTail = 65536;   /* tail-list phonons, kTailUnits float4 each */
 
 /* layout of the scratch array, byte offsets (all 256-byte aligned) */
 constexpr size_t kOffStats = 0;                                /* u64[kStatSlots] */
@@ -50,8 +50,8 @@ constexpr size_t kOffLost = kOffCounts + 8 * kMaxTasks;        /* u64[tasks]    
 constexpr size_t kOffTasks = kOffLost + 8 * kMaxTasks;         /* float4[tasks] */
 constexpr size_t kOffOmega = kOffTasks + 16 * kMaxTasks;       /* double[tasks] */
 constexpr size_t kOffChunks = kOffOmega + 8 * kMaxTasks;       /* int4[chunks]  */
-constexpr size_t kOffTail = kOffChunks + 16 * kMaxChunks;     /* float4[6 * tail] */
-constexpr size_t kScratchBytes = kOffTail + 96 * (size_t)kMaxTail;
+constexpr size_t kOffTail = kOffChunks + 16 * kMaxChunks;     /* float4[kTailUnits * tail] */
+constexpr size_t kScratchBytes = kOffTail + 16 * (size_t)ptg::kTailUnits * (size_t)kMaxTail;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
