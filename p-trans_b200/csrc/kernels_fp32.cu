@@ -473,34 +473,44 @@ __device__ __forceinline__ float box_dist(float4 lo, float4 hi, float px, float 
   return sqrt_approx(fmaf(ex, ex, fmaf(ey, ey, ez * ez)));
 }
 
-/* BVH range query for the safe ball: the smallest lower bound of the
-   distance from p to a surface of the grain, searched below d (nodes
-   farther than the bound so far are pruned; a leaf contributes
-   max(distance to its box, nearest plane / quadric bound of its surfaces)).
-   Out of line, like scan_bvh. */
+/* BVH range query for the safe ball: the smallest lower bound d of the
+   distance from p to a surface of the grain, the surface it belongs to
+   (near) and the smallest bound d2 of every other surface, searched below
+   the initial d (nodes no nearer than the second bound so far are pruned:
+   they cannot change either; a surface's bound is the larger of the
+   distance to its leaf's box and its own plane / quadric bound).  Out of
+   line, like scan_bvh. */
 template <bool EXT, class G_t>
 __device__ __noinline__ float safety_bvh(const G_t& G, int root, float px, float py, float pz,
-                                         float d) {
+                                         float d, float& d2, int& near) {
   int stk[kBvhStack];
   float std_[kBvhStack];
   int sp = 0;
   int node = root;
+  d2 = d;
+  near = -1;
   while (true) {
     const float4 n0 = G.node(2 * node), n1 = G.node(2 * node + 1);
     const int cnt = __float_as_int(n1.w);
     const int a = __float_as_int(n0.w);
     bool descended = false;
     if (cnt > 0) {
-      float e = 3.0e38f;
-      for (int k = a; k < a + cnt; ++k) e = fminf(e, surface_lb<EXT>(G, G.cand(k), px, py, pz));
-      d = fminf(d, fmaxf(box_dist(n0, n1, px, py, pz), e));
+      const float bd = box_dist(n0, n1, px, py, pz);
+      for (int k = a; k < a + cnt; ++k) {
+        const int sk = G.cand(k);
+        const float e = fmaxf(bd, surface_lb<EXT>(G, sk, px, py, pz));
+        const bool nearer = e < d;
+        d2 = nearer ? d : fminf(d2, e);
+        near = nearer ? sk : near;
+        d = nearer ? e : d;
+      }
     } else {
       const float dl = box_dist(G.node(2 * a), G.node(2 * a + 1), px, py, pz);
       const float dg = box_dist(G.node(2 * a + 2), G.node(2 * a + 3), px, py, pz);
       const bool lf = dl <= dg;
       const float dn = lf ? dl : dg, df = lf ? dg : dl;
-      if (dn < d) {
-        if (df < d && sp < kBvhStack) {
+      if (dn < d2) {
+        if (df < d2 && sp < kBvhStack) {
           stk[sp] = lf ? a + 1 : a;
           std_[sp] = df;
           ++sp;
@@ -513,7 +523,7 @@ __device__ __noinline__ float safety_bvh(const G_t& G, int root, float px, float
     bool found = false;
     while (sp > 0) {
       --sp;
-      if (std_[sp] < d) {
+      if (std_[sp] < d2) {
         node = stk[sp];
         found = true;
         break;
@@ -551,8 +561,7 @@ __device__ __forceinline__ float safety(const G_t& G, int grain, float px, float
         dc = nearer ? d : dc;
       }
     } else {
-      dc = safety_bvh<EXT>(G, root, px, py, pz, fminf(dbox, cap));
-      dc2 = dc;  /* no second ball for a grain searched by its BVH */
+      dc = safety_bvh<EXT>(G, root, px, py, pz, fminf(dbox, cap), dc2, near);
     }
   }
   dgrain = dc - 4.0f * eps;
