@@ -45,9 +45,10 @@
  *     a warp that advances it 32 flights per round, one flight per lane, with
  *     the flights' start points summed in flight order (in grains with a BVH
  *     a round tests at most kTestWindow flights from its first one outside
- *     the safe ball); every path (fast, full, cooperative) moves the position
- *     with the same fma, so a trajectory is the same whichever path takes its
- *     flights.
+ *     the safe ball), and takes the phonon's surface events in the warp too;
+ *     every path (fast, full, cooperative) moves the position with the same
+ *     fma and takes events with the same code, so a trajectory is the same
+ *     whichever path takes its flights.
  */
 #include <cuda_runtime.h>
 #include <math.h>
@@ -581,6 +582,154 @@ __device__ __forceinline__ void test_near(const G_t& G, int s, float px, float p
   tb = fmaxf(tr, 0.0f);
 }
 
+/* Adjoint accumulators of the sample: dlogP/dp of surface k goes to
+   base + k, in shared memory (sh) when the block holds them, else global. */
+struct AdjAcc {
+  double* sh;
+  double* gl;
+  float w;
+  int base;
+  bool in_smem;
+};
+
+/* The event at the end of a flight that reaches a surface or box face at
+   distance tb along its direction (calcTransmit's collision branch,
+   src/RTMCphon.f90:1744-1792, with 2225-2413): the phonon moves to the hit
+   point and keeps the rest of its free path; the bath faces end it
+   (returns 1 for x-, 2 for x+), a periodic face wraps it, and any other
+   surface reflects it (determinSpecular, then reflectSpecular or
+   reflectDiffusive) or lets it through into the grain on the other side
+   (determinTransmit).  Returns -1 while the phonon goes on.  u0..u3 are
+   the flight's Philox uniforms.  The one-lane path and the tail phase's
+   rounds both take their events here, so a trajectory does not depend on
+   which of them met the surface. */
+template <int MODE, bool EXT, class G_t>
+__device__ __forceinline__ int surface_hit(const G_t& G, float tb, int sb, float u0, float u1,
+                                           float u2, float u3, float Y, float Z, int pmask,
+                                           int nmat, float omr, float lam, uint32_t flight,
+                                           uint32_t c1, uint32_t slo, uint32_t shi, Key2 key,
+                                           const AdjAcc& acc, float& px, float& py, float& pz,
+                                           float& dx, float& dy, float& dz, float& fp, int& grain,
+                                           float& gr2, float& g2r2, int& last_geom) {
+  int end_side = -1;
+  px = fmaf(tb, dx, px);
+  py = fmaf(tb, dy, py);
+  pz = fmaf(tb, dz, pz);
+  fp -= tb;
+  if (sb == 0) {
+    end_side = 1;
+  } else if (sb == 1) {
+    end_side = 2;
+  } else if (sb < 6 && ((pmask >> sb) & 1)) {
+    const int ax = sb >> 1;
+    const float L = ax == 1 ? Y : Z;
+    const float sg = (sb & 1) ? -L : L;
+    if (ax == 1) py += sg; else pz += sg;
+    last_geom = -1;
+  } else {
+    const float4 C0 = G.cold(sb, 0), C1 = G.cold(sb, 1), C2 = G.cold(sb, 2);
+    const int meta = __float_as_int(C2.w);
+    const int kind = meta & 0xff;
+    /* transmission threshold: a fixed value, or Gamma / TBC of the mode
+       (one material) or drawn between the two materials' values */
+    float thr = 0.0f;
+    if (kind == 1) {
+      thr = C1.w;
+    } else if (kind == 2 || kind == 3) {
+      if (nmat == 1) {
+        thr = __frcp_rn(fmaf(C1.w, omr, 1.0f));
+      } else {
+        const uint4 R2 = philox10(flight, c1 | 1u, slo, shi, key);
+        const float t11 = __frcp_rn(C1.w + 1.0f);
+        thr = fmaf(u23f(R2.x), 1.0f - t11, t11);
+      }
+    }
+    /* surface normal at the hit point and surface frame */
+    float nx, ny, nz, ax1, ay1, az1, ax2, ay2, az2;
+    const int4 B = G.hotB(sb);
+    const int type = B.x & 0xff;
+    if (type == REC_POLY) {
+      nx = C2.x; ny = C2.y; nz = C2.z;
+      ax1 = C0.x; ay1 = C0.y; az1 = C0.z;
+      ax2 = C1.x; ay2 = C1.y; az2 = C1.z;
+    } else {
+      const float4 A = G.hotA(sb);
+      if (EXT && type == REC_CAP) {
+        capped_normal(A, G.edge(B.y), px, py, pz, nx, ny, nz);
+      } else {
+        float rx = px - A.x, ry = py - A.y, rz = (type == REC_SPHERE) ? pz - A.z : 0.0f;
+        const float inv = rsqrtf(fmaf(rx, rx, fmaf(ry, ry, rz * rz)));
+        nx = rx * inv; ny = ry * inv; nz = rz * inv;
+      }
+      const float q2 = fmaf(nx, nx, ny * ny);
+      if (q2 > 1.0e-12f) {
+        const float q = rsqrtf(q2);
+        ax2 = -ny * q; ay2 = nx * q; az2 = 0.0f;
+        /* t1 = t2 x n */
+        ax1 = ay2 * nz - az2 * ny;
+        ay1 = az2 * nx - ax2 * nz;
+        az1 = ax2 * ny - ay2 * nx;
+      } else {
+        ax2 = 0.0f; ay2 = 1.0f; az2 = 0.0f;
+        ax1 = 1.0f; ay1 = 0.0f; az1 = 0.0f;
+      }
+    }
+    /* tmpNormal oriented along the incoming direction */
+    const float dn0 = fmaf(nx, dx, fmaf(ny, dy, nz * dz));
+    const float on = dn0 < 0.0f ? -1.0f : 1.0f;
+    bool transmitted = false;
+    if (MODE == MODE_ADJOINT) {
+      /* d log P / d p of the specular (1/p) or diffuse (-1/(1-p)) choice */
+      const float pk = C0.w;
+      if (pk > 0.0f && pk < 1.0f) {
+        const double sc = (u0 <= pk) ? 1.0 / (double)pk : -1.0 / (1.0 - (double)pk);
+        const double v = (double)acc.w * sc;
+        const int idx = acc.base + sb;
+        if (acc.in_smem) atomicAdd(&acc.sh[idx], v);
+        else atomicAdd(&acc.gl[idx], v);
+      }
+    }
+    if (u0 <= C0.w) {
+      if (u1 <= thr) {
+        transmitted = true;
+      } else {
+        const float k2 = 2.0f * dn0;
+        dx = fmaf(-k2, nx, dx);
+        dy = fmaf(-k2, ny, dy);
+        dz = fmaf(-k2, nz, dz);
+        const float inv = rsqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+        dx *= inv; dy *= inv; dz *= inv;
+      }
+    } else {
+      const float sint = sqrt_approx(u1);
+      const float cost = sqrt_approx(fmaxf(0.0f, 1.0f - u1));
+      float sp, cp;
+      sincos2pi(u2, &sp, &cp);
+      const float a = sint * cp, b = sint * sp;
+      const float vx = fmaf(ax1, a, fmaf(ax2, b, nx * cost));
+      const float vy = fmaf(ay1, a, fmaf(ay2, b, ny * cost));
+      const float vz = fmaf(az1, a, fmaf(az2, b, nz * cost));
+      /* Lambertian into the incidence side, then optionally through */
+      const float s = on * fmaf(vx, nx, fmaf(vy, ny, vz * nz));
+      float sg = s > 0.0f ? -1.0f : 1.0f;
+      if (u3 <= thr) { sg = -sg; transmitted = true; }
+      dx = sg * vx; dy = sg * vy; dz = sg * vz;
+    }
+    if (transmitted) {
+      grain = meta >> 8;
+      gr2 = 0.0f;
+      g2r2 = 0.0f;
+    }
+    last_geom = B.w;
+  }
+  /* a free path used up at the surface: a new one */
+  if (end_side < 0 && fp < 1.0e-10f) {
+    const uint4 R2 = philox10(flight, c1 | 1u, slo, shi, key);
+    fp = -lam * __logf(u23f(R2.y));
+  }
+  return end_side;
+}
+
 /* Trace replay: position after flight f of the sample in replay-list slot t
    (f = 0: the emission point), when the host gave a position buffer. */
 __device__ __forceinline__ void trace_put(const RunF32& r, long long t, unsigned f, float px,
@@ -681,8 +830,9 @@ __device__ bool stage_blob(const float4* gblob, float4* sblob, int units, int* e
 constexpr int kAdjSmemDoubles = 2048;
 
 /* rounds of 32 flights one cooperative visit may take before the phonon's
-   lane returns to the refill / tally step */
-constexpr int kCoopRounds = 32;
+   lane returns to the refill / tally step (a visit also ends where the
+   phonon reaches a bath face, is lost or reaches the flight cap) */
+constexpr int kCoopRounds = 256;
 /* floats between the rows of a warp's cooperative-round block */
 constexpr int kRowStride = 36;
 /* flights a round tests from its first flight outside the safe ball, in a
@@ -1016,8 +1166,11 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
        intersection test of its own flight unless the flight stays in the
        safe ball.  The first flight that hits a surface, leaves the box or
        reaches the cap ends the round; the flights before it are p-p events.
-       The hit flight's Philox block and nearest surface are handed to the
-       phonon's lane, which processes the event below. */
+       A surface or side-face event is taken by the whole warp
+       (surface_hit) and the rounds go on from it; at a bath face (and in
+       the adjoint replay at any surface) the hit flight's Philox block and
+       nearest surface are handed to the phonon's lane, which processes the
+       event below. */
     bool coop = false;       /* this lane was advanced cooperatively          */
     bool pre = false;        /* ... up to a surface hit: preR / pre_tb / pre_sb */
     bool skip_full = false;  /* ... up to the round limit: no event this pass  */
@@ -1053,7 +1206,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           const float clam = s1.w;
           uint32_t cfl = __float_as_uint(s4.z);
           const uint32_t cslo = __float_as_uint(s4.x), cshi = __float_as_uint(s4.y);
-          const int cgrain = __float_as_int(s3.x);
+          int cgrain = __float_as_int(s3.x);
           int clast = __float_as_int(s3.y);
           /* the phonon's safe ball: flights ending inside it skip the test */
           float cbx = s2.x, cby = s2.y, cbz = s2.z, cbr2 = s2.w, cgr2 = s4.w;
@@ -1197,6 +1350,22 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
                 sR.z = __shfl_sync(FULL, R.z, j); sR.w = __shfl_sync(FULL, R.w, j);
                 stb = __shfl_sync(FULL, tb, j);
                 ssb = __shfl_sync(FULL, sb, j);
+                if (MODE != MODE_ADJOINT && ssb > 1) {
+                  /* a surface or a side face, not a bath: every lane takes
+                     the event (the same inputs, the same result) and the
+                     rounds go on from it; a bath face ends the visit */
+                  ++cfl;
+                  ++ctaken;
+                  const AdjAcc none{nullptr, nullptr, 0.0f, 0, false};
+                  surface_hit<MODE, EXT>(G, stb, ssb, u23f(sR.x), u23f(sR.y), u23f(sR.z),
+                                         u23f(sR.w), Y, Z, pmask, nmat, s3.w, clam, cfl, c1, cslo,
+                                         cshi, key, none, cpx, cpy, cpz, cdx, cdy, cdz, cfp, cgrain,
+                                         cgr2, cg2r2, clast);
+                  cbr2 = 0.0f;
+                  stop = 0;
+                  Rnext = philox10(cfl + 1u + (uint32_t)lane, c1, cslo, cshi, key);
+                  continue;
+                }
               }
               break;
             }
@@ -1357,8 +1526,11 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           const float fe2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
           const float fs2 = fmaf(sx, sx, fmaf(sy, sy, sz * sz));
           const bool in_gball = fe2 < gr2 && fs2 < gr2;
+          /* the second ball pays here where the grains' scans walk BVHs or
+             test capped cylinders; in a grain of a few plain surfaces its
+             extra branch costs more than it saves */
           if (grain > 0 && !in_gball) {
-            if (fe2 < g2r2 && fs2 < g2r2)
+            if (EXT && fe2 < g2r2 && fs2 < g2r2)
               test_near<EXT>(G, gnear, px, py, pz, dx, dy, dz, last_geom, eps, Z, tb, sb,
                              my_surf_tests);
             else
@@ -1403,122 +1575,12 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
               }
             }
           } else {
-            br2 = 0.0f;
             if (MODE == MODE_ADJOINT) adj_len += tb;
-            px = fmaf(tb, dx, px);
-            py = fmaf(tb, dy, py);
-            pz = fmaf(tb, dz, pz);
-            fp -= tb;
-            if (sb == 0) {
-              end_side = 1;
-            } else if (sb == 1) {
-              end_side = 2;
-            } else if (sb < 6 && ((pmask >> sb) & 1)) {
-              const int ax = sb >> 1;
-              const float L = ax == 1 ? Y : Z;
-              const float sg = (sb & 1) ? -L : L;
-              if (ax == 1) py += sg; else pz += sg;
-              last_geom = -1;
-            } else {
-              /* surface event: determinSpecular, reflectSpecular /
-                 reflectDiffusive, determinTransmit (src/RTMCphon.f90:2225-2413) */
-              const float4 C0 = G.cold(sb, 0), C1 = G.cold(sb, 1), C2 = G.cold(sb, 2);
-              const int meta = __float_as_int(C2.w);
-              const int kind = meta & 0xff;
-              float thr = 0.0f;
-              if (kind == 1) {
-                thr = C1.w;
-              } else if (kind == 2 || kind == 3) {
-                if (nmat == 1) {
-                  thr = __frcp_rn(fmaf(C1.w, omr, 1.0f));
-                } else {
-                  const uint4 R2 = philox10(flight, c1 | 1u, slo, shi, key);
-                  const float t11 = __frcp_rn(C1.w + 1.0f);
-                  thr = fmaf(u23f(R2.x), 1.0f - t11, t11);
-                }
-              }
-              /* surface normal at the hit point and surface frame */
-              float nx, ny, nz, ax1, ay1, az1, ax2, ay2, az2;
-              const int4 B = G.hotB(sb);
-              const int type = B.x & 0xff;
-              if (type == REC_POLY) {
-                nx = C2.x; ny = C2.y; nz = C2.z;
-                ax1 = C0.x; ay1 = C0.y; az1 = C0.z;
-                ax2 = C1.x; ay2 = C1.y; az2 = C1.z;
-              } else {
-                const float4 A = G.hotA(sb);
-                if (EXT && type == REC_CAP) {
-                  capped_normal(A, G.edge(B.y), px, py, pz, nx, ny, nz);
-                } else {
-                  float rx = px - A.x, ry = py - A.y, rz = (type == REC_SPHERE) ? pz - A.z : 0.0f;
-                  const float inv = rsqrtf(fmaf(rx, rx, fmaf(ry, ry, rz * rz)));
-                  nx = rx * inv; ny = ry * inv; nz = rz * inv;
-                }
-                const float q2 = fmaf(nx, nx, ny * ny);
-                if (q2 > 1.0e-12f) {
-                  const float q = rsqrtf(q2);
-                  ax2 = -ny * q; ay2 = nx * q; az2 = 0.0f;
-                  /* t1 = t2 x n */
-                  ax1 = ay2 * nz - az2 * ny;
-                  ay1 = az2 * nx - ax2 * nz;
-                  az1 = ax2 * ny - ay2 * nx;
-                } else {
-                  ax2 = 0.0f; ay2 = 1.0f; az2 = 0.0f;
-                  ax1 = 1.0f; ay1 = 0.0f; az1 = 0.0f;
-                }
-              }
-              /* tmpNormal oriented along the incoming direction */
-              const float dn0 = fmaf(nx, dx, fmaf(ny, dy, nz * dz));
-              const float on = dn0 < 0.0f ? -1.0f : 1.0f;
-              bool transmitted = false;
-              if (MODE == MODE_ADJOINT) {
-                /* d log P / d p of the specular (1/p) or diffuse (-1/(1-p)) choice */
-                const float pk = C0.w;
-                if (pk > 0.0f && pk < 1.0f) {
-                  const double sc = (u0 <= pk) ? 1.0 / (double)pk : -1.0 / (1.0 - (double)pk);
-                  const double v = (double)adj_w * sc;
-                  const int idx = adj_off + adj_b * adj_stride + sb;
-                  if (adj_in_smem) atomicAdd(&adj_sh[idx], v);
-                  else atomicAdd(&r.adj[idx], v);
-                }
-              }
-              if (u0 <= C0.w) {
-                if (u1 <= thr) {
-                  transmitted = true;
-                } else {
-                  const float k2 = 2.0f * dn0;
-                  dx = fmaf(-k2, nx, dx);
-                  dy = fmaf(-k2, ny, dy);
-                  dz = fmaf(-k2, nz, dz);
-                  const float inv = rsqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
-                  dx *= inv; dy *= inv; dz *= inv;
-                }
-              } else {
-                const float sint = sqrt_approx(u1);
-                const float cost = sqrt_approx(fmaxf(0.0f, 1.0f - u1));
-                float sp, cp;
-                sincos2pi(u2, &sp, &cp);
-                const float a = sint * cp, b = sint * sp;
-                const float vx = fmaf(ax1, a, fmaf(ax2, b, nx * cost));
-                const float vy = fmaf(ay1, a, fmaf(ay2, b, ny * cost));
-                const float vz = fmaf(az1, a, fmaf(az2, b, nz * cost));
-                /* Lambertian into the incidence side, then optionally through */
-                const float s = on * fmaf(vx, nx, fmaf(vy, ny, vz * nz));
-                float sg = s > 0.0f ? -1.0f : 1.0f;
-                if (u3 <= thr) { sg = -sg; transmitted = true; }
-                dx = sg * vx; dy = sg * vy; dz = sg * vz;
-              }
-              if (transmitted) {
-                grain = meta >> 8;
-                gr2 = 0.0f;
-                g2r2 = 0.0f;
-              }
-              last_geom = B.w;
-            }
-            if (end_side < 0 && fp < 1.0e-10f) {
-              const uint4 R2 = philox10(flight, c1 | 1u, slo, shi, key);
-              fp = -lam * __logf(u23f(R2.y));
-            }
+            const AdjAcc acc{adj_sh, r.adj, adj_w, adj_off + adj_b * adj_stride, adj_in_smem};
+            end_side = surface_hit<MODE, EXT>(G, tb, sb, u0, u1, u2, u3, Y, Z, pmask, nmat, omr, lam,
+                                              flight, c1, slo, shi, key, acc, px, py, pz, dx, dy, dz,
+                                              fp, grain, gr2, g2r2, last_geom);
+            br2 = 0.0f;
           }
           if (MODE == MODE_TRACE) trace_put(r, tslot, flight, px, py, pz);
         }
