@@ -188,6 +188,25 @@ __device__ __forceinline__ bool closer(float t, int s, float tr, int sr) {
   return t < tr || (t == tr && s < sr);
 }
 
+/* Polygon s with plane A (unit normal A.xyz along the side it is hit from,
+   offset A.w): the ray's crossing of the plane, in front (within eps) and
+   nearer than (tr, sb), and inside the edges; the edges are read only for a
+   crossing that passes the rest. */
+template <class G_t>
+__device__ __forceinline__ void poly_test(const G_t& G, int s, float4 A, float px, float py,
+                                          float pz, float dx, float dy, float dz, float eps,
+                                          float& tr, int& sb) {
+  const float cosa = fmaf(A.x, dx, fmaf(A.y, dy, A.z * dz));
+  if (cosa <= 0.0f) return;
+  const float t = __fdividef(A.w - fmaf(A.x, px, fmaf(A.y, py, A.z * pz)), cosa);
+  if (!(t >= -eps) || !closer(t, s, tr, sb)) return;
+  const int4 B = G.hotB(s);
+  const float hx = fmaf(t, dx, px), hy = fmaf(t, dy, py), hz = fmaf(t, dz, pz);
+  if (!inside_edges(G, B.y, B.z, hx, hy, hz, eps)) return;
+  tr = t;
+  sb = s;
+}
+
 /* Capped cylinder (centre A.xyz, radius A.w; unit axis E.xyz, half length
    E.w) against the ray p + t d.  From inside (interior record) the exit:
    the mantle's far root when its axial coordinate lies within the caps, or
@@ -271,14 +290,7 @@ __device__ __forceinline__ void test_surface(const G_t& G, int s, float px, floa
   if (EXT && type == REC_CAP) {
     capped_test(G, s, A, B, px, py, pz, dx, dy, dz, last_geom, eps, tr, sb);
   } else if (type == REC_POLY) {
-    const float cosa = fmaf(A.x, dx, fmaf(A.y, dy, A.z * dz));
-    if (cosa <= 0.0f) return;
-    const float t = __fdividef(A.w - fmaf(A.x, px, fmaf(A.y, py, A.z * pz)), cosa);
-    if (!(t >= -eps) || !closer(t, s, tr, sb)) return;
-    const float hx = fmaf(t, dx, px), hy = fmaf(t, dy, py), hz = fmaf(t, dz, pz);
-    if (!inside_edges(G, B.y, B.z, hx, hy, hz, eps)) return;
-    tr = t;
-    sb = s;
+    poly_test(G, s, A, px, py, pz, dx, dy, dz, eps, tr, sb);
   } else {
     /* sphere or z cylinder, written with selects: the lanes of a warp test
        the same surface with different rays, so the only branch is the one
@@ -582,6 +594,168 @@ __device__ __forceinline__ void test_near(const G_t& G, int s, float px, float p
   tb = fmaxf(tr, 0.0f);
 }
 
+/* Local candidate list of the tail phase's rounds in a BVH grain: the
+   surfaces of one grain whose bound from a centre c is below a radius R,
+   at most kList of them, one per lane.  A flight that starts and ends
+   within R - 4 eps of c can meet only listed surfaces, and the safe ball of
+   a point p within that radius follows from the listed bounds and
+   R - |p - c|, so while the walk stays near c neither needs the tree. */
+constexpr int kList = 32;
+/* radius of a new list, in units of the MFP (the safe ball's cap) */
+constexpr float kListMfp = 32.0f;
+
+/* Largest v over the warp and the lowest lane holding it. */
+__device__ __forceinline__ void warp_argmax(float v, int lane, float& vmax, int& lmax) {
+  int l = lane;
+  for (int o = 16; o > 0; o >>= 1) {
+    const float ov = __shfl_xor_sync(FULL, v, o);
+    const int ol = __shfl_xor_sync(FULL, l, o);
+    const bool other = ov > v || (ov == v && ol < l);
+    v = other ? ov : v;
+    l = other ? ol : l;
+  }
+  vmax = v;
+  lmax = l;
+}
+
+/* BVH range query for a local list: the surfaces of the grain whose bound
+   from p (as in safety_bvh) is below R, kList at most: lane k holds entry
+   k while the tree is searched; once the list is full a nearer surface
+   replaces the one with the largest bound, and R drops to the bound of
+   whatever leaves the list.  Returns the final R (every surface missing
+   from the list has a bound of at least R from p) and stores the entries
+   to lst and their planes (hotA) to lpl; allpoly tells whether every entry
+   is a polygon.  Warp-collective: every lane searches the same nodes. */
+template <bool EXT, class G_t>
+__device__ __noinline__ float list_bvh(const G_t& G, int root, float px, float py, float pz,
+                                       float R, int lane, int* lst, float4* lpl, int& n,
+                                       int& allpoly) {
+  int stk[kBvhStack];
+  float std_[kBvhStack];
+  int sp = 0;
+  int node = root;
+  int my_s = -1;
+  float my_e = -1.0f;
+  float emax = 3.0e38f;
+  int lmax = 0;
+  n = 0;
+  while (true) {
+    const float4 n0 = G.node(2 * node), n1 = G.node(2 * node + 1);
+    const int cnt = __float_as_int(n1.w);
+    const int a = __float_as_int(n0.w);
+    bool descended = false;
+    if (cnt > 0) {
+      const float bd = box_dist(n0, n1, px, py, pz);
+      for (int k = a; k < a + cnt; ++k) {
+        const int sk = G.cand(k);
+        const float e = fmaxf(bd, surface_lb<EXT>(G, sk, px, py, pz));
+        if (e < R) {
+          if (n < kList) {
+            if (lane == n) { my_s = sk; my_e = e; }
+            if (++n == kList) warp_argmax(my_e, lane, emax, lmax);
+          } else if (e < emax) {
+            R = fminf(R, emax);
+            if (lane == lmax) { my_s = sk; my_e = e; }
+            warp_argmax(my_e, lane, emax, lmax);
+          } else {
+            R = e;
+          }
+        }
+      }
+    } else {
+      const float dl = box_dist(G.node(2 * a), G.node(2 * a + 1), px, py, pz);
+      const float dg = box_dist(G.node(2 * a + 2), G.node(2 * a + 3), px, py, pz);
+      const bool lf = dl <= dg;
+      const float dn = lf ? dl : dg, df = lf ? dg : dl;
+      if (dn < R) {
+        if (df < R && sp < kBvhStack) {
+          stk[sp] = lf ? a + 1 : a;
+          std_[sp] = df;
+          ++sp;
+        }
+        node = lf ? a : a + 1;
+        descended = true;
+      }
+    }
+    if (descended) continue;
+    bool found = false;
+    while (sp > 0) {
+      --sp;
+      if (std_[sp] < R) {
+        node = stk[sp];
+        found = true;
+        break;
+      }
+    }
+    if (!found) break;
+  }
+  bool poly = true;
+  if (lane < n) {
+    lst[lane] = my_s;
+    lpl[lane] = G.hotA(my_s);
+    poly = (G.hotB(my_s).x & 0xff) == REC_POLY;
+  }
+  allpoly = __all_sync(FULL, poly) ? 1 : 0;
+  return R;
+}
+
+/* safety() for a point p within the radius lc.w of a local list's centre
+   lc.xyz: the listed surfaces' bounds (lane k takes entry k) and
+   lc.w - |p - c| for every other surface of the grain.  Warp-collective. */
+template <bool EXT, class G_t>
+__device__ __forceinline__ float safety_list(const G_t& G, const int* lst, int n, float4 lc,
+                                             float px, float py, float pz, float X, float Y,
+                                             float Z, float eps, int lane, float& dgrain,
+                                             float& dgrain2, int& near) {
+  const float dbox = fminf(fminf(fminf(px, X - px), fminf(py, Y - py)), fminf(pz, Z - pz));
+  float e = 3.0e38f, e2 = 3.0e38f;
+  int s = -1;
+  if (lane < n) {
+    s = lst[lane];
+    e = surface_lb<EXT>(G, s, px, py, pz);
+  }
+  /* the smallest bound, its surface and the second smallest */
+  for (int o = 16; o > 0; o >>= 1) {
+    const float oe = __shfl_xor_sync(FULL, e, o), oe2 = __shfl_xor_sync(FULL, e2, o);
+    const int os = __shfl_xor_sync(FULL, s, o);
+    const bool other = oe < e || (oe == e && os < s);
+    e2 = other ? fminf(e, oe2) : fminf(oe, e2);
+    e = other ? oe : e;
+    s = other ? os : s;
+  }
+  const float wx = px - lc.x, wy = py - lc.y, wz = pz - lc.z;
+  const float du = lc.w - sqrt_approx(fmaf(wx, wx, fmaf(wy, wy, wz * wz)));
+  near = e < du ? s : -1;
+  const float dc = fminf(e, du);
+  dgrain = dc - 4.0f * eps;
+  dgrain2 = (near >= 0 ? fminf(e2, du) : dc) - 4.0f * eps;
+  return fminf(dbox, dc) - 4.0f * eps;
+}
+
+/* scan_grain over a local list, for a flight within its radius: the listed
+   surfaces are the only ones the flight can meet.  A hit beyond the free
+   path cannot end the flight, so the search stops at the float above fp:
+   the nearest hit up to fp is the full scan's, and without one tb stays
+   above fp, as it would. */
+template <bool EXT, class G_t>
+__device__ __forceinline__ void scan_list(const G_t& G, const int* lst, const float4* lpl, int n,
+                                          bool allpoly, float px, float py, float pz, float dx,
+                                          float dy, float dz, int last_geom, float eps,
+                                          float zmax, float fp, float& tb, int& sb,
+                                          unsigned& nsurf) {
+  float tr = fminf(tb, __uint_as_float(__float_as_uint(fp) + 1u));
+  nsurf += (unsigned)n;
+  if (allpoly) {
+    /* polygons only: the planes come from the list's shared-memory copy,
+       the edges only for a crossing in front of the ray and in range */
+    for (int k = 0; k < n; ++k) poly_test(G, lst[k], lpl[k], px, py, pz, dx, dy, dz, eps, tr, sb);
+  } else {
+    for (int k = 0; k < n; ++k)
+      test_surface<EXT>(G, lst[k], px, py, pz, dx, dy, dz, last_geom, eps, zmax, tr, sb);
+  }
+  tb = fmaxf(tr, 0.0f);
+}
+
 /* Adjoint accumulators of the sample: dlogP/dp of surface k goes to
    base + k, in shared memory (sh) when the block holds them, else global. */
 struct AdjAcc {
@@ -742,6 +916,20 @@ __device__ __forceinline__ void trace_put(const RunF32& r, long long t, unsigned
   r.trace[3 * at + 2] = pz;
 }
 
+/* The Philox blocks of flights f+1+s+lane, s in [0, 32], from those of
+   f+1+lane (cur) and f+33+lane (nxt) held across the warp: a round that
+   advances s flights passes the blocks it drew on instead of drawing them
+   again (the blocks depend on the flight counter alone). */
+__device__ __forceinline__ uint4 rotate_blocks(uint4 cur, uint4 nxt, int s, int lane) {
+  const int src = (lane + s) & 31;
+  const bool fc = lane + s < 32;
+  const unsigned a0 = __shfl_sync(FULL, cur.x, src), b0 = __shfl_sync(FULL, nxt.x, src);
+  const unsigned a1 = __shfl_sync(FULL, cur.y, src), b1 = __shfl_sync(FULL, nxt.y, src);
+  const unsigned a2 = __shfl_sync(FULL, cur.z, src), b2 = __shfl_sync(FULL, nxt.z, src);
+  const unsigned a3 = __shfl_sync(FULL, cur.w, src), b3 = __shfl_sync(FULL, nxt.w, src);
+  return make_uint4(fc ? a0 : b0, fc ? a1 : b1, fc ? a2 : b2, fc ? a3 : b3);
+}
+
 __device__ __forceinline__ unsigned lanemask_lt() {
   unsigned m;
   asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
@@ -894,6 +1082,18 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   /* ... and six rows where the lanes' own phonons wait during the rounds */
   __shared__ float4 coop_park[PH == PH_TAIL ? kBlock / 32 : 1][6][32];
   float4 (*const park)[32] = coop_park[PH == PH_TAIL ? (threadIdx.x >> 5) : 0];
+  /* ... and, in kernels built for BVH grains, the warp's local candidate
+     list: its entries, its centre and radius, and (count, grain); not in
+     the adjoint replay, whose shared accumulators leave no room */
+  constexpr bool kUseList = PH == PH_TAIL && EXT && MODE != MODE_ADJOINT;
+  constexpr int kLW = kUseList ? kBlock / 32 : 1;
+  __shared__ int coop_list[kLW][kList];
+  __shared__ float4 coop_lplane[kLW][kList];
+  __shared__ float4 coop_lball[kLW];
+  __shared__ int4 coop_lmeta[kLW];  /* count, grain, every entry a polygon */
+  int* const lst = coop_list[kLW > 1 ? (threadIdx.x >> 5) : 0];
+  float4* const lpl = coop_lplane[kLW > 1 ? (threadIdx.x >> 5) : 0];
+  if (kUseList && lane == 0) coop_lmeta[threadIdx.x >> 5] = make_int4(0, -1, 0, 0);
   /* tail phase: phonons the drain left (the counts are final at launch),
      long ones from the front of the list, the others from the back */
   const int nlong = PH == PH_TAIL ? min(r.queue[2], r.tail_cap) : 0;
@@ -1220,7 +1420,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
           int ssb = -1;
           /* the blocks of the next round are drawn while this one runs,
              assuming it advances all 32 flights (counters alone fix them);
-             a round that advances fewer draws them again */
+             a round that advances fewer passes the ones it has on
+             (rotate_blocks) */
           uint4 Rnext = philox10(cfl + 1u + (uint32_t)lane, c1, cslo, cshi, key);
           for (int round = 0; round < max_rounds; ++round) {
             ++crounds;
@@ -1311,8 +1512,27 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
                ball only they and the grain's nearest candidate */
             const bool in_gball = de2 < cgr2 && ds2 < cgr2;
             const bool in_g2 = de2 < cg2r2 && ds2 < cg2r2;
-            const unsigned outm = __ballot_sync(FULL, !in_ball);
-            const int jw = (EXT && outm) ? min(32, __ffs(outm) - 1 + kTestWindow) : 32;
+            /* ... and within the local list's radius only the listed ones */
+            bool in_list = false, lpoly = false;
+            int ln = 0;
+            if (kUseList) {
+              const int4 lm = coop_lmeta[threadIdx.x >> 5];
+              const float4 lc = coop_lball[threadIdx.x >> 5];
+              const float ru = lc.w - 4.0f * eps;
+              lpoly = lm.z != 0;
+              const float lx = fmaf(sfp, sdx, qx) - lc.x, ly = fmaf(sfp, sdy, qy) - lc.y;
+              const float lz = fmaf(sfp, sdz, qz) - lc.z;
+              const float mx = qx - lc.x, my = qy - lc.y, mz = qz - lc.z;
+              ln = lm.x;
+              in_list = lm.y == cgrain && ru > 0.0f &&
+                        fmaf(lx, lx, fmaf(ly, ly, lz * lz)) < ru * ru &&
+                        fmaf(mx, mx, fmaf(my, my, mz * mz)) < ru * ru;
+            }
+            /* in kernels built for BVH grains a round tests at most
+               kTestWindow flights from its first one that needs the whole
+               grain's search */
+            const unsigned needm = __ballot_sync(FULL, !in_ball && !in_gball && !in_g2 && !in_list);
+            const int jw = (EXT && needm) ? min(32, __ffs(needm) - 1 + kTestWindow) : 32;
             float tb = 3.0e38f;
             int sb = -1;
             if (!in_ball && lane < jw) {
@@ -1321,6 +1541,9 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
                 if (in_g2)
                   test_near<EXT>(G, cnear, qx, qy, qz, sdx, sdy, sdz, lane == 0 ? clast : -1, eps, Z,
                                  tb, sb, my_surf_tests);
+                else if (kUseList && in_list)
+                  scan_list<EXT>(G, lst, lpl, ln, lpoly, qx, qy, qz, sdx, sdy, sdz,
+                                 lane == 0 ? clast : -1, eps, Z, sfp, tb, sb, my_surf_tests);
                 else
                   scan_grain<EXT>(G, cgrain, qx, qy, qz, sdx, sdy, sdz, lane == 0 ? clast : -1, eps,
                                   Z, sfp, tb, sb, my_box_tests, my_surf_tests);
@@ -1363,7 +1586,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
                                          cgr2, cg2r2, clast);
                   cbr2 = 0.0f;
                   stop = 0;
-                  Rnext = philox10(cfl + 1u + (uint32_t)lane, c1, cslo, cshi, key);
+                  Rnext = rotate_blocks(R, Rnext, j + 1, lane);
                   continue;
                 }
               }
@@ -1385,12 +1608,48 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
               cdz = __shfl_sync(FULL, nz, 31); cfp = __shfl_sync(FULL, nf, 31);
             }
             cfl += (uint32_t)j;
-            if (j != 32) Rnext = philox10(cfl + 1u + (uint32_t)lane, c1, cslo, cshi, key);
+            if (j != 32) Rnext = rotate_blocks(R, Rnext, j, lane);
             /* a new ball where the walk left the old one */
             if (!__shfl_sync(FULL, in_ball, j - 1) && r.fast_steps > 0) {
-              float dg, dg2;
-              const float d = safety<EXT>(G, cgrain, cpx, cpy, cpz, X, Y, Z, eps,
-                                          kBallCapMfp * clam, dg, dg2, cnear);
+              float dg, dg2, d;
+              if (kUseList && cgrain > 0 && G.bvh_root(cgrain) >= 0) {
+                /* from the local list, built anew (one tree search) when the
+                   point is past half its radius or in another grain */
+                const int4 lm = coop_lmeta[threadIdx.x >> 5];
+                const float4 lc = coop_lball[threadIdx.x >> 5];
+                bool fresh = lm.y != cgrain;
+                if (!fresh) {
+                  d = safety_list<EXT>(G, lst, lm.x, lc, cpx, cpy, cpz, X, Y, Z, eps, lane, dg, dg2,
+                                       cnear);
+                  /* a ball bounded by the list's edge, not by a listed
+                     surface, and short of half the search radius: a new
+                     list about this point */
+                  const float wx = cpx - lc.x, wy = cpy - lc.y, wz = cpz - lc.z;
+                  const float du = lc.w - sqrt_approx(fmaf(wx, wx, fmaf(wy, wy, wz * wz)));
+                  fresh = cnear < 0 && du < 0.5f * kListMfp * clam;
+                }
+                if (fresh) {
+                  /* the search radius: kListMfp MFPs, or a quarter more than
+                     the last list's if that one filled up in this grain
+                     (fewer replacements in a dense grain) */
+                  const float rt = kListMfp * clam;
+                  const float r0 = (lm.y == cgrain && lm.x == kList) ? fminf(rt, 1.25f * lc.w) : rt;
+                  int n, ap;
+                  const float R = list_bvh<EXT>(G, G.bvh_root(cgrain), cpx, cpy, cpz, r0, lane, lst,
+                                                lpl, n, ap);
+                  const float4 nc = make_float4(cpx, cpy, cpz, R);
+                  if (lane == 0) {
+                    coop_lball[threadIdx.x >> 5] = nc;
+                    coop_lmeta[threadIdx.x >> 5] = make_int4(n, cgrain, ap, 0);
+                  }
+                  __syncwarp();
+                  d = safety_list<EXT>(G, lst, n, nc, cpx, cpy, cpz, X, Y, Z, eps, lane, dg, dg2,
+                                       cnear);
+                }
+              } else {
+                d = safety<EXT>(G, cgrain, cpx, cpy, cpz, X, Y, Z, eps, kBallCapMfp * clam, dg, dg2,
+                                cnear);
+              }
               cbx = cpx; cby = cpy; cbz = cpz;
               cbr2 = d > 0.0f ? d * d : 0.0f;
               cgr2 = dg > 0.0f ? dg * dg : 0.0f;
@@ -1812,8 +2071,13 @@ cudaError_t launch_persistent_fp32(const GeoF32& g, const RunF32& r, int grid, i
 cudaError_t launch_tail_fp32(const GeoF32& g, const RunF32& r, int grid, int block, size_t smem,
                              cudaStream_t st, int mode) {
   if (block > kBlock || block % 32) return cudaErrorInvalidConfiguration;
-  return g.has_ext ? launch_bvh<true, PH_TAIL>(g, r, grid, block, smem, st, mode)
-                   : launch_bvh<false, PH_TAIL>(g, r, grid, block, smem, st, mode);
+  /* the tail phase reads its BVH nodes through L1 without staging the tree
+     tops: its few live warps keep the nodes they walk in L1, and the staged
+     copy would take that L1 from them */
+  GeoF32 gt = g;
+  gt.node_stage = 0;
+  return g.has_ext ? launch_bvh<true, PH_TAIL>(gt, r, grid, block, smem, st, mode)
+                   : launch_bvh<false, PH_TAIL>(gt, r, grid, block, smem, st, mode);
 }
 
 namespace {
