@@ -930,6 +930,35 @@ __device__ __forceinline__ uint4 rotate_blocks(uint4 cur, uint4 nxt, int s, int 
   return make_uint4(fc ? a0 : b0, fc ? a1 : b1, fc ? a2 : b2, fc ? a3 : b3);
 }
 
+/* Direction and free path after a p-p event, from the event flight's Philox
+   block (createRandomDirectionAllSphere, createRandomFreePath). */
+__device__ __forceinline__ void pp_dir(uint4 R, float lam, float& nx, float& ny, float& nz,
+                                       float& nf) {
+  const float ct = fmaf(u23f(R.x), 2.0f, -1.0f);
+  const float st = sqrt_approx(fmaxf(0.0f, fmaf(-ct, ct, 1.0f)));
+  float sp, cp;
+  sincos2pi(u23f(R.y), &sp, &cp);
+  nx = ct; ny = st * cp; nz = st * sp;
+  nf = -lam * __logf(u23f(R.z));
+}
+/* rotate_blocks for the (free path, direction) a round's lanes drew from
+   their blocks: those of this round sit in its rows (flight j at index
+   j + 1, RS floats apart), those of the next one in (f2, x2, y2, z2). */
+template <int RS>
+__device__ __forceinline__ void rotate_dirs(const float* frow, int s, int lane, float f2,
+                                            float x2, float y2, float z2, float& f, float& x,
+                                            float& y, float& z) {
+  const int src = lane + s;
+  const int sl = src & 31;
+  const float a0 = __shfl_sync(FULL, f2, sl), a1 = __shfl_sync(FULL, x2, sl);
+  const float a2 = __shfl_sync(FULL, y2, sl), a3 = __shfl_sync(FULL, z2, sl);
+  const bool cur = src < 32;
+  const int ri = cur ? src + 1 : 0;
+  const float r0 = frow[ri], r1 = frow[RS + ri];
+  const float r2 = frow[2 * RS + ri], r3 = frow[3 * RS + ri];
+  f = cur ? r0 : a0; x = cur ? r1 : a1; y = cur ? r2 : a2; z = cur ? r3 : a3;
+}
+
 __device__ __forceinline__ unsigned lanemask_lt() {
   unsigned m;
   asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
@@ -1423,17 +1452,16 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
              a round that advances fewer passes the ones it has on
              (rotate_blocks) */
           uint4 Rnext = philox10(cfl + 1u + (uint32_t)lane, c1, cslo, cshi, key);
+          /* ... and so are the directions and free paths they give, which
+             the round writes to its rows without waiting for them */
+          float nx, ny, nz, nf;
+          pp_dir(Rnext, clam, nx, ny, nz, nf);
           for (int round = 0; round < max_rounds; ++round) {
             ++crounds;
             const uint4 R = Rnext;
             Rnext = philox10(cfl + 33u + (uint32_t)lane, c1, cslo, cshi, key);
-            /* direction and free path after a p-p event ending flight `lane` */
-            const float ct = fmaf(u23f(R.x), 2.0f, -1.0f);
-            const float st = sqrt_approx(fmaxf(0.0f, fmaf(-ct, ct, 1.0f)));
-            float sp, cp;
-            sincos2pi(u23f(R.y), &sp, &cp);
-            const float nx = ct, ny = st * cp, nz = st * sp;
-            const float nf = -clam * __logf(u23f(R.z));
+            float nx2, ny2, nz2, nf2;
+            pp_dir(Rnext, clam, nx2, ny2, nz2, nf2);
             /* flight `lane` starts with the state the previous flight drew:
                the rows hold the (free path, direction) of the round's 32
                flights.  The start point of flight j is the chain p,
@@ -1442,12 +1470,11 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
                loads, four fmas and one 4-wide store of the chain per four
                flights) and every lane then reads its own start point */
             float* const frow = crow;
-            if (lane < 31) {
-              frow[lane + 1] = nf;
-              frow[kRowStride + lane + 1] = nx;
-              frow[2 * kRowStride + lane + 1] = ny;
-              frow[3 * kRowStride + lane + 1] = nz;
-            }
+            /* (lane 31's entry, index 32, serves rotate_dirs) */
+            frow[lane + 1] = nf;
+            frow[kRowStride + lane + 1] = nx;
+            frow[2 * kRowStride + lane + 1] = ny;
+            frow[3 * kRowStride + lane + 1] = nz;
             if (lane == 0) {
               frow[0] = cfp;
               frow[kRowStride] = cdx;
@@ -1587,6 +1614,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
                   cbr2 = 0.0f;
                   stop = 0;
                   Rnext = rotate_blocks(R, Rnext, j + 1, lane);
+                  rotate_dirs<kRowStride>(frow, j + 1, lane, nf2, nx2, ny2, nz2, nf, nx, ny, nz);
                   continue;
                 }
               }
@@ -1608,13 +1636,21 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
               cdz = __shfl_sync(FULL, nz, 31); cfp = __shfl_sync(FULL, nf, 31);
             }
             cfl += (uint32_t)j;
-            if (j != 32) Rnext = rotate_blocks(R, Rnext, j, lane);
-            /* a new ball where the walk left the old one */
-            if (!__shfl_sync(FULL, in_ball, j - 1) && r.fast_steps > 0) {
+            if (j != 32) {
+              Rnext = rotate_blocks(R, Rnext, j, lane);
+              rotate_dirs<kRowStride>(frow, j, lane, nf2, nx2, ny2, nz2, nf, nx, ny, nz);
+            } else {
+              nf = nf2; nx = nx2; ny = ny2; nz = nz2;
+            }
+            /* a new ball where the walk left the grain ball: while it stays
+               in the grain ball only the box faces can be hit, and a slab
+               test per flight costs less than renewing the safe ball each
+               time the walk leaves it (the old safe ball stays valid) */
+            if (!__shfl_sync(FULL, in_gball, j - 1) && r.fast_steps > 0) {
               float dg, dg2, d;
               if (kUseList && cgrain > 0 && G.bvh_root(cgrain) >= 0) {
-                /* from the local list, built anew (one tree search) when the
-                   point is past half its radius or in another grain */
+                /* from the local list, built anew (one tree search) in
+                   another grain or where the list's edge bounds the ball */
                 const int4 lm = coop_lmeta[threadIdx.x >> 5];
                 const float4 lc = coop_lball[threadIdx.x >> 5];
                 bool fresh = lm.y != cgrain;
