@@ -269,7 +269,8 @@ typedef struct ptg_stats {
   uint64_t surface_tests;   /* FP32 kernel: grain surfaces tested (box faces    */
                             /*   are one slab test and not counted)             */
   double drain_kernel_ms;   /* FP32: CUDA-event time of the drain-phase kernel  */
-  double tail_kernel_ms;    /* FP32: CUDA-event time of the tail-phase kernel   */
+  double tail_kernel_ms;    /* FP32: CUDA-event time of the tail phase (its
+                               ordering kernel and the tail-phase kernel)      */
                             /*   (0 when the tail phase is off)                 */
   uint64_t tail_phonons;    /* FP32: phonons the drain phase handed over        */
   uint64_t tail_flights;    /* FP32: free flights taken in the tail phase       */

@@ -677,9 +677,11 @@ int run_transport(ptg_handle* h, const Transport& T) {
        dry), so the drain grid's lanes bound the tail list */
     const bool tail = r.coop_lanes > 0 && T.mode != ptg::MODE_TRACE;
     if (tail) {
-      CU(h->tail.ensure(sizeof(float4) * ptg::kTailUnits * (size_t)grid * block));
+      /* the list, then the order the tail phase takes it in */
+      CU(h->tail.ensure((sizeof(float4) * ptg::kTailUnits + sizeof(int)) * (size_t)grid * block));
       r.tail = h->tail.as<float4>();
       r.tail_cap = grid * block;
+      r.tail_order = reinterpret_cast<int*>(r.tail + (size_t)ptg::kTailUnits * r.tail_cap);
     }
     int tgrid = 0;
     if (tail) {
@@ -692,12 +694,15 @@ int run_transport(ptg_handle* h, const Transport& T) {
     if (work) {
       CU(ptg::launch_persistent_fp32(h->g32, r, grid, block, smem, h->stream, T.mode));
       CU(cudaEventRecord(h->ev[4], h->stream));
-      if (tail) CU(ptg::launch_tail_fp32(h->g32, r, tgrid, block, smem, h->stream, T.mode));
+      if (tail) {
+        CU(ptg::launch_tail_order(r, h->g32.box[0], h->stream));
+        CU(ptg::launch_tail_fp32(h->g32, r, tgrid, block, smem, h->stream, T.mode));
+      }
     }
     CU(cudaEventRecord(h->ev[1], h->stream));
     h->last.grid = grid;
     h->last.block = block;
-    h->last.launches = (work ? (tail ? 2 : 1) : 0) + (r.nchunk > 0 ? 1 : 0);
+    h->last.launches = (work ? (tail ? 3 : 1) : 0) + (r.nchunk > 0 ? 1 : 0);
     h->fp32_split = work;
     h->tail_cap = tail ? r.tail_cap : 0;
   }

@@ -140,6 +140,8 @@ struct RunF32 {
                                  advances it 32 flights a round (0: off)          */
   float4* tail;               /* tail list: kTailUnits float4 per phonon           */
   int32_t tail_cap;           /* its capacity in phonons                           */
+  int32_t* tail_order;        /* the tail phase takes list slots in this order
+                                 (launch_tail_order), else front then back         */
   int32_t stage_test;         /* test only: set up the shared-memory staging
                                  barrier without issuing the copy, so its
                                  bounded wait runs out (PTG_ERR_TIMEOUT)          */
@@ -198,6 +200,10 @@ cudaError_t launch_persistent_fp32(const GeoF32& g, const RunF32& r, int grid, i
                                    size_t smem, cudaStream_t st, int mode = MODE_FORWARD);
 /* The tail phase after it (forward, list and adjoint modes): the phonons
    the drain phase left in r.tail, one per warp. */
+/* Orders the tail list for the tail phase (r.tail_order, tail_cap ints):
+   longest expected remaining walk first.  One block, between the drain and
+   the tail launch on the same stream; x_len is the box length along x. */
+cudaError_t launch_tail_order(const RunF32& r, float x_len, cudaStream_t st);
 cudaError_t launch_tail_fp32(const GeoF32& g, const RunF32& r, int grid, int block, size_t smem,
                              cudaStream_t st, int mode = MODE_FORWARD);
 cudaError_t tail_occupancy(int block, size_t smem, int* blocks_per_sm, int mode = MODE_FORWARD,

@@ -1175,7 +1175,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
       if (c >= ntail) {
         queue_done = true;
       } else if (lane == 0) {
-        const int slot = c < nlong ? c : r.tail_cap - 1 - (c - nlong);
+        const int slot =
+            r.tail_order ? r.tail_order[c] : (c < nlong ? c : r.tail_cap - 1 - (c - nlong));
         const float4* e = r.tail + (size_t)kTailUnits * slot;
         const float4 e0 = e[0], e1 = e[1], e2 = e[2], e3 = e[3], e4 = e[4];
         px = e0.x; py = e0.y; pz = e0.z; dx = e0.w;
@@ -2129,7 +2130,57 @@ __global__ void k_expand_chunks(const int* __restrict__ order, int norder, int p
     chunks[c] = make_int4(__ldg(order + k), j, min(csz, np_local - j), 0);
   }
 }
+
+/* Buckets of the tail order: a quarter octave of the expected walk each. */
+constexpr int kOrderBuckets = 128;
+
+/* Tail-list slot of hand-over c (front list, then back list) and the
+   bucket of its phonon's expected remaining walk.  A diffusive phonon at x
+   between the baths at 0 and L takes about 1.5 x (L - x) / MFP^2 more
+   flights to leave (the exit time of a random walk whose flights move it
+   by 2 MFP^2 / 3 squared along x); walls and holes stretch the walk, but the
+   phonons the tail phase waits for are those that rank high on it. */
+__device__ __forceinline__ int order_bucket(const float4* tail, int slot, float x_len) {
+  const float4 e0 = tail[(size_t)kTailUnits * slot];
+  const float4 e1 = tail[(size_t)kTailUnits * slot + 1];
+  const float w = fmaxf(e0.x * (x_len - e0.x), 0.0f) / (e1.w * e1.w);
+  return w > 1.0f ? min(kOrderBuckets - 1, (int)(4.0f * __log2f(w))) : 0;
+}
+
+/* One block: a histogram of the buckets, their offsets from the top bucket
+   down, and the slots scattered to their bucket's range. */
+__global__ void k_tail_order(const float4* __restrict__ tail, int tail_cap,
+                             const int* __restrict__ queue, float x_len, int* __restrict__ order) {
+  __shared__ int hist[kOrderBuckets];
+  const int nlong = min(queue[2], tail_cap);
+  const int ntail = nlong + min(queue[4], tail_cap - nlong);
+  for (int b = threadIdx.x; b < kOrderBuckets; b += blockDim.x) hist[b] = 0;
+  __syncthreads();
+  for (int c = threadIdx.x; c < ntail; c += blockDim.x) {
+    const int slot = c < nlong ? c : tail_cap - 1 - (c - nlong);
+    atomicAdd(&hist[order_bucket(tail, slot, x_len)], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int b = kOrderBuckets - 1; b >= 0; --b) {
+      const int h = hist[b];
+      hist[b] = run;
+      run += h;
+    }
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < ntail; c += blockDim.x) {
+    const int slot = c < nlong ? c : tail_cap - 1 - (c - nlong);
+    order[atomicAdd(&hist[order_bucket(tail, slot, x_len)], 1)] = slot;
+  }
+}
 }  // namespace
+
+cudaError_t launch_tail_order(const RunF32& r, float x_len, cudaStream_t st) {
+  k_tail_order<<<1, 1024, 0, st>>>(r.tail, r.tail_cap, r.queue, x_len, r.tail_order);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_expand_chunks(const int* order, int norder, int per_task, int csz, int np_local,
                                  int4* chunks, cudaStream_t st) {
