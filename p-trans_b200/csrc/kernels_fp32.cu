@@ -192,19 +192,35 @@ __device__ __forceinline__ bool closer(float t, int s, float tr, int sr) {
    offset A.w): the ray's crossing of the plane, in front (within eps) and
    nearer than (tr, sb), and inside the edges; the edges are read only for a
    crossing that passes the rest. */
-template <class G_t>
-__device__ __forceinline__ void poly_test(const G_t& G, int s, float4 A, float px, float py,
-                                          float pz, float dx, float dy, float dz, float eps,
-                                          float& tr, int& sb) {
+__device__ __forceinline__ float poly_cross(float4 A, float px, float py, float pz, float dx,
+                                            float dy, float dz, float eps) {
+  /* the plane crossing, or -inf for a ray not heading into the plane's
+     front or crossing it behind the start (beyond eps) */
   const float cosa = fmaf(A.x, dx, fmaf(A.y, dy, A.z * dz));
-  if (cosa <= 0.0f) return;
   const float t = __fdividef(A.w - fmaf(A.x, px, fmaf(A.y, py, A.z * pz)), cosa);
+  return (cosa > 0.0f && t >= -eps) ? t : -3.0e38f;
+}
+
+/* The rest of the polygon test for a plane crossing t (poly_cross): nearer
+   than (tr, sb) and inside the edges. */
+template <class G_t>
+__device__ __forceinline__ void poly_inside(const G_t& G, int s, float t, float px, float py,
+                                            float pz, float dx, float dy, float dz, float eps,
+                                            float& tr, int& sb) {
   if (!(t >= -eps) || !closer(t, s, tr, sb)) return;
   const int4 B = G.hotB(s);
   const float hx = fmaf(t, dx, px), hy = fmaf(t, dy, py), hz = fmaf(t, dz, pz);
   if (!inside_edges(G, B.y, B.z, hx, hy, hz, eps)) return;
   tr = t;
   sb = s;
+}
+
+template <class G_t>
+__device__ __forceinline__ void poly_test(const G_t& G, int s, float4 A, float px, float py,
+                                          float pz, float dx, float dy, float dz, float eps,
+                                          float& tr, int& sb) {
+  poly_inside(G, s, poly_cross(A, px, py, pz, dx, dy, dz, eps), px, py, pz, dx, dy, dz, eps, tr,
+              sb);
 }
 
 /* Capped cylinder (centre A.xyz, radius A.w; unit axis E.xyz, half length
@@ -747,8 +763,19 @@ __device__ __forceinline__ void scan_list(const G_t& G, const int* lst, const fl
   nsurf += (unsigned)n;
   if (allpoly) {
     /* polygons only: the planes come from the list's shared-memory copy,
-       the edges only for a crossing in front of the ray and in range */
-    for (int k = 0; k < n; ++k) poly_test(G, lst[k], lpl[k], px, py, pz, dx, dy, dz, eps, tr, sb);
+       four crossings at a time (independent), then the edges in list
+       order only for a crossing in front of the ray and in range */
+    for (int k = 0; k < n; k += 4) {
+      float t[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        t[i] = k + i < n ? poly_cross(lpl[min(k + i, n - 1)], px, py, pz, dx, dy, dz, eps)
+                         : -3.0e38f;
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        if (t[i] > -3.0e38f && t[i] <= tr)
+          poly_inside(G, lst[k + i], t[i], px, py, pz, dx, dy, dz, eps, tr, sb);
+    }
   } else {
     for (int k = 0; k < n; ++k)
       test_surface<EXT>(G, lst[k], px, py, pz, dx, dy, dz, last_geom, eps, zmax, tr, sb);
