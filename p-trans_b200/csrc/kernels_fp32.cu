@@ -171,13 +171,17 @@ struct GeoBatch {
   __device__ __forceinline__ float4 node(int i) const { return ld(lay.bvh_node + i); }
 };
 
+/* Point (x, y, z) on a polygon's plane against its edge half-spaces m
+   (unit normal in the plane, pointing in, offset m.w), within eps. */
+__device__ __forceinline__ bool inside_edge(float4 m, float x, float y, float z, float eps) {
+  return !(fmaf(m.x, x, fmaf(m.y, y, m.z * z)) < m.w - eps);
+}
+
 template <class G_t>
 __device__ __forceinline__ bool inside_edges(const G_t& G, int e0, int ne, float x, float y,
                                              float z, float eps) {
-  for (int e = 0; e < ne; ++e) {
-    const float4 m = G.edge(e0 + e);
-    if (fmaf(m.x, x, fmaf(m.y, y, m.z * z)) < m.w - eps) return false;
-  }
+  for (int e = 0; e < ne; ++e)
+    if (!inside_edge(G.edge(e0 + e), x, y, z, eps)) return false;
   return true;
 }
 
@@ -211,6 +215,19 @@ __device__ __forceinline__ void poly_inside(const G_t& G, int s, float t, float 
   const int4 B = G.hotB(s);
   const float hx = fmaf(t, dx, px), hy = fmaf(t, dy, py), hz = fmaf(t, dz, pz);
   if (!inside_edges(G, B.y, B.z, hx, hy, hz, eps)) return;
+  tr = t;
+  sb = s;
+}
+
+/* poly_inside for a triangle whose three edges are at E (shared memory). */
+__device__ __forceinline__ void tri_inside(const float4* E, int s, float t, float px, float py,
+                                           float pz, float dx, float dy, float dz, float eps,
+                                           float& tr, int& sb) {
+  if (!(t >= -eps) || !closer(t, s, tr, sb)) return;
+  const float hx = fmaf(t, dx, px), hy = fmaf(t, dy, py), hz = fmaf(t, dz, pz);
+  if (!inside_edge(E[0], hx, hy, hz, eps) || !inside_edge(E[1], hx, hy, hz, eps) ||
+      !inside_edge(E[2], hx, hy, hz, eps))
+    return;
   tr = t;
   sb = s;
 }
@@ -640,12 +657,14 @@ __device__ __forceinline__ void warp_argmax(float v, int lane, float& vmax, int&
    replaces the one with the largest bound, and R drops to the bound of
    whatever leaves the list.  Returns the final R (every surface missing
    from the list has a bound of at least R from p) and stores the entries
-   to lst and their planes (hotA) to lpl; allpoly tells whether every entry
-   is a polygon.  Warp-collective: every lane searches the same nodes. */
+   to lst, their planes (hotA) to lpl and, for triangles, their edges to
+   led (three per entry); kind is 2 when every entry is a triangle, 1 when
+   every entry is a polygon, else 0.  Warp-collective: every lane searches
+   the same nodes. */
 template <bool EXT, class G_t>
 __device__ __noinline__ float list_bvh(const G_t& G, int root, float px, float py, float pz,
-                                       float R, int lane, int* lst, float4* lpl, int& n,
-                                       int& allpoly) {
+                                       float R, int lane, int* lst, float4* lpl, float4* led,
+                                       int& n, int& kind) {
   int stk[kBvhStack];
   float std_[kBvhStack];
   int sp = 0;
@@ -705,13 +724,20 @@ __device__ __noinline__ float list_bvh(const G_t& G, int root, float px, float p
     }
     if (!found) break;
   }
-  bool poly = true;
+  bool poly = true, tri = true;
   if (lane < n) {
     lst[lane] = my_s;
     lpl[lane] = G.hotA(my_s);
-    poly = (G.hotB(my_s).x & 0xff) == REC_POLY;
+    const int4 B = G.hotB(my_s);
+    poly = (B.x & 0xff) == REC_POLY;
+    tri = poly && B.z == 3;
+    if (tri) {
+      led[3 * lane] = G.edge(B.y);
+      led[3 * lane + 1] = G.edge(B.y + 1);
+      led[3 * lane + 2] = G.edge(B.y + 2);
+    }
   }
-  allpoly = __all_sync(FULL, poly) ? 1 : 0;
+  kind = __all_sync(FULL, tri) ? 2 : (__all_sync(FULL, poly) ? 1 : 0);
   return R;
 }
 
@@ -754,14 +780,27 @@ __device__ __forceinline__ float safety_list(const G_t& G, const int* lst, int n
    the nearest hit up to fp is the full scan's, and without one tb stays
    above fp, as it would. */
 template <bool EXT, class G_t>
-__device__ __forceinline__ void scan_list(const G_t& G, const int* lst, const float4* lpl, int n,
-                                          bool allpoly, float px, float py, float pz, float dx,
-                                          float dy, float dz, int last_geom, float eps,
-                                          float zmax, float fp, float& tb, int& sb,
+__device__ __forceinline__ void scan_list(const G_t& G, const int* lst, const float4* lpl,
+                                          const float4* led, int n, int kind, float px, float py,
+                                          float pz, float dx, float dy, float dz, int last_geom,
+                                          float eps, float zmax, float fp, float& tb, int& sb,
                                           unsigned& nsurf) {
   float tr = fminf(tb, __uint_as_float(__float_as_uint(fp) + 1u));
   nsurf += (unsigned)n;
-  if (allpoly) {
+  if (kind == 2) {
+    /* triangles: planes and edges from the list's shared-memory copy */
+    for (int k = 0; k < n; k += 4) {
+      float t[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        t[i] = k + i < n ? poly_cross(lpl[min(k + i, n - 1)], px, py, pz, dx, dy, dz, eps)
+                         : -3.0e38f;
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        if (t[i] > -3.0e38f && t[i] <= tr)
+          tri_inside(led + 3 * (k + i), lst[k + i], t[i], px, py, pz, dx, dy, dz, eps, tr, sb);
+    }
+  } else if (kind == 1) {
     /* polygons only: the planes come from the list's shared-memory copy,
        four crossings at a time (independent), then the edges in list
        order only for a crossing in front of the ray and in range */
@@ -1136,8 +1175,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   __shared__ __align__(16) float coop_rowf[PH == PH_TAIL ? kBlock / 32 : 1][kRowStride * 7];
   float* const crow = coop_rowf[PH == PH_TAIL ? (threadIdx.x >> 5) : 0];
   /* ... and six rows where the lanes' own phonons wait during the rounds */
-  __shared__ float4 coop_park[PH == PH_TAIL ? kBlock / 32 : 1][6][32];
-  float4 (*const park)[32] = coop_park[PH == PH_TAIL ? (threadIdx.x >> 5) : 0];
+  __shared__ float4 coop_park[PH == PH_TAIL ? kBlock / 32 : 1][6];
+  float4* const park = coop_park[PH == PH_TAIL ? (threadIdx.x >> 5) : 0];
   /* ... and, in kernels built for BVH grains, the warp's local candidate
      list: its entries, its centre and radius, and (count, grain); not in
      the adjoint replay, whose shared accumulators leave no room */
@@ -1145,10 +1184,12 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
   constexpr int kLW = kUseList ? kBlock / 32 : 1;
   __shared__ int coop_list[kLW][kList];
   __shared__ float4 coop_lplane[kLW][kList];
+  __shared__ float4 coop_ledge[kLW][3 * kList];
   __shared__ float4 coop_lball[kLW];
-  __shared__ int4 coop_lmeta[kLW];  /* count, grain, every entry a polygon */
+  __shared__ int4 coop_lmeta[kLW];  /* count, grain, kind (list_bvh) */
   int* const lst = coop_list[kLW > 1 ? (threadIdx.x >> 5) : 0];
   float4* const lpl = coop_lplane[kLW > 1 ? (threadIdx.x >> 5) : 0];
+  float4* const led = coop_ledge[kLW > 1 ? (threadIdx.x >> 5) : 0];
   if (kUseList && lane == 0) coop_lmeta[threadIdx.x >> 5] = make_int4(0, -1, 0, 0);
   /* tail phase: phonons the drain left (the counts are final at launch),
      long ones from the front of the list, the others from the back */
@@ -1435,29 +1476,31 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
     float pre_tb = 0.0f;
     int pre_sb = -1;
     if (PH == PH_TAIL) {
-      const unsigned todo0 = __ballot_sync(FULL, alive && lam < flmax);
+      const unsigned todo0 = __ballot_sync(FULL, lane == 0 && alive && lam < flmax);
       const int max_rounds = kCoopRounds;
       if (todo0) {
-        /* every lane's own phonon waits in the warp's park rows while the
-           warp runs the rounds, so its registers serve the rounds; each
-           cooperative phonon is read from its lane's slot (broadcast loads)
-           and written back there by its lane */
-        park[0][lane] = make_float4(px, py, pz, dx);
-        park[1][lane] = make_float4(dy, dz, fp, lam);
-        park[2][lane] = make_float4(bx, by, bz, br2);
-        park[3][lane] = make_float4(__int_as_float(grain), __int_as_float(last_geom),
-                                    __int_as_float(task), omr);
-        park[4][lane] = make_float4(__uint_as_float(slo), __uint_as_float(shi),
-                                    __uint_as_float(flight), gr2);
-        park[5][lane] = make_float4(g2r2, __int_as_float(gnear), 0.0f, 0.0f);
+        /* the warp's phonon (in the tail phase lane 0 holds the only one)
+           waits in the warp's park row while the warp runs the rounds, so
+           its registers serve the rounds; every lane reads it (broadcast
+           loads) and lane 0 writes it back */
+        if (lane == 0) {
+          park[0] = make_float4(px, py, pz, dx);
+          park[1] = make_float4(dy, dz, fp, lam);
+          park[2] = make_float4(bx, by, bz, br2);
+          park[3] = make_float4(__int_as_float(grain), __int_as_float(last_geom),
+                                __int_as_float(task), omr);
+          park[4] = make_float4(__uint_as_float(slo), __uint_as_float(shi),
+                                __uint_as_float(flight), gr2);
+          park[5] = make_float4(g2r2, __int_as_float(gnear), 0.0f, 0.0f);
+        }
         __syncwarp();
         unsigned todo = todo0;
         while (todo) {
           const int L = __ffs(todo) - 1;
           todo &= todo - 1;
-          const float4 s0 = park[0][L], s1 = park[1][L], s2 = park[2][L], s3 = park[3][L];
-          const float4 s4 = park[4][L];
-          const float4 s5 = park[5][L];
+          const float4 s0 = park[0], s1 = park[1], s2 = park[2], s3 = park[3];
+          const float4 s4 = park[4];
+          const float4 s5 = park[5];
           float cpx = s0.x, cpy = s0.y, cpz = s0.z;
           float cdx = s0.w, cdy = s1.x, cdz = s1.y, cfp = s1.z;
           const float clam = s1.w;
@@ -1568,13 +1611,14 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             const bool in_gball = de2 < cgr2 && ds2 < cgr2;
             const bool in_g2 = de2 < cg2r2 && ds2 < cg2r2;
             /* ... and within the local list's radius only the listed ones */
-            bool in_list = false, lpoly = false;
+            bool in_list = false;
+            int lkind = 0;
             int ln = 0;
             if (kUseList) {
               const int4 lm = coop_lmeta[threadIdx.x >> 5];
               const float4 lc = coop_lball[threadIdx.x >> 5];
               const float ru = lc.w - 4.0f * eps;
-              lpoly = lm.z != 0;
+              lkind = lm.z;
               const float lx = fmaf(sfp, sdx, qx) - lc.x, ly = fmaf(sfp, sdy, qy) - lc.y;
               const float lz = fmaf(sfp, sdz, qz) - lc.z;
               const float mx = qx - lc.x, my = qy - lc.y, mz = qz - lc.z;
@@ -1597,7 +1641,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
                   test_near<EXT>(G, cnear, qx, qy, qz, sdx, sdy, sdz, lane == 0 ? clast : -1, eps, Z,
                                  tb, sb, my_surf_tests);
                 else if (kUseList && in_list)
-                  scan_list<EXT>(G, lst, lpl, ln, lpoly, qx, qy, qz, sdx, sdy, sdz,
+                  scan_list<EXT>(G, lst, lpl, led, ln, lkind, qx, qy, qz, sdx, sdy, sdz,
                                  lane == 0 ? clast : -1, eps, Z, sfp, tb, sb, my_surf_tests);
                 else
                   scan_grain<EXT>(G, cgrain, qx, qy, qz, sdx, sdy, sdz, lane == 0 ? clast : -1, eps,
@@ -1700,7 +1744,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
                   const float r0 = (lm.y == cgrain && lm.x == kList) ? fminf(rt, 1.25f * lc.w) : rt;
                   int n, ap;
                   const float R = list_bvh<EXT>(G, G.bvh_root(cgrain), cpx, cpy, cpz, r0, lane, lst,
-                                                lpl, n, ap);
+                                                lpl, led, n, ap);
                   const float4 nc = make_float4(cpx, cpy, cpz, R);
                   if (lane == 0) {
                     coop_lball[threadIdx.x >> 5] = nc;
@@ -1722,13 +1766,13 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             clast = -1;
           }
           if (lane == L) {
-            park[0][lane] = make_float4(cpx, cpy, cpz, cdx);
-            park[1][lane] = make_float4(cdy, cdz, cfp, clam);
-            park[2][lane] = make_float4(cbx, cby, cbz, cbr2);
-            park[3][lane] = make_float4(__int_as_float(cgrain), __int_as_float(clast),
+            park[0] = make_float4(cpx, cpy, cpz, cdx);
+            park[1] = make_float4(cdy, cdz, cfp, clam);
+            park[2] = make_float4(cbx, cby, cbz, cbr2);
+            park[3] = make_float4(__int_as_float(cgrain), __int_as_float(clast),
                                         s3.z, s3.w);
-            park[4][lane] = make_float4(s4.x, s4.y, __uint_as_float(cfl), cgr2);
-            park[5][lane] = make_float4(cg2r2, __int_as_float(cnear), 0.0f, 0.0f);
+            park[4] = make_float4(s4.x, s4.y, __uint_as_float(cfl), cgr2);
+            park[5] = make_float4(cg2r2, __int_as_float(cnear), 0.0f, 0.0f);
             if (MODE == MODE_ADJOINT) {
               adj_len += clen;
               adj_npp += cnpp;
@@ -1746,10 +1790,12 @@ __global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
             my_coop_flights += ctaken;
           }
         }
-        /* every lane takes its phonon back (each slot was last written by its
-           own lane) */
-        const float4 s0 = park[0][lane], s1 = park[1][lane], s2 = park[2][lane];
-        const float4 s3 = park[3][lane], s4 = park[4][lane], s5 = park[5][lane];
+        /* lane 0 takes its phonon back (it wrote the row last); the other
+           lanes, which hold no phonon, read the same row, so that no state
+           of theirs has to live through the rounds */
+        __syncwarp();
+        const float4 s0 = park[0], s1 = park[1], s2 = park[2];
+        const float4 s3 = park[3], s4 = park[4], s5 = park[5];
         px = s0.x; py = s0.y; pz = s0.z; dx = s0.w;
         dy = s1.x; dz = s1.y; fp = s1.z; lam = s1.w;
         bx = s2.x; by = s2.y; bz = s2.z; br2 = s2.w;
