@@ -205,7 +205,7 @@ def test_rank_partition_is_exact_fp32():
 
 
 @pytest.mark.parametrize("name", ["film_periodic", "film_mirror_transmit", "spheres", "brick_tris",
-                                  "nanowire_mixed", "capped"])
+                                  "nanowire_mixed", "capped", "lattice_tris"])
 @pytest.mark.parametrize("cap", [0, 40])
 def test_cooperative_tail_takes_the_same_trajectories(name, cap):
     """The tail phase (a warp of cooperating lanes per diffusive phonon once
@@ -213,7 +213,10 @@ def test_cooperative_tail_takes_the_same_trajectories(name, cap):
     warp holds at most 8 or 1 live phonons) and the one-lane path to the end
     (tune_flags bit 1) give identical per-task counts, lost counts and
     flight totals: a flight advances the position with the same rounding on
-    every path, so the trajectory depends only on its Philox counter.  With
+    every path, so the trajectory depends only on its Philox counter.  The
+    tail phase takes its surface events inside the rounds, orders its list
+    by expected walk, and in a BVH grain (lattice_tris: 324 triangles) tests
+    flights against its warp's local list of the nearest triangles.  With
     the fast path off (tune_flags bit 0) no safe ball or grain ball is ever
     computed and every flight takes the full test, so the variants without
     it also show that the tests the balls skip could not have hit."""
