@@ -1142,8 +1142,15 @@ constexpr uint32_t kTailLong = 8192;
    walk needs about (radius / MFP)^2 flights to leave the ball */
 constexpr float kBallCapMfp = 32.0f;
 
+/* Blocks per SM the register budget is cut for: three for the forward and
+   listing drain phase of structures without BVH or capped cylinders (80
+   registers, no spills: a drain 7% shorter on the thin film, 6% on the
+   Voronoi polycrystal), two for the rest (the tail phase's rounds, and the
+   BVH, batched and adjoint kernels, which would spill). */
 template <bool SMEM, int MODE, bool BATCH, bool EXT, int PH>
-__global__ void __launch_bounds__(kBlock, 2) k_persistent(GeoF32 gp, RunF32 r) {
+__global__ void __launch_bounds__(kBlock,
+                                  (PH == PH_DRAIN && !EXT && !BATCH && MODE != MODE_ADJOINT) ? 3 : 2)
+    k_persistent(GeoF32 gp, RunF32 r) {
   typename std::conditional<BATCH, GeoBatch, Geo<SMEM>>::type G;
   G.lay = gp.lay;
   G.base = gp.blob;
