@@ -541,9 +541,10 @@ int ptg_autotune(ptg_handle* h, const ptg_run* run, int32_t reps, ptg_options* b
  * lost-phonon limit; the same ptg_last_stats record, kernel times aside) but
  * allocates no device or host memory: the kernels' scratch (work-queue
  * counter, statistics, tallies, task and chunk tables, a 65536-phonon
- * tail-phase list; hand-overs past its capacity stay in the drain phase and
- * are counted in ptg_stats.tail_refused) lives in one static device array of
- * fixed size (about 9 MB) that every GPU loading the library keeps until
+ * tail-phase list and its order; hand-overs past its capacity stay in the
+ * drain phase and are counted in ptg_stats.tail_refused) lives in one static
+ * device array of fixed size (about 9.3 MB) that every GPU loading the
+ * library keeps until
  * exit, and the caller's transmit array receives the counts before they are
  * divided by np in place (on PTG_ERR_TIMEOUT or PTG_ERR_CUDA after the
  * launch it is zeroed).  Limits: nbranch*nkpoint*(nangle-1) <=

@@ -51,7 +51,8 @@ constexpr size_t kOffTasks = kOffLost + 8 * kMaxTasks;         /* float4[tasks] 
 constexpr size_t kOffOmega = kOffTasks + 16 * kMaxTasks;       /* double[tasks] */
 constexpr size_t kOffChunks = kOffOmega + 8 * kMaxTasks;       /* int4[chunks]  */
 constexpr size_t kOffTail = kOffChunks + 16 * kMaxChunks;     /* float4[kTailUnits * tail] */
-constexpr size_t kScratchBytes = kOffTail + 16 * (size_t)ptg::kTailUnits * (size_t)kMaxTail;
+constexpr size_t kOffOrder = kOffTail + 16 * (size_t)ptg::kTailUnits * (size_t)kMaxTail; /* int[tail] */
+constexpr size_t kScratchBytes = kOffOrder + 4 * (size_t)kMaxTail;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
@@ -197,6 +198,7 @@ extern "C" int ptg_transmission_noalloc(ptg_handle* h, double mfp_nm, int32_t na
        holds keeps the extra phonons in the drain phase */
     r.tail = reinterpret_cast<float4*>(base + kOffTail);
     r.tail_cap = std::min(kMaxTail, grid * block);
+    r.tail_order = reinterpret_cast<int*>(base + kOffOrder);
     int tbps = 0;
     if (ptg::tail_occupancy(block, smem, &tbps, ptg::MODE_FORWARD, v.g32.has_ext != 0, v.g32.stage_smem != 0) != cudaSuccess)
       return PTG_ERR_CUDA;
@@ -205,7 +207,8 @@ extern "C" int ptg_transmission_noalloc(ptg_handle* h, double mfp_nm, int32_t na
   if (r.nchunk > 0) {
     if (ptg::launch_persistent_fp32(v.g32, r, grid, block, smem, s) != cudaSuccess)
       return PTG_ERR_CUDA;
-    if (tgrid > 0 && ptg::launch_tail_fp32(v.g32, r, tgrid, block, smem, s) != cudaSuccess)
+    if (tgrid > 0 && (ptg::launch_tail_order(r, v.g32.box[0], s) != cudaSuccess ||
+                      ptg::launch_tail_fp32(v.g32, r, tgrid, block, smem, s) != cudaSuccess))
       return PTG_ERR_CUDA;
   }
   /* the counts land in the caller's transmit array (ntask <= its length),
@@ -236,7 +239,7 @@ extern "C" int ptg_transmission_noalloc(ptg_handle* h, double mfp_nm, int32_t na
   L->coop_flights = sv[13];
   L->box_tests = sv[14];
   L->surface_tests = sv[15];
-  L->launches = 1 + (r.nchunk > 0 ? (tgrid > 0 ? 2 : 1) : 0);
+  L->launches = 1 + (r.nchunk > 0 ? (tgrid > 0 ? 3 : 1) : 0);
   L->grid = grid;
   L->block = block;
   L->h2d_bytes = sizeof(double) * nmode;
