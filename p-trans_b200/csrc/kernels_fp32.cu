@@ -40,7 +40,7 @@
  *     together so that four independent chains fill the issue slots; tallies
  *     are integer, aggregated per warp by task (match_any) before one atomic;
  *   - two phases: the drain phase runs the work queue one lane per phonon
- *     and, once the queue is dry, hands its diffusive phonons to a tail list;
+ *     and, once the queue is dry, hands its live phonons to a tail list;
  *     the tail phase (a second launch of the same kernel) gives each of them
  *     a warp that advances it 32 flights per round, one flight per lane, with
  *     the flights' start points summed in flight order (in grains with a BVH
@@ -1125,8 +1125,8 @@ constexpr int kTestWindow = 4;
 
 /* Kernel phases.  PH_DRAIN pulls (task, particle range) chunks from the
    work queue, one phonon per lane; once the queue is dry a warp holding at
-   most coop_lanes live phonons moves its diffusive ones (MFP below the
-   fast-path limit) to the tail list and finishes the others.  PH_TAIL runs
+   most coop_lanes live phonons moves them to the tail list (a phonon past
+   the list's capacity stays and is finished here).  PH_TAIL runs
    after it: every warp takes one phonon of the tail list at a time into
    lane 0 and advances it with cooperative rounds, so the longest
    trajectories get a warp each instead of sharing one. */
@@ -1410,10 +1410,12 @@ __global__ void __launch_bounds__(kBlock,
       if (queue_done) break;
       continue;
     }
-    /* ---- drain phase, queue dry: diffusive phonons go to the tail list */
+    /* ---- drain phase, queue dry: live phonons go to the tail list (the
+       diffusive ones and, as well, the few long-MFP ones, which would
+       otherwise hold their warp, and the drain launch, to the end) */
     if (PH == PH_DRAIN && !BATCH && MODE != MODE_TRACE && queue_done && r.coop_lanes > 0 &&
         !tail_full && __popc(__ballot_sync(FULL, alive)) <= r.coop_lanes) {
-      const unsigned mw = __ballot_sync(FULL, alive && lam < flmax);
+      const unsigned mw = __ballot_sync(FULL, alive);
       if (mw) {
         /* a slot is reserved from one counter of all requests (queue[5])
            before the phonon picks its end of the list: the phonons admitted
@@ -1483,7 +1485,7 @@ __global__ void __launch_bounds__(kBlock,
     float pre_tb = 0.0f;
     int pre_sb = -1;
     if (PH == PH_TAIL) {
-      const unsigned todo0 = __ballot_sync(FULL, lane == 0 && alive && lam < flmax);
+      const unsigned todo0 = __ballot_sync(FULL, lane == 0 && alive);
       const int max_rounds = kCoopRounds;
       if (todo0) {
         /* the warp's phonon (in the tail phase lane 0 holds the only one)
