@@ -135,9 +135,9 @@ struct RunF32 {
   int32_t fast_steps;         /* max safe-distance p-p flights per iteration (0: off) */
   float fast_lambda_max;      /* tasks with a smaller MFP use the fast path           */
   int32_t coop_lanes;         /* once the queue is dry, a warp with at most this many
-                                 live phonons moves its diffusive ones to the tail
-                                 list, where each gets a warp of its own that
-                                 advances it 32 flights a round (0: off)          */
+                                 live phonons moves them to the tail list, where
+                                 each gets a warp of its own that advances it 32
+                                 flights a round (0: off)                         */
   float4* tail;               /* tail list: kTailUnits float4 per phonon           */
   int32_t tail_cap;           /* its capacity in phonons                           */
   int32_t* tail_order;        /* the tail phase takes list slots in this order
