@@ -643,7 +643,7 @@ int run_transport(ptg_handle* h, const Transport& T) {
        against 11.1 ms for 8) */
     int rt = h->opt.regen_threshold > 0 ? h->opt.regen_threshold : ptg::kDefaultRegen;
     r.regen_threshold = rt > 32 ? 32 : rt;
-    r.fast_steps = (h->opt.tune_flags & 1) ? 0 : (h->opt.fast_steps > 0 ? h->opt.fast_steps : ptg::kDefaultFastSteps);
+    r.fast_steps = (h->opt.tune_flags & 1) ? 0 : (h->opt.fast_steps > 0 ? h->opt.fast_steps : ptg::default_fast_steps(h->g32));
     const double lmin = std::min(h->geom.box[0], std::min(h->geom.box[1], h->geom.box[2]));
     r.fast_lambda_max = (float)(0.1 * lmin);
     /* tune_flags bit 1 turns the tail phase off; 0 selects 32 lanes (every

@@ -184,9 +184,17 @@ constexpr int kStatSlots = 24;
 
 /* Scheduling defaults of the persistent kernel (ptg_options 0 = these):
    idle lanes before a warp refills, fast-path flights per lane and
-   iteration. */
+   iteration (structures whose grains are scanned linearly take short
+   fast-path bursts, their full flights being cheap: thin film 16.5 ->
+   15.8 ms, Voronoi 312 -> 305 ms at 4 against 8; those with a BVH or capped
+   cylinders amortise dearer full flights over longer ones: C3 738 ms at 8,
+   766 at 4). */
 constexpr int kDefaultRegen = 2;
 constexpr int kDefaultFastSteps = 8;
+constexpr int kDefaultFastStepsPlain = 4;
+inline int default_fast_steps(const GeoF32& g) {
+  return g.has_ext ? kDefaultFastSteps : kDefaultFastStepsPlain;
+}
 
 /* Replays are split in this many interleaved batches (sample % kAdjBatches)
    whose spread gives the standard error of the adjoint estimates. */

@@ -169,7 +169,7 @@ extern "C" int ptg_transmission_noalloc(ptg_handle* h, double mfp_nm, int32_t na
   r.ref_quirks = v.opt.ref_quirks;
   const int rt = v.opt.regen_threshold > 0 ? v.opt.regen_threshold : ptg::kDefaultRegen;
   r.regen_threshold = rt > 32 ? 32 : rt;
-  r.fast_steps = (v.opt.tune_flags & 1) ? 0 : (v.opt.fast_steps > 0 ? v.opt.fast_steps : ptg::kDefaultFastSteps);
+  r.fast_steps = (v.opt.tune_flags & 1) ? 0 : (v.opt.fast_steps > 0 ? v.opt.fast_steps : ptg::default_fast_steps(v.g32));
   const double lmin = fmin(v.geom->box[0], fmin(v.geom->box[1], v.geom->box[2]));
   r.fast_lambda_max = (float)(0.1 * lmin);
   r.counts = counts;
