@@ -678,7 +678,8 @@ int run_transport(ptg_handle* h, const Transport& T) {
     const bool tail = r.coop_lanes > 0 && T.mode != ptg::MODE_TRACE;
     if (tail) {
       /* the list, then the order the tail phase takes it in */
-      CU(h->tail.ensure((sizeof(float4) * ptg::kTailUnits + sizeof(int)) * (size_t)grid * block));
+      CU(h->tail.ensure((sizeof(float4) * ptg::kTailUnits + sizeof(int)) * (size_t)grid * block +
+                        sizeof(int) * ptg::kTailOrderExtra));
       r.tail = h->tail.as<float4>();
       r.tail_cap = grid * block;
       r.tail_order = reinterpret_cast<int*>(r.tail + (size_t)ptg::kTailUnits * r.tail_cap);
@@ -702,7 +703,7 @@ int run_transport(ptg_handle* h, const Transport& T) {
     CU(cudaEventRecord(h->ev[1], h->stream));
     h->last.grid = grid;
     h->last.block = block;
-    h->last.launches = (work ? (tail ? 3 : 1) : 0) + (r.nchunk > 0 ? 1 : 0);
+    h->last.launches = (work ? (tail ? 4 : 1) : 0) + (r.nchunk > 0 ? 1 : 0);
     h->fp32_split = work;
     h->tail_cap = tail ? r.tail_cap : 0;
   }

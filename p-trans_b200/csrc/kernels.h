@@ -208,9 +208,11 @@ cudaError_t launch_persistent_fp32(const GeoF32& g, const RunF32& r, int grid, i
                                    size_t smem, cudaStream_t st, int mode = MODE_FORWARD);
 /* The tail phase after it (forward, list and adjoint modes): the phonons
    the drain phase left in r.tail, one per warp. */
-/* Orders the tail list for the tail phase (r.tail_order, tail_cap ints):
-   longest expected remaining walk first.  One block, between the drain and
-   the tail launch on the same stream; x_len is the box length along x. */
+/* Orders the tail list for the tail phase (r.tail_order: tail_cap ints and
+   kTailOrderExtra more for a histogram and cursors): longest expected
+   remaining walk first.  A memset and two kernels between the drain and the
+   tail launch on the same stream; x_len is the box length along x. */
+constexpr int kTailOrderExtra = 256;
 cudaError_t launch_tail_order(const RunF32& r, float x_len, cudaStream_t st);
 cudaError_t launch_tail_fp32(const GeoF32& g, const RunF32& r, int grid, int block, size_t smem,
                              cudaStream_t st, int mode = MODE_FORWARD);

@@ -2215,6 +2215,7 @@ __global__ void k_expand_chunks(const int* __restrict__ order, int norder, int p
 
 /* Buckets of the tail order: a quarter octave of the expected walk each. */
 constexpr int kOrderBuckets = 128;
+static_assert(2 * kOrderBuckets == kTailOrderExtra, "tail order histogram and cursors");
 
 /* Tail-list slot of hand-over c (front list, then back list) and the
    bucket of its phonon's expected remaining walk.  A diffusive phonon at x
@@ -2229,38 +2230,62 @@ __device__ __forceinline__ int order_bucket(const float4* tail, int slot, float 
   return w > 1.0f ? min(kOrderBuckets - 1, (int)(4.0f * __log2f(w))) : 0;
 }
 
-/* One block: a histogram of the buckets, their offsets from the top bucket
-   down, and the slots scattered to their bucket's range. */
-__global__ void k_tail_order(const float4* __restrict__ tail, int tail_cap,
-                             const int* __restrict__ queue, float x_len, int* __restrict__ order) {
-  __shared__ int hist[kOrderBuckets];
+/* Hand-over c of the tail list: its slot (front list, then back list). */
+__device__ __forceinline__ int tail_slot(int c, int nlong, int tail_cap) {
+  return c < nlong ? c : tail_cap - 1 - (c - nlong);
+}
+
+/* One thread per hand-over: its bucket, kept in the entry's spare word
+   (float4 6, z), and the bucket histogram. */
+__global__ void k_order_hist(float4* __restrict__ tail, int tail_cap, const int* __restrict__ queue,
+                             float x_len, int* __restrict__ hist) {
   const int nlong = min(queue[2], tail_cap);
   const int ntail = nlong + min(queue[4], tail_cap - nlong);
-  for (int b = threadIdx.x; b < kOrderBuckets; b += blockDim.x) hist[b] = 0;
-  __syncthreads();
-  for (int c = threadIdx.x; c < ntail; c += blockDim.x) {
-    const int slot = c < nlong ? c : tail_cap - 1 - (c - nlong);
-    atomicAdd(&hist[order_bucket(tail, slot, x_len)], 1);
-  }
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ntail) return;
+  const int slot = tail_slot(c, nlong, tail_cap);
+  const int b = order_bucket(tail, slot, x_len);
+  reinterpret_cast<int*>(tail + (size_t)kTailUnits * slot + 6)[2] = b;
+  atomicAdd(&hist[b], 1);
+}
+
+/* One thread per hand-over: the bucket offsets from the top bucket down
+   (every block from the histogram), then the slot to its bucket's range. */
+__global__ void k_order_scatter(const float4* __restrict__ tail, int tail_cap,
+                                const int* __restrict__ queue, const int* __restrict__ hist,
+                                int* __restrict__ cursor, int* __restrict__ order) {
+  __shared__ int h[kOrderBuckets];
+  const int nlong = min(queue[2], tail_cap);
+  const int ntail = nlong + min(queue[4], tail_cap - nlong);
+  if ((int)(blockIdx.x * blockDim.x) >= ntail) return;
+  for (int b = threadIdx.x; b < kOrderBuckets; b += blockDim.x) h[b] = hist[b];
   __syncthreads();
   if (threadIdx.x == 0) {
     int run = 0;
     for (int b = kOrderBuckets - 1; b >= 0; --b) {
-      const int h = hist[b];
-      hist[b] = run;
-      run += h;
+      const int n = h[b];
+      h[b] = run;
+      run += n;
     }
   }
   __syncthreads();
-  for (int c = threadIdx.x; c < ntail; c += blockDim.x) {
-    const int slot = c < nlong ? c : tail_cap - 1 - (c - nlong);
-    order[atomicAdd(&hist[order_bucket(tail, slot, x_len)], 1)] = slot;
-  }
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ntail) return;
+  const int slot = tail_slot(c, nlong, tail_cap);
+  const int b = reinterpret_cast<const int*>(tail + (size_t)kTailUnits * slot + 6)[2];
+  order[h[b] + atomicAdd(&cursor[b], 1)] = slot;
 }
 }  // namespace
 
 cudaError_t launch_tail_order(const RunF32& r, float x_len, cudaStream_t st) {
-  k_tail_order<<<1, 1024, 0, st>>>(r.tail, r.tail_cap, r.queue, x_len, r.tail_order);
+  /* the histogram and the bucket cursors follow the order array */
+  int* hist = r.tail_order + r.tail_cap;
+  cudaError_t e = cudaMemsetAsync(hist, 0, sizeof(int) * 2 * kOrderBuckets, st);
+  if (e != cudaSuccess) return e;
+  const unsigned blocks = (unsigned)((r.tail_cap + 255) / 256);
+  k_order_hist<<<blocks, 256, 0, st>>>(r.tail, r.tail_cap, r.queue, x_len, hist);
+  k_order_scatter<<<blocks, 256, 0, st>>>(r.tail, r.tail_cap, r.queue, hist, hist + kOrderBuckets,
+                                          r.tail_order);
   return cudaGetLastError();
 }
 

@@ -52,7 +52,7 @@ constexpr size_t kOffOmega = kOffTasks + 16 * kMaxTasks;       /* double[tasks] 
 constexpr size_t kOffChunks = kOffOmega + 8 * kMaxTasks;       /* int4[chunks]  */
 constexpr size_t kOffTail = kOffChunks + 16 * kMaxChunks;     /* float4[kTailUnits * tail] */
 constexpr size_t kOffOrder = kOffTail + 16 * (size_t)ptg::kTailUnits * (size_t)kMaxTail; /* int[tail] */
-constexpr size_t kScratchBytes = kOffOrder + 4 * (size_t)kMaxTail;
+constexpr size_t kScratchBytes = kOffOrder + 4 * ((size_t)kMaxTail + ptg::kTailOrderExtra);
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
@@ -239,7 +239,7 @@ extern "C" int ptg_transmission_noalloc(ptg_handle* h, double mfp_nm, int32_t na
   L->coop_flights = sv[13];
   L->box_tests = sv[14];
   L->surface_tests = sv[15];
-  L->launches = 1 + (r.nchunk > 0 ? (tgrid > 0 ? 3 : 1) : 0);
+  L->launches = 1 + (r.nchunk > 0 ? (tgrid > 0 ? 4 : 1) : 0);
   L->grid = grid;
   L->block = block;
   L->h2d_bytes = sizeof(double) * nmode;
