@@ -777,7 +777,7 @@ def main():
         per_launch_flights = flights / world / args.steps
         # the transport is two launches of k_persistent per step: the drain
         # phase (queue) and the tail phase (handed-over phonons, after a
-        # one-block kernel that orders them, timed with the tail); the
+        # two small kernels that order them, timed with the tail); the
         # roofline is the longer one's, with its own flights and CUDA-event time
         kernels = {
             "drain": {"ms_per_step": drain_k_ms / args.steps,
