@@ -776,7 +776,7 @@ def main():
         peak, peak_kind = measured_peaks()
         per_launch_flights = flights / world / args.steps
         # the transport is two launches of k_persistent per step: the drain
-        # phase (queue) and the tail phase (handed-over phonons, after a
+        # phase (queue) and the tail phase (handed-over phonons, after
         # two small kernels that order them, timed with the tail); the
         # roofline is the longer one's, with its own flights and CUDA-event time
         kernels = {
