@@ -187,13 +187,14 @@ constexpr int kStatSlots = 24;
    iteration (structures whose grains are scanned linearly take short
    fast-path bursts, their full flights being cheap: thin film 16.5 ->
    15.8 ms, Voronoi 312 -> 305 ms at 4 against 8; those with a BVH or capped
-   cylinders amortise dearer full flights over longer ones: C3 738 ms at 8,
-   766 at 4). */
+   cylinders amortise dearer full flights over longer ones: C3 766 / 740 /
+   733 ms and C4 3877 -> 3817 ms at 4 / 8 / 12; the batched launch keeps 8). */
 constexpr int kDefaultRegen = 2;
 constexpr int kDefaultFastSteps = 8;
 constexpr int kDefaultFastStepsPlain = 4;
+constexpr int kDefaultFastStepsExt = 12;
 inline int default_fast_steps(const GeoF32& g) {
-  return g.has_ext ? kDefaultFastSteps : kDefaultFastStepsPlain;
+  return g.has_ext ? kDefaultFastStepsExt : kDefaultFastStepsPlain;
 }
 
 /* Replays are split in this many interleaved batches (sample % kAdjBatches)
