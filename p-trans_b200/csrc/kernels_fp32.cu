@@ -1143,13 +1143,14 @@ constexpr uint32_t kTailLong = 8192;
 constexpr float kBallCapMfp = 32.0f;
 
 /* Blocks per SM the register budget is cut for: three for the forward and
-   listing drain phase of structures without BVH or capped cylinders (80
-   registers, no spills: a drain 7% shorter on the thin film, 6% on the
-   Voronoi polycrystal), two for the rest (the tail phase's rounds, and the
-   BVH, batched and adjoint kernels, which would spill). */
+   listing drain phase (80 registers: a drain 7% shorter on the thin film, 6%
+   on the Voronoi polycrystal; the BVH / capped-cylinder variant spills ~70
+   bytes and still gains, C4 3833 -> 3677 ms, C3 735 -> 724 ms), two for the
+   rest (the tail phase's rounds, and the batched and adjoint kernels, which
+   would spill more). */
 template <bool SMEM, int MODE, bool BATCH, bool EXT, int PH>
 __global__ void __launch_bounds__(kBlock,
-                                  (PH == PH_DRAIN && !EXT && !BATCH && MODE != MODE_ADJOINT) ? 3 : 2)
+                                  (PH == PH_DRAIN && !BATCH && MODE != MODE_ADJOINT) ? 3 : 2)
     k_persistent(GeoF32 gp, RunF32 r) {
   typename std::conditional<BATCH, GeoBatch, Geo<SMEM>>::type G;
   G.lay = gp.lay;
