@@ -199,7 +199,7 @@ typedef struct ptg_options {
   int32_t fast_steps;       /* fast p-p flights per iteration before a warp     */
                             /* goes on only while half its lanes still can      */
                             /* (at most 4x; 0 = 4 for structures without BVH or */
-                            /* capped cylinders, 12 for the others, 8 in a      */
+                            /* capped cylinders, 20 for the others, 8 in a      */
                             /* batched launch)                                  */
   int32_t coop_lanes;       /* once the work queue is dry, a warp with at most  */
                             /* this many live phonons hands its diffusive ones  */

@@ -188,11 +188,12 @@ constexpr int kStatSlots = 24;
    fast-path bursts, their full flights being cheap: thin film 16.5 ->
    15.8 ms, Voronoi 312 -> 305 ms at 4 against 8; those with a BVH or capped
    cylinders amortise dearer full flights over longer ones: C3 766 / 740 /
-   733 ms and C4 3877 -> 3817 ms at 4 / 8 / 12; the batched launch keeps 8). */
+   733 ms and C4 3877 -> 3817 ms at 4 / 8 / 12, and with three drain blocks
+   per SM C4 3661 -> 3592 ms at 12 -> 20; the batched launch keeps 8). */
 constexpr int kDefaultRegen = 2;
 constexpr int kDefaultFastSteps = 8;
 constexpr int kDefaultFastStepsPlain = 4;
-constexpr int kDefaultFastStepsExt = 12;
+constexpr int kDefaultFastStepsExt = 20;
 inline int default_fast_steps(const GeoF32& g) {
   return g.has_ext ? kDefaultFastStepsExt : kDefaultFastStepsPlain;
 }
