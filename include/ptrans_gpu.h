@@ -202,8 +202,8 @@ typedef struct ptg_options {
                             /* capped cylinders, 20 for the others, 8 in a      */
                             /* batched launch)                                  */
   int32_t coop_lanes;       /* once the work queue is dry, a warp with at most  */
-                            /* this many live phonons hands its diffusive ones  */
-                            /* to the tail phase, a second kernel that gives    */
+                            /* this many live phonons hands them over to the    */
+                            /* tail phase, a second kernel that gives           */
                             /* each a warp of 32 cooperating lanes (0 = 32)     */
   int32_t reserved;         /* reserved, must be 0                              */
 } ptg_options;
